@@ -1,0 +1,156 @@
+// common.cuh -- shared device infrastructure of libmctdhb_b200.
+//
+// Configuration ranking.  The reference ranks an occupation vector n of N
+// bosons in M orbitals with (space.c:159-178)
+//     hash(n) = sum_{m=M-1..1} sum_{t<n_m} dim(N_basket - t, m)
+// which telescopes into a combinatorial-number-system rank over the
+// cumulative occupations L_m = n_0 + ... + n_m:
+//     hash(n) = D - 1 - sum_{m=0}^{M-2} T_m(L_m),   T_m(L) = C(L+m, m+1),
+// D = C(N+M-1, M-1).  Every jump map entry of the reference (space.c:202,
+// 297, 399) is therefore a sum over the few m whose L_m a particle move
+// shifts: moving bosons changes L_m by dL_m in {-2..2} and
+//     j = i - sum_m [T_m(L_m + dL_m) - T_m(L_m)].
+// Each thread precomputes F[m][d] = T_m(L_m + d) - T_m(L_m) for its row, so a
+// jump costs a handful of register adds and the 2.6-48 GB map tables of the
+// reference never have to be read (or even built) on the hot path.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+
+namespace mctdhb {
+
+constexpr int kMaxOrb = 30;      // MAX_ORBITALS of the reference
+constexpr int kMaxTemplOrb = 8;  // orbital counts with a register-resident kernel
+
+// thread-local error record of the C ABI (the reference calls exit(); this
+// library reports instead)
+void set_error(const char* fmt, ...);
+const char* last_error();
+void clear_error();
+
+#define MCTDHB_CUDA_TRY(call)                                                  \
+    do {                                                                       \
+        cudaError_t _e = (call);                                               \
+        if (_e != cudaSuccess) {                                               \
+            ::mctdhb::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,     \
+                                cudaGetErrorString(_e));                       \
+            return -1;                                                         \
+        }                                                                      \
+    } while (0)
+
+// Device view of one Fock space.  T is the (M-1) x (N+1) rank-weight table,
+// sq the sqrt table sqrt(x), x = 0..N+2.
+struct SpaceView {
+    int N, M;
+    uint32_t dim;
+    const uint32_t* T;
+    const double* sq;
+};
+
+__host__ __device__ constexpr int dl_index(int d) { return d < 0 ? d + 2 : d + 1; }
+
+// Register-resident state of one configuration (row) of the Fock space.
+template <int M>
+struct RowState {
+    int n[M];                 // occupations
+    uint32_t F[M > 1 ? M - 1 : 1][4];  // T_m(L_m+d) - T_m(L_m), d = -2,-1,+1,+2
+};
+
+// Unrank `row` (greedy CNS decode, identical to set_config of space.c:138)
+// and fill the jump offsets.
+template <int M>
+__device__ __forceinline__ void load_row(const SpaceView& sp, uint32_t row,
+                                         RowState<M>& st) {
+    const int N = sp.N;
+    uint32_t S = sp.dim - 1u - row;
+    int Lnext = N;
+    int L[M > 1 ? M - 1 : 1];
+#pragma unroll
+    for (int m = M - 2; m >= 0; m--) {
+        const uint32_t* Tm = sp.T + m * (N + 1);
+        int lo = 0, hi = Lnext;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (__ldg(Tm + mid) <= S)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        S -= __ldg(Tm + lo);
+        st.n[m + 1] = Lnext - lo;
+        L[m] = lo;
+        Lnext = lo;
+    }
+    st.n[0] = Lnext;
+#pragma unroll
+    for (int m = 0; m < M - 1; m++) {
+        const uint32_t* Tm = sp.T + m * (N + 1);
+        uint32_t t0 = __ldg(Tm + L[m]);
+#pragma unroll
+        for (int di = 0; di < 4; di++) {
+            int d = di < 2 ? di - 2 : di - 1;
+            int x = L[m] + d;
+            x = x < 0 ? 0 : (x > N ? N : x);  // only reached by invalid moves
+            st.F[m][di] = __ldg(Tm + x) - t0;
+        }
+    }
+}
+
+// Rank of the configuration reached from `row` by removing bosons from
+// orbitals k and s and adding them to q and l (k==s, q==l allowed; a single
+// move k->l is jump(k, -1, l, -1) with -1 meaning "none").  All orbital
+// indices are compile-time constants after unrolling.
+template <int M>
+__device__ __forceinline__ uint32_t jump(const RowState<M>& st, uint32_t row,
+                                         int k, int s, int q, int l) {
+    uint32_t d = 0;
+#pragma unroll
+    for (int m = 0; m < M - 1; m++) {
+        int dl = (q >= 0 && m >= q) + (l >= 0 && m >= l) -
+                 (k >= 0 && m >= k) - (s >= 0 && m >= s);
+        if (dl != 0) d += st.F[m][dl_index(dl)];
+    }
+    return row - d;
+}
+
+// complex helpers on double2
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 acc) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+    return acc;
+}
+// acc += conj(a) * b
+__device__ __forceinline__ double2 cfma_conj(double2 a, double2 b, double2 acc) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(-a.y, b.x, acc.y);
+    return acc;
+}
+__device__ __forceinline__ double2 cscale(double2 a, double r) {
+    return make_double2(a.x * r, a.y * r);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+    return make_double2(a.x + b.x, a.y + b.y);
+}
+
+inline int num_sms() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+}  // namespace mctdhb

@@ -1,0 +1,247 @@
+// density.cu -- one- and two-body density matrices rho1 (M x M) and rho2
+// (M^4) in one pass over the configurations (replaces set_onebody_dm and
+// set_twobody_dm, density_matrices.c:9-443, which make one full pass over
+// the coefficients per unique element).
+//
+// Every unique element of the reference (its rules 1-8 for rho2 plus rho1)
+// is a sum over rows i of conj(C_i) C_j b(n_i) for one particle move; the
+// kernel visits each row once, computes all its element contributions in
+// registers (moves.cuh order) and reduces them across the warp in groups of
+// eight with a transposed butterfly (4.5 shuffles per element instead of
+// 20), accumulating into warp-private shared memory.  Blocks write partial
+// sums; dens_finalize adds them in a fixed order and fills rho1/rho2 with
+// the reference's symmetric pattern.  The result is deterministic for a
+// given launch geometry, which depends only on the Fock-space size.
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "moves.cuh"
+
+namespace mctdhb {
+
+// generic M (<= 30): runtime loops, contributions reduced naively across the
+// warp and accumulated into the warp's own slice of the global partial buffer
+// (the element count grows as M^4/4, too large for shared memory).
+// Correctness path for orbital counts without a register-resident kernel.
+__global__ void __launch_bounds__(128)
+    dens_generic_kernel(SpaceView sp, const double2* __restrict__ C, double2* __restrict__ partial,
+                        int EP) {
+    const int M = sp.M, N = sp.N;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t gwarp = blockIdx.x * nwarps + warp;
+    double2* wacc = partial + (size_t)gwarp * EP;
+    for (int i = lane; i < EP; i += 32) wacc[i] = make_double2(0.0, 0.0);
+    __syncwarp();
+    const uint32_t twarps = gridDim.x * nwarps;
+    for (uint32_t base = gwarp * 32u; base < sp.dim; base += twarps * 32u) {
+        const uint32_t row = base + lane;
+        const bool live = row < sp.dim;
+        int n[kMaxOrb], L[kMaxOrb];
+        for (int m = 0; m < M; m++) n[m] = 0, L[m] = 0;
+        double2 ci = make_double2(0.0, 0.0);
+        if (live) {
+            uint32_t S = sp.dim - 1u - row;
+            int Lnext = N;
+            for (int m = M - 2; m >= 0; m--) {
+                const uint32_t* Tm = sp.T + m * (N + 1);
+                int lo = 0, hi = Lnext;
+                while (lo < hi) {
+                    int mid = (lo + hi + 1) >> 1;
+                    if (Tm[mid] <= S)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                S -= Tm[lo];
+                n[m + 1] = Lnext - lo;
+                L[m] = lo;
+                Lnext = lo;
+            }
+            n[0] = Lnext;
+            ci = C[row];
+        }
+        auto target = [&](int k, int s, int q, int l) -> uint32_t {
+            uint32_t d = 0;
+            for (int m = 0; m < M - 1; m++) {
+                int dl = (q >= 0 && m >= q) + (l >= 0 && m >= l) - (k >= 0 && m >= k) -
+                         (s >= 0 && m >= s);
+                if (dl != 0) {
+                    const uint32_t* Tm = sp.T + m * (N + 1);
+                    d += Tm[L[m] + dl] - Tm[L[m]];
+                }
+            }
+            return row - d;
+        };
+        const double m2 = ci.x * ci.x + ci.y * ci.y;
+        int e = 0;
+        double2 t1 = make_double2(0.0, 0.0);
+        for_each_density_element(M, [&](int kind, int k, int s, int q, int l) {
+            double2 x = make_double2(0.0, 0.0);
+            switch (kind) {
+                case D_R1_DIAG: x.x = m2 * n[k]; break;
+                case D_R2_KKKK: x.x = m2 * (n[k] * (n[k] - 1)); break;
+                case D_R2_KSKS: x.x = m2 * (n[k] * n[s]); break;
+                case D_R1_OFF:  // k -> l single move, l stored in s
+                    t1 = make_double2(0.0, 0.0);
+                    if (live && n[k] > 0) {
+                        const uint32_t j = target(k, -1, s, -1);
+                        t1 = cscale(cfma_conj(ci, C[j], make_double2(0.0, 0.0)),
+                                    sp.sq[n[k]] * sp.sq[n[s] + 1]);
+                    }
+                    x = t1;
+                    break;
+                case D_R2_KKKL: x = cscale(t1, (double)(n[k] - 1)); break;
+                case D_R2_KLLL: x = cscale(t1, (double)n[s]); break;
+                case D_R2_KSSL: x = cscale(t1, (double)n[s]); break;
+                default: {
+                    const bool valid = (k == s) ? (n[k] >= 2) : (n[k] >= 1 && n[s] >= 1);
+                    if (live && valid) {
+                        const uint32_t j = target(k, s, q, l);
+                        double sa = (k == s) ? sp.sq[n[k]] * sp.sq[n[k] - 1] : sp.sq[n[k]] * sp.sq[n[s]];
+                        double sb = (q == l) ? sp.sq[n[q] + 1] * sp.sq[n[q] + 2]
+                                             : sp.sq[n[q] + 1] * sp.sq[n[l] + 1];
+                        x = cscale(cfma_conj(ci, C[j], make_double2(0.0, 0.0)), sa * sb);
+                    }
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                x.x += __shfl_xor_sync(0xffffffffu, x.x, o);
+                x.y += __shfl_xor_sync(0xffffffffu, x.y, o);
+            }
+            if (lane == 0) {
+                wacc[e].x += x.x;
+                wacc[e].y += x.y;
+            }
+            e++;
+        });
+    }
+}
+
+// one thread per element: fixed-order sum over block partials, then the
+// reference's symmetric fill (density_matrices.c:33-50, 86-442)
+__global__ void dens_finalize_kernel(int M, int E, int EP, int nblocks,
+                                     const double2* __restrict__ partial,
+                                     const int* __restrict__ desc, double2* __restrict__ rho1,
+                                     double2* __restrict__ rho2) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    double2 v = partial[e];
+    for (int b = 1; b < nblocks; b++) {
+        double2 p = partial[(size_t)b * EP + e];
+        v.x += p.x;
+        v.y += p.y;
+    }
+    const int kind = desc[5 * e], k = desc[5 * e + 1], s = desc[5 * e + 2], q = desc[5 * e + 3],
+              l = desc[5 * e + 4];
+    const double2 c = make_double2(v.x, -v.y);
+    const int M2 = M * M, M3 = M2 * M;
+    auto R = [&](int a, int b, int cc, int d) -> double2& { return rho2[a + b * M + cc * M2 + d * M3]; };
+    switch (kind) {
+        case D_R1_DIAG: rho1[k * M + k] = v; break;
+        case D_R2_KKKK: R(k, k, k, k) = v; break;
+        case D_R2_KSKS:
+            R(k, s, k, s) = v; R(s, k, k, s) = v; R(s, k, s, k) = v; R(k, s, s, k) = v;
+            break;
+        case D_R1_OFF:  // (k, l) stored as (k, s=l)
+            rho1[k * M + s] = v;
+            rho1[s * M + k] = c;
+            break;
+        case D_R2_KKKL:
+            R(k, k, k, l) = v; R(k, k, l, k) = v; R(l, k, k, k) = c; R(k, l, k, k) = c;
+            break;
+        case D_R2_KLLL:  // (k, l, l, l) stored as (k, s=l, q=l, l)
+            R(k, l, l, l) = v; R(l, k, l, l) = v; R(l, l, l, k) = c; R(l, l, k, l) = c;
+            break;
+        case D_R2_KSSL:
+            R(k, s, s, l) = v; R(s, k, s, l) = v; R(s, k, l, s) = v; R(k, s, l, s) = v;
+            R(l, s, s, k) = c; R(s, l, s, k) = c; R(s, l, k, s) = c; R(l, s, k, s) = c;
+            break;
+        case D_R2_KKQQ:
+            R(k, k, q, q) = v; R(q, q, k, k) = c;
+            break;
+        case D_R2_KKQL:
+            R(k, k, q, l) = v; R(k, k, l, q) = v; R(l, q, k, k) = c; R(q, l, k, k) = c;
+            break;
+        case D_R2_KSQL:
+            R(k, s, q, l) = v; R(s, k, q, l) = v; R(k, s, l, q) = v; R(s, k, l, q) = v;
+            break;
+    }
+}
+
+int dens_descriptors(int M, int* desc) {
+    int e = 0;
+    for_each_density_element(M, [&](int kind, int k, int s, int q, int l) {
+        if (desc) {
+            desc[5 * e] = kind;
+            desc[5 * e + 1] = k;
+            desc[5 * e + 2] = s;
+            desc[5 * e + 3] = q;
+            desc[5 * e + 4] = l;
+        }
+        e++;
+    });
+    return e;
+}
+
+static int dens_ep(int M) { return (dens_nelem(M) + 7) / 8 * 8; }
+
+static bool dens_templated(int M) { return M >= 2 && M <= kMaxTemplOrb; }
+
+int dens_grid(const SpaceView& sp) {
+    uint64_t need = ((uint64_t)sp.dim + 127) / 128;
+    uint64_t cap = dens_templated(sp.M) ? (uint64_t)num_sms() * 2 : 16;
+    return (int)std::max<uint64_t>(1, std::min(need, cap));
+}
+
+// number of partial slices the finalize pass adds: blocks for the templated
+// kernels, warps for the generic one
+static int dens_slices(const SpaceView& sp) {
+    return dens_templated(sp.M) ? dens_grid(sp) : dens_grid(sp) * 4;
+}
+
+size_t dens_partial_elems(const SpaceView& sp) {
+    return (size_t)dens_slices(sp) * dens_ep(sp.M);
+}
+
+int dens_prepare(const SpaceView& sp) {
+    switch (sp.M) {
+        case 2: return dens_launch_tmpl<2>(sp, nullptr, nullptr, 0, 0);
+        case 3: return dens_launch_tmpl<3>(sp, nullptr, nullptr, 0, 0);
+        case 4: return dens_launch_tmpl<4>(sp, nullptr, nullptr, 0, 0);
+        case 5: return dens_launch_tmpl<5>(sp, nullptr, nullptr, 0, 0);
+        case 6: return dens_launch_tmpl<6>(sp, nullptr, nullptr, 0, 0);
+        case 7: return dens_launch_tmpl<7>(sp, nullptr, nullptr, 0, 0);
+        case 8: return dens_launch_tmpl<8>(sp, nullptr, nullptr, 0, 0);
+        default: return 0;
+    }
+}
+
+int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
+               double2* rho2, const int* d_desc, cudaStream_t st) {
+    const int grid = dens_grid(sp);
+    const int M = sp.M;
+    const int EP = dens_ep(M);
+    int rc = 0;
+    switch (M) {
+        case 2: rc = dens_launch_tmpl<2>(sp, C, partial, grid, st); break;
+        case 3: rc = dens_launch_tmpl<3>(sp, C, partial, grid, st); break;
+        case 4: rc = dens_launch_tmpl<4>(sp, C, partial, grid, st); break;
+        case 5: rc = dens_launch_tmpl<5>(sp, C, partial, grid, st); break;
+        case 6: rc = dens_launch_tmpl<6>(sp, C, partial, grid, st); break;
+        case 7: rc = dens_launch_tmpl<7>(sp, C, partial, grid, st); break;
+        case 8: rc = dens_launch_tmpl<8>(sp, C, partial, grid, st); break;
+        default:
+            dens_generic_kernel<<<grid, 128, 0, st>>>(sp, C, partial, EP);
+            MCTDHB_CUDA_TRY(cudaGetLastError());
+    }
+    if (rc) return rc;
+    const int E = dens_nelem(M);
+    dens_finalize_kernel<<<(E + 127) / 128, 128, 0, st>>>(M, E, EP, dens_slices(sp), partial,
+                                                          d_desc, rho1, rho2);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace mctdhb

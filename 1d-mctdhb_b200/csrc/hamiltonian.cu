@@ -1,0 +1,204 @@
+// hamiltonian.cu -- the many-body Hamiltonian action HC = H C in complex128
+// (replaces apply_hamiltonian, hamiltonian.c:7-406 of the reference).
+//
+// Design (B200): H.C is a gather-bound sparse action (~0.5 flop/byte), so
+// the kernel is organised around the gathers, not around arithmetic:
+//   * one thread per configuration (row); consecutive rows of a warp reach
+//     consecutive neighbours for every move (the rank offset of a move is
+//     constant over runs of rows that differ only in orbitals 0 and 1), so
+//     each gather of the warp is a coalesced 16-byte-per-lane load;
+//   * jump targets come from the rank offsets F[m][d] held in registers --
+//     no map table is read (the reference's maps would cost 4 bytes of
+//     index per 16 bytes of coefficient, and do not fit at N=30, M=8);
+//   * every distinct neighbour is gathered once, with all rules that reach
+//     it folded into one coefficient (moves.cuh);
+//   * h_kl / g_ksql enter through a packed coefficient table staged in
+//     shared memory (uniform broadcast loads);
+//   * for M <= 8 the move loops are fully unrolled so occupations, rank
+//     offsets and sqrt factors stay in registers;  larger M use a generic
+//     runtime-loop kernel.
+#include "common.cuh"
+#include "kernels.h"
+#include "moves.cuh"
+
+namespace mctdhb {
+
+// ---------------------------------------------------------------------------
+// coefficient table (hob row-major M*M, hint M^4) -> packed table
+// ---------------------------------------------------------------------------
+__global__ void hc_prep_kernel(int M, const double2* __restrict__ hob,
+                               const double2* __restrict__ hint,
+                               double2* __restrict__ tab) {
+    const int M2 = M * M, M3 = M2 * M;
+    auto g = [&](int a, int b, int c, int d) { return hint[a + b * M + c * M2 + d * M3]; };
+    const int nd = hc_ndiag(M), ns = hc_nsingle(M);
+    // one thread does the (tiny) enumeration in order; the table is a few KB
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int p = 0;
+    for (int k = 0; k < M; k++) tab[p++] = hob[k * M + k];
+    for (int k = 0; k < M; k++) tab[p++] = cscale(g(k, k, k, k), 0.5);
+    for (int k = 0; k < M; k++)
+        for (int s = k + 1; s < M; s++) tab[p++] = cscale(g(k, s, k, s), 2.0);
+    for (int k = 0; k < M; k++)
+        for (int l = 0; l < M; l++) {
+            if (l == k) continue;
+            double2 gk = g(k, k, k, l);
+            double2 h = hob[k * M + l];
+            tab[p++] = make_double2(h.x - gk.x, h.y - gk.y);
+            for (int s = 0; s < M; s++) {
+                if (s == k)
+                    tab[p++] = gk;
+                else if (s == l)
+                    tab[p++] = g(k, l, l, l);
+                else
+                    tab[p++] = cscale(g(k, s, s, l), 2.0);
+            }
+        }
+    (void)nd;
+    (void)ns;
+    for (int k = 0; k < M; k++)
+        for (int s = k; s < M; s++)
+            for (int q = 0; q < M; q++)
+                for (int l = q; l < M; l++) {
+                    if (q == k || q == s || l == k || l == s) continue;
+                    double f = (k == s && q == l) ? 0.5 : ((k == s || q == l) ? 1.0 : 2.0);
+                    tab[p++] = cscale(g(k, s, q, l), f);
+                }
+}
+
+// ---------------------------------------------------------------------------
+// generic kernel, any M <= 30 (runtime loops, local arrays)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+    hc_generic_kernel(SpaceView sp, const double2* __restrict__ C, double2* __restrict__ HC,
+                      const double2* __restrict__ tab, HcEpilogue ep) {
+    if (ep.flag != nullptr && *ep.flag != 0) return;
+    const int M = sp.M, N = sp.N;
+    const int ND = hc_ndiag(M), NS = hc_nsingle(M);
+    double2 dot_acc = make_double2(0.0, 0.0);
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < sp.dim;
+         row += gridDim.x * blockDim.x) {
+        int n[kMaxOrb], L[kMaxOrb];
+        uint32_t S = sp.dim - 1u - row;
+        int Lnext = N;
+        for (int m = M - 2; m >= 0; m--) {
+            const uint32_t* Tm = sp.T + m * (N + 1);
+            int lo = 0, hi = Lnext;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (Tm[mid] <= S)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            S -= Tm[lo];
+            n[m + 1] = Lnext - lo;
+            L[m] = lo;
+            Lnext = lo;
+        }
+        n[0] = Lnext;
+        auto rank_delta = [&](int k, int s, int q, int l) -> uint32_t {
+            uint32_t d = 0;
+            for (int m = 0; m < M - 1; m++) {
+                int dl = (q >= 0 && m >= q) + (l >= 0 && m >= l) - (k >= 0 && m >= k) -
+                         (s >= 0 && m >= s);
+                if (dl != 0) {
+                    const uint32_t* Tm = sp.T + m * (N + 1);
+                    d += Tm[L[m] + dl] - Tm[L[m]];
+                }
+            }
+            return row - d;
+        };
+        const double2 ci = C[row];
+        double2 dg = make_double2(0.0, 0.0);
+        for (int k = 0; k < M; k++) {
+            dg = cadd(dg, cscale(tab[k], (double)n[k]));
+            dg = cadd(dg, cscale(tab[M + k], (double)(n[k] * (n[k] - 1))));
+        }
+        int p = 2 * M;
+        for (int k = 0; k < M; k++)
+            for (int s = k + 1; s < M; s++, p++) dg = cadd(dg, cscale(tab[p], (double)(n[k] * n[s])));
+        double2 acc = cmul(dg, ci);
+        p = ND;
+        for (int k = 0; k < M; k++)
+            for (int l = 0; l < M; l++) {
+                if (l == k) continue;
+                if (n[k] > 0) {
+                    const uint32_t j = rank_delta(k, -1, l, -1);
+                    double2 c = tab[p];
+                    for (int s = 0; s < M; s++) c = cadd(c, cscale(tab[p + 1 + s], (double)n[s]));
+                    acc = cfma(cscale(c, sp.sq[n[k]] * sp.sq[n[l] + 1]), C[j], acc);
+                }
+                p += M + 1;
+            }
+        p = ND + NS;
+        for (int k = 0; k < M; k++)
+            for (int s = k; s < M; s++) {
+                const bool valid = (k == s) ? (n[k] >= 2) : (n[k] >= 1 && n[s] >= 1);
+                const double sa = valid ? ((k == s) ? sp.sq[n[k]] * sp.sq[n[k] - 1]
+                                                    : sp.sq[n[k]] * sp.sq[n[s]])
+                                        : 0.0;
+                for (int q = 0; q < M; q++)
+                    for (int l = q; l < M; l++) {
+                        if (q == k || q == s || l == k || l == s) continue;
+                        if (valid) {
+                            const uint32_t j = rank_delta(k, s, q, l);
+                            const double sb = (q == l) ? sp.sq[n[q] + 1] * sp.sq[n[q] + 2]
+                                                       : sp.sq[n[q] + 1] * sp.sq[n[l] + 1];
+                            acc = cfma(tab[p], cscale(C[j], sa * sb), acc);
+                        }
+                        p++;
+                    }
+            }
+        if (ep.prev != nullptr) {
+            const double2 pv = ep.prev[row];
+            const double b = *ep.beta;
+            acc.x -= b * pv.x;
+            acc.y -= b * pv.y;
+        }
+        HC[row] = acc;
+        if (ep.dot_partial != nullptr) dot_acc = cfma_conj(ci, acc, dot_acc);
+    }
+    if (ep.dot_partial != nullptr) block_reduce_store(dot_acc, ep.dot_partial);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+int hc_prep(int M, const double2* d_hob, const double2* d_hint, double2* d_tab,
+            cudaStream_t st) {
+    hc_prep_kernel<<<1, 32, 0, st>>>(M, d_hob, d_hint, d_tab);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int hc_grid(const SpaceView& sp) {
+    if (sp.M >= 2 && sp.M <= kMaxTemplOrb) {
+        uint64_t need = ((uint64_t)sp.dim + 255) / 256;
+        uint64_t cap = (uint64_t)num_sms() * 2;
+        return (int)(need < cap ? (need ? need : 1) : cap);
+    }
+    uint64_t need = ((uint64_t)sp.dim + 127) / 128;
+    uint64_t cap = (uint64_t)num_sms() * 8;
+    return (int)(need < cap ? (need ? need : 1) : cap);
+}
+
+int hc_apply(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+             const HcEpilogue& ep, cudaStream_t st) {
+    const int grid = hc_grid(sp);
+    switch (sp.M) {
+        case 2: return hc_launch_tmpl<2>(sp, C, HC, tab, ep, grid, st);
+        case 3: return hc_launch_tmpl<3>(sp, C, HC, tab, ep, grid, st);
+        case 4: return hc_launch_tmpl<4>(sp, C, HC, tab, ep, grid, st);
+        case 5: return hc_launch_tmpl<5>(sp, C, HC, tab, ep, grid, st);
+        case 6: return hc_launch_tmpl<6>(sp, C, HC, tab, ep, grid, st);
+        case 7: return hc_launch_tmpl<7>(sp, C, HC, tab, ep, grid, st);
+        case 8: return hc_launch_tmpl<8>(sp, C, HC, tab, ep, grid, st);
+        default:
+            hc_generic_kernel<<<grid, 128, 0, st>>>(sp, C, HC, tab, ep);
+            MCTDHB_CUDA_TRY(cudaGetLastError());
+            return 0;
+    }
+}
+
+}  // namespace mctdhb

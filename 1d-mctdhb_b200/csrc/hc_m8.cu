@@ -1,0 +1,6 @@
+// H.C kernel instantiation for 8 orbitals (own translation unit: parallel build)
+#include "hc_tmpl.cuh"
+namespace mctdhb {
+template int hc_launch_tmpl<8>(const SpaceView&, const double2*, double2*, const double2*,
+                                const HcEpilogue&, int, cudaStream_t);
+}

@@ -1,0 +1,130 @@
+// hc_tmpl.cuh -- register-resident H.C kernel for M <= 8 orbitals, one
+// explicit instantiation per translation unit (hc_m*.cu).  See
+// hamiltonian.cu for the design notes and moves.cuh for the coefficient
+// folding.
+#pragma once
+#include "common.cuh"
+#include "kernels.h"
+#include "movelist.cuh"
+
+namespace mctdhb {
+
+// jump target with compile-time orbitals (k, s removed; q, l added; -1 none)
+template <int M, int k, int s, int q, int l>
+__device__ __forceinline__ uint32_t jumpc(const RowState<M>& st, uint32_t row) {
+    uint32_t d = 0;
+    static_for<M - 1>([&](auto mi) {
+        constexpr int m = decltype(mi)::value;
+        constexpr int dl = (q >= 0 && m >= q) + (l >= 0 && m >= l) - (k >= 0 && m >= k) -
+                           (s >= 0 && m >= s);
+        if constexpr (dl != 0) d += st.F[m][dl_index(dl)];
+    });
+    return row - d;
+}
+
+template <int M>
+__global__ void __launch_bounds__(256, 2)
+    hc_kernel(SpaceView sp, const double2* __restrict__ C, double2* __restrict__ HC,
+              const double2* __restrict__ tab_g, HcEpilogue ep) {
+    constexpr int TAB = hc_table_size(M);
+    constexpr int NMOVE = HcMoveList<M>::N;
+    __shared__ double2 tab[TAB];
+    for (int i = threadIdx.x; i < TAB; i += blockDim.x) tab[i] = tab_g[i];
+    __syncthreads();
+    if (ep.flag != nullptr && *ep.flag != 0) return;  // Lanczos breakdown: no-op
+
+    double2 dot_acc = make_double2(0.0, 0.0);
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < sp.dim;
+         row += gridDim.x * blockDim.x) {
+        RowState<M> st;
+        load_row<M>(sp, row, st);
+        double sq0[M], sq1[M];
+        static_for<M>([&](auto mi) {
+            constexpr int m = decltype(mi)::value;
+            sq0[m] = __ldg(sp.sq + st.n[m]);
+            sq1[m] = __ldg(sp.sq + st.n[m] + 1);
+        });
+        const double2 ci = __ldg(C + row);
+
+        // diagonal: h_kk n_k + 1/2 g_kkkk n_k (n_k - 1) + 2 g_ksks n_k n_s
+        double2 dg = make_double2(0.0, 0.0);
+        static_for<M>([&](auto ki) {
+            constexpr int k = decltype(ki)::value;
+            dg = cadd(dg, cscale(tab[k], (double)st.n[k]));
+            dg = cadd(dg, cscale(tab[M + k], (double)(st.n[k] * (st.n[k] - 1))));
+            static_for<M>([&](auto si) {
+                constexpr int s = decltype(si)::value;
+                if constexpr (s > k) {
+                    constexpr int p = 2 * M + k * M - k * (k + 1) / 2 + (s - k - 1);
+                    dg = cadd(dg, cscale(tab[p], (double)(st.n[k] * st.n[s])));
+                }
+            });
+        });
+        double2 acc = cmul(dg, ci);
+
+        bool vs = false;
+        double sa = 0.0;
+        double2 as = make_double2(0.0, 0.0);
+        static_for<NMOVE>([&](auto ei) {
+            constexpr HcMove mv = kHcMoves<M>.m[decltype(ei)::value];
+            constexpr int k = mv.k, s = mv.s, q = mv.q, l = mv.l;
+            if constexpr (s < 0) {
+                // single move k -> q
+                if (st.n[k] > 0) {
+                    const uint32_t j = jumpc<M, k, -1, q, -1>(st, row);
+                    const double2 cj = __ldg(C + j);
+                    double2 c = tab[mv.tab];
+                    static_for<M>([&](auto xi) {
+                        constexpr int x = decltype(xi)::value;
+                        c = cadd(c, cscale(tab[mv.tab + 1 + x], (double)st.n[x]));
+                    });
+                    acc = cfma(cscale(c, sq0[k] * sq1[q]), cj, acc);
+                }
+            } else {
+                // double move (k, s) -> (q, l), accumulated per source pair
+                if constexpr (mv.first) {
+                    if constexpr (k == s) {
+                        vs = st.n[k] >= 2;
+                        sa = vs ? sq0[k] * __ldg(sp.sq + st.n[k] - 1) : 0.0;
+                    } else {
+                        vs = st.n[k] >= 1 && st.n[s] >= 1;
+                        sa = sq0[k] * sq0[s];
+                    }
+                    as = make_double2(0.0, 0.0);
+                }
+                if (vs) {
+                    const uint32_t j = jumpc<M, k, s, q, l>(st, row);
+                    const double2 cj = __ldg(C + j);
+                    double sb;
+                    if constexpr (q == l)
+                        sb = sq1[q] * __ldg(sp.sq + st.n[q] + 2);
+                    else
+                        sb = sq1[q] * sq1[l];
+                    as = cfma(tab[mv.tab], cscale(cj, sb), as);
+                }
+                if constexpr (mv.last) acc = cadd(acc, cscale(as, sa));
+            }
+        });
+
+        // Lanczos epilogue: out = HC - beta * prev; dot += conj(C) * out
+        if (ep.prev != nullptr) {
+            const double2 pv = __ldg(ep.prev + row);
+            const double b = *ep.beta;
+            acc.x -= b * pv.x;
+            acc.y -= b * pv.y;
+        }
+        HC[row] = acc;
+        if (ep.dot_partial != nullptr) dot_acc = cfma_conj(ci, acc, dot_acc);
+    }
+    if (ep.dot_partial != nullptr) block_reduce_store(dot_acc, ep.dot_partial);
+}
+
+template <int M>
+int hc_launch_tmpl(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+                   const HcEpilogue& ep, int grid, cudaStream_t st) {
+    hc_kernel<M><<<grid, 256, 0, st>>>(sp, C, HC, tab, ep);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace mctdhb

@@ -1,0 +1,83 @@
+// kernels.h -- internal launch interface between the kernel files and the
+// host runtime (space.cu, capi.cu).  Not part of the public C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace mctdhb {
+
+// Optional fused epilogue of the H.C kernel, used by the Lanczos recurrence
+// (multiconfig_lanczos.c:40-41, 78-83): out = H v - beta * prev and the
+// per-block partials of <v, out>.  `flag` != 0 turns the launch into a no-op
+// (a breakdown detected on the device earlier in the same step).
+struct HcEpilogue {
+    const int* flag = nullptr;
+    const double2* prev = nullptr;
+    const double* beta = nullptr;
+    double2* dot_partial = nullptr;
+};
+
+// Deterministic block reduction of one complex value per thread; thread 0
+// writes the block's sum to out[blockIdx.x].  Every thread must call it.
+__device__ __forceinline__ void block_reduce_store(double2 v, double2* out) {
+    __shared__ double2 red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 s = red[0];
+        for (int i = 1; i < nw; i++) {
+            s.x += red[i].x;
+            s.y += red[i].y;
+        }
+        out[blockIdx.x] = s;
+    }
+}
+
+// per-M register-resident kernels (hc_tmpl.cuh / dens_tmpl.cuh, explicit
+// instantiations in hc_m*.cu / dens_m*.cu)
+template <int M>
+int hc_launch_tmpl(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+                   const HcEpilogue& ep, int grid, cudaStream_t st);
+template <int M>
+int dens_launch_tmpl(const SpaceView& sp, const double2* C, double2* partial, int grid,
+                     cudaStream_t st);
+
+// hamiltonian.cu
+int hc_prep(int M, const double2* d_hob, const double2* d_hint, double2* d_tab,
+            cudaStream_t st);
+int hc_grid(const SpaceView& sp);
+int hc_apply(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+             const HcEpilogue& ep, cudaStream_t st);
+
+// density.cu
+int dens_grid(const SpaceView& sp);
+size_t dens_partial_elems(const SpaceView& sp);  // doubles2 in the partial buffer
+int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
+               double2* rho2, const int* d_desc, cudaStream_t st);
+int dens_descriptors(int M, int* host_desc);
+int dens_prepare(const SpaceView& sp);  // one-time launch attributes  // returns count; desc = 5 ints/elem
+
+// space.cu (map kernels)
+int build_hash_table(const SpaceView& sp, uint16_t* d_ht, cudaStream_t st);
+int build_single_map(const SpaceView& sp, uint32_t* d_map, cudaStream_t st);
+int count_double_chunks(const SpaceView& sp, int diff, uint64_t* d_cnt, cudaStream_t st);
+int exclusive_scan_u64(uint64_t* d_data, uint64_t n, uint64_t* d_total, void* d_tmp,
+                       size_t tmp_bytes, cudaStream_t st);
+size_t exclusive_scan_tmp_bytes(uint64_t n);
+int build_double_map(const SpaceView& sp, int diff, const uint64_t* d_offsets,
+                     uint32_t* d_map, cudaStream_t st);
+int scale_offsets(uint64_t* d_off, uint64_t n, uint64_t factor, cudaStream_t st);
+
+// lanczos.cu
+struct LanczosDev;
+}  // namespace mctdhb

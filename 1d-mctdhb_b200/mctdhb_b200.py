@@ -1,0 +1,341 @@
+"""Python binding of libmctdhb_b200.so (include/mctdhb_gpu.h) via ctypes.
+
+Two layers, mirroring the C ABI:
+
+* `DropIn` -- the reference's own entry points (apply_hamiltonian,
+  set_onebody_dm, set_twobody_dm, lanczos, lowest_state_lanczos,
+  propagate_coef_sil, get_multiconf_struct, ...) called with host numpy
+  buffers laid out as the reference's structs (mctdhb_types.py).
+* `Space` -- the device-resident API on torch CUDA tensors (complex128),
+  used for throughput work.
+
+The product path has no CPU fallback: importing this module on a machine
+without the built library raises, and every call checks the C status and
+raises with the library's own error message.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+import mctdhb_types as T
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmctdhb_b200.so")
+
+# every symbol include/mctdhb_gpu.h declares
+EXPORTED = [
+    "mctdhb_gpu_last_error", "mctdhb_gpu_clear_error",
+    "space_dimension", "get_subspaces_dim", "set_config", "hash_index", "get_hash_table",
+    "get_single_jump_map", "get_double_diffjump_map", "get_double_equaljump_map",
+    "get_multiconf_struct", "destroy_multiconf_struct",
+    "apply_hamiltonian", "set_onebody_dm", "set_twobody_dm",
+    "lanczos", "lowest_state_lanczos", "propagate_coef_sil",
+    "total_energy", "eig_residual",
+    "mctdhb_space_create", "mctdhb_space_destroy", "mctdhb_space_dim",
+    "mctdhb_dev_set_matrices", "mctdhb_dev_apply_hamiltonian", "mctdhb_dev_density_matrices",
+    "mctdhb_dev_sil_step", "mctdhb_dev_hash_table", "mctdhb_dev_single_jump_map",
+    "mctdhb_dev_double_jump_chunks", "mctdhb_dev_double_jump_map",
+    "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
+    "mctdhb_step_create", "mctdhb_step_launch", "mctdhb_step_kernel_count",
+    "mctdhb_step_destroy",
+]
+
+_lib = None
+
+
+class MctdhbError(RuntimeError):
+    pass
+
+
+def load(path=LIB_PATH):
+    """Load the library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise MctdhbError(f"{path} is missing: build it with `python {HERE}/build.py`")
+    L = C.CDLL(path, mode=C.RTLD_LOCAL)
+    vp, u16, u32, i = C.c_void_p, C.c_uint16, C.c_uint32, C.c_int
+    L.mctdhb_gpu_last_error.restype = C.c_char_p
+    L.space_dimension.restype = u32
+    L.space_dimension.argtypes = [u16, u16]
+    L.get_subspaces_dim.restype = C.POINTER(u32)
+    L.get_subspaces_dim.argtypes = [u16, u16]
+    L.set_config.argtypes = [u32, u16, u16, C.POINTER(u16)]
+    L.hash_index.restype = u32
+    L.hash_index.argtypes = [u16, u16, C.POINTER(u32), C.POINTER(u16)]
+    L.get_hash_table.restype = C.POINTER(u16)
+    L.get_hash_table.argtypes = [u16, u16]
+    L.get_single_jump_map.restype = C.POINTER(u32)
+    L.get_single_jump_map.argtypes = [u16, u16, C.POINTER(u32), C.POINTER(u16)]
+    for f in (L.get_double_diffjump_map, L.get_double_equaljump_map):
+        f.restype = C.POINTER(u32)
+        f.argtypes = [u16, u16, C.POINTER(u32), C.POINTER(u16), C.POINTER(u32)]
+    L.get_multiconf_struct.restype = T.MultiConfiguration
+    L.get_multiconf_struct.argtypes = [u16, u16]
+    L.destroy_multiconf_struct.argtypes = [T.MultiConfiguration]
+    L.apply_hamiltonian.argtypes = [T.MultiConfiguration, T.Carray, T.Cmatrix, T.Carray, T.Carray]
+    L.set_onebody_dm.argtypes = [T.MultiConfiguration, T.Carray, T.Cmatrix]
+    L.set_twobody_dm.argtypes = [T.MultiConfiguration, T.Carray, T.Carray]
+    L.lanczos.restype = i
+    L.lanczos.argtypes = [T.MultiConfiguration, T.Cmatrix, T.Carray, i, T.Carray, T.Carray,
+                          T.Cmatrix]
+    L.lowest_state_lanczos.restype = C.c_double
+    L.lowest_state_lanczos.argtypes = [u16, T.MultiConfiguration, T.Cmatrix, T.Carray, T.Carray]
+    L.propagate_coef_sil.argtypes = [T.MCTDHBDataStruct, T.Carray]
+    L.total_energy.restype = T.dcomplex
+    L.total_energy.argtypes = [T.ManyBodyState]
+    L.eig_residual.restype = C.c_double
+    L.eig_residual.argtypes = [T.MultiConfiguration, T.Carray, T.Cmatrix, T.Carray, C.c_double]
+    L.mctdhb_space_create.restype = i
+    L.mctdhb_space_create.argtypes = [u16, u16, C.POINTER(vp)]
+    L.mctdhb_space_destroy.argtypes = [vp]
+    L.mctdhb_space_dim.restype = u32
+    L.mctdhb_space_dim.argtypes = [vp]
+    L.mctdhb_dev_set_matrices.restype = i
+    L.mctdhb_dev_set_matrices.argtypes = [vp, vp, vp, vp]
+    L.mctdhb_dev_apply_hamiltonian.restype = i
+    L.mctdhb_dev_apply_hamiltonian.argtypes = [vp, vp, vp, vp]
+    L.mctdhb_dev_density_matrices.restype = i
+    L.mctdhb_dev_density_matrices.argtypes = [vp, vp, vp, vp, vp]
+    L.mctdhb_dev_sil_step.restype = i
+    L.mctdhb_dev_sil_step.argtypes = [vp, vp, i, C.c_double, i, vp]
+    L.mctdhb_dev_hash_table.restype = i
+    L.mctdhb_dev_hash_table.argtypes = [vp, vp, vp]
+    L.mctdhb_dev_single_jump_map.restype = i
+    L.mctdhb_dev_single_jump_map.argtypes = [vp, vp, vp]
+    L.mctdhb_dev_double_jump_chunks.restype = i
+    L.mctdhb_dev_double_jump_chunks.argtypes = [vp, i, C.POINTER(C.c_uint64)]
+    L.mctdhb_dev_double_jump_map.restype = i
+    L.mctdhb_dev_double_jump_map.argtypes = [vp, i, vp, vp, vp]
+    L.sync_density_matrices.argtypes = [T.MultiConfiguration, T.ManyBodyState]
+    L.set_regulatization_factor.argtypes = [C.c_double]
+    L.get_current_regularization_factor.restype = C.c_double
+    L.mctdhb_step_create.restype = i
+    L.mctdhb_step_create.argtypes = [vp, vp, vp, vp, i, C.c_double, i, C.POINTER(vp)]
+    L.mctdhb_step_launch.restype = i
+    L.mctdhb_step_launch.argtypes = [vp, vp]
+    L.mctdhb_step_kernel_count.restype = i
+    L.mctdhb_step_kernel_count.argtypes = [vp]
+    L.mctdhb_step_destroy.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def last_error():
+    return load().mctdhb_gpu_last_error().decode()
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise MctdhbError(f"{what}: {last_error()}")
+
+
+def _stream_ptr(stream=None):
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+class Space:
+    """A Fock space (npar bosons, norb orbitals) on the current CUDA device."""
+
+    def __init__(self, npar, norb):
+        L = load()
+        h = C.c_void_p()
+        _check(L.mctdhb_space_create(npar, norb, C.byref(h)), "mctdhb_space_create")
+        self.h, self.npar, self.norb = h, npar, norb
+        self.dim = int(L.mctdhb_space_dim(h))
+
+    def close(self):
+        if self.h:
+            load().mctdhb_space_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_matrices(self, hob, hint, stream=None):
+        _check(load().mctdhb_dev_set_matrices(self.h, _ptr(hob), _ptr(hint), _stream_ptr(stream)),
+               "mctdhb_dev_set_matrices")
+
+    def apply_hamiltonian(self, coef, out, stream=None):
+        _check(load().mctdhb_dev_apply_hamiltonian(self.h, _ptr(coef), _ptr(out),
+                                                   _stream_ptr(stream)),
+               "mctdhb_dev_apply_hamiltonian")
+
+    def density_matrices(self, coef, rho1, rho2, stream=None):
+        _check(load().mctdhb_dev_density_matrices(self.h, _ptr(coef), _ptr(rho1), _ptr(rho2),
+                                                  _stream_ptr(stream)),
+               "mctdhb_dev_density_matrices")
+
+    def sil_step(self, coef, lanczos_iter, dt, imagtime, stream=None):
+        _check(load().mctdhb_dev_sil_step(self.h, _ptr(coef), lanczos_iter, dt, int(imagtime),
+                                          _stream_ptr(stream)),
+               "mctdhb_dev_sil_step")
+
+    def hash_table(self, out, stream=None):
+        _check(load().mctdhb_dev_hash_table(self.h, _ptr(out), _stream_ptr(stream)),
+               "mctdhb_dev_hash_table")
+
+    def single_jump_map(self, out, stream=None):
+        _check(load().mctdhb_dev_single_jump_map(self.h, _ptr(out), _stream_ptr(stream)),
+               "mctdhb_dev_single_jump_map")
+
+    def double_jump_chunks(self, diff):
+        n = C.c_uint64()
+        _check(load().mctdhb_dev_double_jump_chunks(self.h, int(diff), C.byref(n)),
+               "mctdhb_dev_double_jump_chunks")
+        return int(n.value)
+
+    def double_jump_map(self, diff, strides, out, stream=None):
+        _check(load().mctdhb_dev_double_jump_map(self.h, int(diff), _ptr(strides), _ptr(out),
+                                                 _stream_ptr(stream)),
+               "mctdhb_dev_double_jump_map")
+
+
+class Step:
+    """One configurational step (SIL + rho1/rho2) as a replayable CUDA graph
+    over fixed device tensors."""
+
+    def __init__(self, space, coef, rho1, rho2, lanczos_iter, dt, imagtime):
+        L = load()
+        h = C.c_void_p()
+        _check(L.mctdhb_step_create(space.h, _ptr(coef), _ptr(rho1), _ptr(rho2), lanczos_iter,
+                                    dt, int(imagtime), C.byref(h)), "mctdhb_step_create")
+        self.h = h
+        self.kernels = int(L.mctdhb_step_kernel_count(h))
+        self._keep = (space, coef, rho1, rho2)
+
+    def launch(self, stream=None):
+        _check(load().mctdhb_step_launch(self.h, _stream_ptr(stream)), "mctdhb_step_launch")
+
+    def close(self):
+        if self.h:
+            load().mctdhb_step_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DropIn:
+    """The reference's C entry points, on host numpy buffers."""
+
+    def __init__(self):
+        self.lib = load()
+
+    def space_dimension(self, N, M):
+        return int(self.lib.space_dimension(N, M))
+
+    def multiconf(self, N, M):
+        mc = self.lib.get_multiconf_struct(N, M)
+        if not mc:
+            raise MctdhbError(f"get_multiconf_struct: {last_error()}")
+        return mc
+
+    def destroy(self, mc):
+        self.lib.destroy_multiconf_struct(mc)
+
+    def apply_hamiltonian(self, mc, c, hob, hint):
+        c = np.ascontiguousarray(c, np.complex128)
+        hint = np.ascontiguousarray(hint, np.complex128).reshape(-1)
+        out = np.zeros_like(c)
+        H = T.RowMatrix(hob)
+        self.lib.mctdhb_gpu_clear_error()
+        self.lib.apply_hamiltonian(mc, T.carray(c), H.ptr, T.carray(hint), T.carray(out))
+        if last_error():
+            raise MctdhbError(last_error())
+        return out
+
+    def onebody_dm(self, mc, c):
+        M = mc.contents.norb
+        R = T.RowMatrix(np.zeros((M, M), np.complex128))
+        self.lib.mctdhb_gpu_clear_error()
+        self.lib.set_onebody_dm(mc, T.carray(np.ascontiguousarray(c, np.complex128)), R.ptr)
+        if last_error():
+            raise MctdhbError(last_error())
+        return R.a
+
+    def twobody_dm(self, mc, c):
+        M = mc.contents.norb
+        r = np.zeros(M ** 4, np.complex128)
+        self.lib.mctdhb_gpu_clear_error()
+        self.lib.set_twobody_dm(mc, T.carray(np.ascontiguousarray(c, np.complex128)), T.carray(r))
+        if last_error():
+            raise MctdhbError(last_error())
+        return r
+
+    def lanczos(self, mc, hob, hint, m, c0):
+        nc = mc.contents.dim
+        lv = np.zeros((m, nc), np.complex128)
+        lv[0] = c0
+        L = T.RowMatrix(lv)
+        diag = np.zeros(m, np.complex128)
+        offd = np.zeros(m, np.complex128)
+        H = T.RowMatrix(hob)
+        hint = np.ascontiguousarray(hint, np.complex128).reshape(-1)
+        it = self.lib.lanczos(mc, H.ptr, T.carray(hint), m, T.carray(diag), T.carray(offd), L.ptr)
+        if it < 0:
+            raise MctdhbError(last_error())
+        return it, diag, offd, L.a
+
+    def lowest_state_lanczos(self, mc, hob, hint, m, c):
+        c = np.ascontiguousarray(c, np.complex128).copy()
+        H = T.RowMatrix(hob)
+        hint = np.ascontiguousarray(hint, np.complex128).reshape(-1)
+        e = self.lib.lowest_state_lanczos(m, mc, H.ptr, T.carray(hint), T.carray(c))
+        if np.isnan(e):
+            raise MctdhbError(last_error())
+        return e, c
+
+    def propagate_coef_sil(self, mc, hob, hint, c, m, dt, imagtime):
+        """Builds the parts of an MCTDHBDataStruct propagate_coef_sil reads
+        (coefficients_integration.c:59-160) and runs one SIL step.
+        Returns (cnext, state_coef, decomp_diag, decomp_offd)."""
+        M = mc.contents.norb
+        nc = mc.contents.dim
+        keep = []
+        coef = np.ascontiguousarray(c, np.complex128).copy()
+        hintv = np.ascontiguousarray(hint, np.complex128).reshape(-1).copy()
+        H = T.RowMatrix(hob)
+        st = T.ManyBodyStateS()
+        st.npar, st.norb, st.space_dim = mc.contents.npar, M, nc
+        st.coef, st.hint, st.hob = T.carray(coef), T.carray(hintv), H.ptr
+        eq = T.OrbitalEquationS()
+        eq.tstep = dt
+        eq.prop_dt = T.dcomplex.of(-1j * dt if imagtime else dt)
+        eq.time_fac = T.dcomplex.of(-1j if imagtime else 1.0)
+        lw = T.WorkspaceLanczosS()
+        lw.iter, lw.space_dim = m, nc
+        ddiag = np.zeros(m, np.complex128)
+        doffd = np.zeros(m, np.complex128)
+        lw.decomp_diag, lw.decomp_offd = T.carray(ddiag), T.carray(doffd)
+        cw = T.CoefWorkspaceS()
+        cw.lan_work = C.pointer(lw)
+        ms = T.MCTDHBDataStructS()
+        ms.integ_type = T.IMAGTIME if imagtime else T.REALTIME
+        ms.coef_integ_method = T.LANCZOS
+        ms.multiconfig_space = mc
+        ms.orb_eq = C.pointer(eq)
+        ms.coef_workspace = C.pointer(cw)
+        ms.state = C.pointer(st)
+        keep += [H, st, eq, lw, cw]
+        cnext = np.zeros(nc, np.complex128)
+        self.lib.mctdhb_gpu_clear_error()
+        self.lib.propagate_coef_sil(C.pointer(ms), T.carray(cnext))
+        if last_error():
+            raise MctdhbError(last_error())
+        return cnext, coef, ddiag, doffd

@@ -1,0 +1,156 @@
+/* mctdhb_gpu.h -- C ABI of libmctdhb_b200.so.
+ *
+ * Part 1 re-exports the reference's own entry points for the configurational
+ * path under the same names and signatures (host pointers, reference struct
+ * layout from mctdhb_types.h), so a program linked against the reference's
+ * libmctdhb can link against this library instead.  Each declaration cites
+ * the reference declaration it replaces (paths relative to the reference
+ * project root, andriati-alex/1d-mctdhb).
+ *
+ * Differences of behaviour, all deliberate:
+ *   - no exit(): failures are recorded and readable with
+ *     mctdhb_gpu_last_error(); functions returning pointers return NULL,
+ *     `lanczos` returns -1, void functions leave outputs untouched;
+ *   - the index tables of a MultiConfiguration are optional: the GPU path
+ *     ranks configurations on the fly, and get_multiconf_struct only builds
+ *     the double-jump tables when they fit the reference's 32-bit layout
+ *     (it leaves maptt / mapot and their strides NULL otherwise, where the
+ *     reference would exit);
+ *   - propagate_coef_sil leaves the Lanczos vectors on the device: the
+ *     WorkspaceLanczos vectors are not written back (decomposition
+ *     coefficients are).
+ *
+ * Part 2 is a device-resident API: Fock-space handles and operations on
+ * device pointers with an explicit CUDA stream (passed as void*), used for
+ * throughput work where coefficients, orbitals and matrices stay in HBM.
+ */
+#ifndef MCTDHB_B200_GPU_H
+#define MCTDHB_B200_GPU_H
+
+#include "mctdhb_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* errors                                                                  */
+/* ---------------------------------------------------------------------- */
+/* Message of the last failure on the calling thread ("" if none). */
+const char* mctdhb_gpu_last_error(void);
+void        mctdhb_gpu_clear_error(void);
+
+/* ---------------------------------------------------------------------- */
+/* Part 1: drop-in replacements (host memory)                              */
+/* ---------------------------------------------------------------------- */
+/* include/configurational/space.h:23 (space.c:85) */
+uint32_t space_dimension(uint16_t npar, uint16_t norb);
+/* space.h:37 (space.c:120) -- malloc'd, caller frees */
+uint32_t* get_subspaces_dim(uint16_t npar, uint16_t norb);
+/* space.h:54 (space.c:138) */
+void set_config(uint32_t hash_i, uint16_t npar, uint16_t norb, uint16_t* conf);
+/* space.h:71 (space.c:159) */
+uint32_t hash_index(uint16_t npar, uint16_t norb, uint32_t* subsdim, uint16_t* conf);
+/* space.h:41 (space.c:181) -- built on the GPU, malloc'd */
+uint16_t* get_hash_table(uint16_t npar, uint16_t norb);
+/* space.h:88 (space.c:202) -- built on the GPU, malloc'd */
+uint32_t* get_single_jump_map(uint16_t npar, uint16_t norb, uint32_t* subsdim,
+                              uint16_t* hash_table);
+/* space.h:149 (space.c:297) -- strides: dim entries; NULL when the table
+ * exceeds 32-bit indexing (the reference exits there) */
+uint32_t* get_double_diffjump_map(uint16_t npar, uint16_t norb, uint32_t* subsdim,
+                                  uint16_t* hash_table, uint32_t* strides);
+/* space.h:186 (space.c:399) */
+uint32_t* get_double_equaljump_map(uint16_t npar, uint16_t norb, uint32_t* subsdim,
+                                   uint16_t* hash_table, uint32_t* strides);
+/* include/assistant/types_definition.h:43 (types_definition.c:111) */
+MultiConfiguration get_multiconf_struct(uint16_t npar, uint16_t norb);
+/* types_definition.h:98 (types_definition.c:348) */
+void destroy_multiconf_struct(MultiConfiguration multiconf);
+
+/* include/configurational/hamiltonian.h:8 (hamiltonian.c:7) */
+void apply_hamiltonian(MultiConfiguration multiconf, Carray coef, Cmatrix hob, Carray hint,
+                       Carray hcoef);
+/* include/configurational/density_matrices.h:8 (density_matrices.c:9) */
+void set_onebody_dm(MultiConfiguration multiconf, Carray coef, Cmatrix rho);
+/* density_matrices.h:12 (density_matrices.c:55) */
+void set_twobody_dm(MultiConfiguration multiconf, Carray coef, Carray rho);
+
+/* include/linalg/multiconfig_lanczos.h:32 (multiconfig_lanczos.c:12) */
+int lanczos(MultiConfiguration multiconf, Cmatrix Ho, Carray Hint, int lm, Carray diag,
+            Carray offdiag, Cmatrix lvec);
+/* multiconfig_lanczos.h:58 (multiconfig_lanczos.c:93) */
+double lowest_state_lanczos(uint16_t niter, MultiConfiguration multiconf, Cmatrix Ho,
+                            Carray Hint, Carray C);
+/* include/integrator/coefficients_integration.h:26 (coefficients_integration.c:59) */
+void propagate_coef_sil(MCTDHBDataStruct mctdhb, Carray cnext);
+
+/* include/integrator/synchronize.h:49 (synchronize.c:42): rho1, rho2 on the
+ * GPU in one pass; regularisation and rho1^{-1} (M x M) on the host */
+void sync_density_matrices(MultiConfiguration mc_space, ManyBodyState psi);
+/* synchronize.h:37 (synchronize.c:12), name as spelled by the reference */
+void set_regulatization_factor(double reg_fac);
+/* synchronize.h:41 (synchronize.c:28) */
+double get_current_regularization_factor(void);
+
+/* include/assistant/integrator_monitor.h:53 (integrator_monitor.c:56) */
+dcomplex total_energy(ManyBodyState psi);
+/* integrator_monitor.h:26 (integrator_monitor.c:10) */
+double eig_residual(MultiConfiguration multiconf, Carray c, Cmatrix hob, Carray hint, double e);
+
+/* ---------------------------------------------------------------------- */
+/* Part 2: device-resident API                                             */
+/* ---------------------------------------------------------------------- */
+/* Layouts: coefficients are complex128 (interleaved re, im) of length dim;
+ * hob is M x M row-major; hint and rho2 are M^4 with element (a,b,c,d) at
+ * a + b M + c M^2 + d M^3 (the reference's layout); rho1 is M x M
+ * row-major.  `stream` is a cudaStream_t (NULL = legacy default stream).
+ * All functions return 0 on success and -1 on failure. */
+typedef struct mctdhb_space_s* mctdhb_space;
+
+int      mctdhb_space_create(uint16_t npar, uint16_t norb, mctdhb_space* out);
+void     mctdhb_space_destroy(mctdhb_space sp);
+uint32_t mctdhb_space_dim(mctdhb_space sp);
+
+/* Pack h_kl and g_ksql into the coefficient table used by H.C (call after
+ * each change of the orbital matrices). */
+int mctdhb_dev_set_matrices(mctdhb_space sp, const void* d_hob, const void* d_hint,
+                            void* stream);
+/* HC = H C with the matrices of the last mctdhb_dev_set_matrices. */
+int mctdhb_dev_apply_hamiltonian(mctdhb_space sp, const void* d_coef, void* d_hc,
+                                 void* stream);
+/* rho1 and rho2 of C in one pass. */
+int mctdhb_dev_density_matrices(mctdhb_space sp, const void* d_coef, void* d_rho1,
+                                void* d_rho2, void* stream);
+/* One short-iterative-Lanczos step of C in place with `lanczos_iter`
+ * vectors (2..15 as in the reference, up to 64 accepted); real time when
+ * imagtime == 0, imaginary time (and renormalisation) otherwise. */
+int mctdhb_dev_sil_step(mctdhb_space sp, void* d_coef, int lanczos_iter, double dt,
+                        int imagtime, void* stream);
+/* One configurational step -- the SIL step of C followed by rho1 and rho2
+ * of the new C -- captured once into a CUDA graph on fixed device buffers
+ * and replayed with one launch.  The matrices are read at replay time, so
+ * mctdhb_dev_set_matrices between replays takes effect. */
+typedef struct mctdhb_step_s* mctdhb_step;
+int  mctdhb_step_create(mctdhb_space sp, void* d_coef, void* d_rho1, void* d_rho2,
+                        int lanczos_iter, double dt, int imagtime, mctdhb_step* out);
+int  mctdhb_step_launch(mctdhb_step st, void* stream);
+int  mctdhb_step_kernel_count(mctdhb_step st); /* kernels launched per replay */
+void mctdhb_step_destroy(mctdhb_step st);
+
+/* Index tables on the device, bit-exact with the reference's: hash table
+ * (dim x M uint16), single-jump map (M^2 dim uint32). */
+int mctdhb_dev_hash_table(mctdhb_space sp, void* d_ht, void* stream);
+int mctdhb_dev_single_jump_map(mctdhb_space sp, void* d_map, void* stream);
+/* Double-jump tables: chunk counts first (total chunks to *n_chunks, host),
+ * then the table (n_chunks M^2 uint32) with 64-bit strides (dim uint64,
+ * in units of table entries).  diff = 1: two different orbitals
+ * (maptt/stridett), diff = 0: one orbital twice (mapot/strideot). */
+int mctdhb_dev_double_jump_chunks(mctdhb_space sp, int diff, uint64_t* n_chunks);
+int mctdhb_dev_double_jump_map(mctdhb_space sp, int diff, void* d_strides, void* d_map,
+                               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,295 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle (itself
+pinned to the reference) and the reference's golden vectors.
+
+Tolerances (from the stated accuracy targets): index tables bit-exact;
+H.C, rho1, rho2 within 1e-12 relative (max-norm over the max-norm of the
+oracle); Lanczos / SIL outputs within 1e-10.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from helpers import phys_hint, rand_coef, rand_hint, rand_hob, rel_err
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_*.npz")))
+TOL = 1e-12
+
+
+def dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    import torch
+
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+@pytest.fixture(params=GOLDEN, ids=[os.path.basename(p)[4:-4] for p in GOLDEN])
+def gold(request):
+    return dict(np.load(request.param))
+
+
+# ---------------------------------------------------------------------------
+# index tables
+# ---------------------------------------------------------------------------
+def test_tables_vs_golden(gpu, gold):
+    import torch
+
+    N, M = int(gold["npar"]), int(gold["norb"])
+    sp = gpu.Space(N, M)
+    ht = torch.empty(sp.dim * M, dtype=torch.int16, device="cuda")
+    sp.hash_table(ht)
+    assert np.array_equal(host(ht).view(np.uint16), gold["hash_table"])
+    mp = torch.empty(sp.dim * M * M, dtype=torch.int32, device="cuda")
+    sp.single_jump_map(mp)
+    assert np.array_equal(host(mp).view(np.uint32), gold["map"])
+    for diff, key, skey in ((1, "maptt", "stridett"), (0, "mapot", "strideot")):
+        n = sp.double_jump_chunks(diff)
+        st = torch.empty(sp.dim + 1, dtype=torch.int64, device="cuda")
+        m = torch.empty(max(n * M * M, 1), dtype=torch.int32, device="cuda")
+        sp.double_jump_map(diff, st, m)
+        assert np.array_equal(host(m).view(np.uint32)[: n * M * M], gold[key])
+        assert np.array_equal(host(st)[: sp.dim].astype(np.uint32), gold[skey])
+
+
+@pytest.mark.parametrize("N,M", [(30, 6), (40, 4), (12, 8), (5, 11)])
+def test_tables_vs_oracle(gpu, oracle, N, M):
+    import torch
+
+    sp = gpu.Space(N, M)
+    ht = torch.empty(sp.dim * M, dtype=torch.int16, device="cuda")
+    sp.hash_table(ht)
+    assert np.array_equal(host(ht).view(np.uint16), oracle.hash_table(N, M))
+    mp = torch.empty(sp.dim * M * M, dtype=torch.int32, device="cuda")
+    sp.single_jump_map(mp)
+    assert np.array_equal(host(mp).view(np.uint32), oracle.single_jump_map(N, M))
+    st_o, m_o = oracle.double_diffjump_map(N, M)
+    n = sp.double_jump_chunks(1)
+    st = torch.empty(sp.dim + 1, dtype=torch.int64, device="cuda")
+    m = torch.empty(max(n * M * M, 1), dtype=torch.int32, device="cuda")
+    sp.double_jump_map(1, st, m)
+    assert np.array_equal(host(m).view(np.uint32)[: n * M * M], m_o)
+    assert np.array_equal(host(st)[: sp.dim].view(np.uint64), st_o)
+
+
+def test_dropin_multiconf_struct(gpu, gold):
+    import mctdhb_types as T
+
+    N, M = int(gold["npar"]), int(gold["norb"])
+    D = gpu.DropIn()
+    mc = D.multiconf(N, M)
+    try:
+        s = mc.contents
+        assert s.dim == len(gold["coef"])
+        assert np.array_equal(T.uint_array_to_numpy(s.hash_table, s.dim * M, np.uint16),
+                              gold["hash_table"])
+        om = s.op_maps.contents
+        assert np.array_equal(T.uint_array_to_numpy(om.map, s.dim * M * M, np.uint32), gold["map"])
+        assert np.array_equal(T.uint_array_to_numpy(om.stridett, s.dim, np.uint32),
+                              gold["stridett"])
+        n = len(gold["maptt"])
+        if n:
+            assert np.array_equal(T.uint_array_to_numpy(om.maptt, n, np.uint32), gold["maptt"])
+    finally:
+        D.destroy(mc)
+
+
+# ---------------------------------------------------------------------------
+# H.C
+# ---------------------------------------------------------------------------
+HC_SIZES = [(10, 4), (2, 2), (6, 1), (1, 5), (25, 3), (16, 5), (14, 6), (9, 7), (8, 8),
+            (30, 6), (4, 9), (3, 12)]
+
+
+@pytest.mark.parametrize("N,M", HC_SIZES)
+def test_hc_vs_oracle(gpu, oracle, N, M):
+    import torch
+
+    rng = np.random.default_rng(1000 + 37 * N + M)
+    sp = gpu.Space(N, M)
+    nc = sp.dim
+    c, h, g = rand_coef(rng, nc), rand_hob(rng, M), rand_hint(rng, M)
+    sp.set_matrices(dev(h), dev(g))
+    out = torch.empty(nc, dtype=torch.complex128, device="cuda")
+    sp.apply_hamiltonian(dev(c), out)
+    ref = oracle.apply_hamiltonian(N, M, c, h, g)
+    assert rel_err(host(out), ref) < TOL
+
+
+def test_hc_dropin_vs_golden(gpu, gold):
+    N, M = int(gold["npar"]), int(gold["norb"])
+    D = gpu.DropIn()
+    mc = D.multiconf(N, M)
+    try:
+        for gk, hk in (("hint", "hc"), ("hint_phys", "hc_phys")):
+            got = D.apply_hamiltonian(mc, gold["coef"], gold["hob"], gold[gk])
+            assert rel_err(got, gold[hk]) < TOL
+    finally:
+        D.destroy(mc)
+
+
+# ---------------------------------------------------------------------------
+# density matrices
+# ---------------------------------------------------------------------------
+DENS_SIZES = [(10, 4), (2, 2), (6, 1), (25, 3), (16, 5), (14, 6), (9, 7), (8, 8), (30, 6),
+              (4, 9)]
+
+
+@pytest.mark.parametrize("N,M", DENS_SIZES)
+def test_density_vs_oracle(gpu, oracle, N, M):
+    import torch
+
+    rng = np.random.default_rng(2000 + 37 * N + M)
+    sp = gpu.Space(N, M)
+    c = rand_coef(rng, sp.dim)
+    r1 = torch.empty(M * M, dtype=torch.complex128, device="cuda")
+    r2 = torch.empty(M ** 4, dtype=torch.complex128, device="cuda")
+    sp.density_matrices(dev(c), r1, r2)
+    assert rel_err(host(r1).reshape(M, M), oracle.onebody_dm(N, M, c)) < TOL
+    assert rel_err(host(r2), oracle.twobody_dm(N, M, c)) < TOL
+
+
+def test_density_dropin_vs_golden(gpu, gold):
+    N, M = int(gold["npar"]), int(gold["norb"])
+    D = gpu.DropIn()
+    mc = D.multiconf(N, M)
+    try:
+        assert rel_err(D.onebody_dm(mc, gold["coef"]), gold["rho1"]) < TOL
+        assert rel_err(D.twobody_dm(mc, gold["coef"]), gold["rho2"]) < TOL
+    finally:
+        D.destroy(mc)
+
+
+def test_density_deterministic(gpu):
+    """same input, same bits (fixed-order reductions)"""
+    import torch
+
+    rng = np.random.default_rng(7)
+    sp = gpu.Space(20, 6)
+    c = dev(rand_coef(rng, sp.dim))
+    outs = []
+    for _ in range(3):
+        r1 = torch.empty(36, dtype=torch.complex128, device="cuda")
+        r2 = torch.empty(6 ** 4, dtype=torch.complex128, device="cuda")
+        sp.density_matrices(c, r1, r2)
+        outs.append((host(r1), host(r2)))
+    for a, b in outs[1:]:
+        assert np.array_equal(a, outs[0][0]) and np.array_equal(b, outs[0][1])
+
+
+# ---------------------------------------------------------------------------
+# Lanczos / SIL
+# ---------------------------------------------------------------------------
+def test_lanczos_dropin_vs_golden(gpu, gold):
+    N, M, m = int(gold["npar"]), int(gold["norb"]), int(gold["m"])
+    D = gpu.DropIn()
+    mc = D.multiconf(N, M)
+    try:
+        it, diag, offd, lv = D.lanczos(mc, gold["hob"], gold["hint_phys"], m, gold["coef"])
+        assert it == int(gold["lanczos_iters"])
+        assert rel_err(diag[:it], gold["lanczos_diag"]) < 1e-10
+        assert rel_err(offd[: it - 1], gold["lanczos_offd"]) < 1e-10
+        assert rel_err(lv[:it], gold["lanczos_vecs"]) < 1e-9
+    finally:
+        D.destroy(mc)
+
+
+def test_lowest_state_dropin_vs_golden(gpu, gold):
+    N, M = int(gold["npar"]), int(gold["norb"])
+    D = gpu.DropIn()
+    mc = D.multiconf(N, M)
+    try:
+        e, c = D.lowest_state_lanczos(mc, gold["hob"], gold["hint_phys"], int(gold["lowest_m"]),
+                                      gold["coef"])
+        e0 = float(gold["lowest_e"])
+        assert abs(e - e0) < 1e-10 * abs(e0)
+        ph = np.vdot(c, gold["lowest_c"])
+        ph /= abs(ph)
+        assert rel_err(c * ph, gold["lowest_c"]) < 1e-8
+    finally:
+        D.destroy(mc)
+
+
+@pytest.mark.parametrize("N,M,m,imag", [(10, 4, 5, True), (10, 4, 5, False), (14, 6, 6, False),
+                                        (8, 8, 6, True), (30, 6, 6, False), (4, 9, 4, True)])
+def test_sil_step_vs_oracle(gpu, oracle, N, M, m, imag):
+    rng = np.random.default_rng(3000 + N * 7 + M)
+    sp = gpu.Space(N, M)
+    c, h, g = rand_coef(rng, sp.dim), rand_hob(rng, M), phys_hint(rng, M)
+    h = h * 0.1
+    g = g * (0.05 / np.abs(g).max())
+    dt = 0.01
+    sp.set_matrices(dev(h), dev(g))
+    cd = dev(c)
+    sp.sil_step(cd, m, dt, imag)
+    it, ref = oracle.sil_step(N, M, h, g, m, dt, imag, c)
+    assert rel_err(host(cd), ref) < 1e-10
+    assert abs(np.linalg.norm(host(cd)) - 1) < 1e-12
+
+
+def test_propagate_coef_sil_dropin(gpu, oracle):
+    rng = np.random.default_rng(77)
+    N, M, m = 10, 4, 5
+    D = gpu.DropIn()
+    mc = D.multiconf(N, M)
+    try:
+        c, h, g = rand_coef(rng, mc.contents.dim), rand_hob(rng, M), phys_hint(rng, M)
+        g = g * (0.1 / np.abs(g).max())
+        for imag in (True, False):
+            cnext, coef, dd, od = D.propagate_coef_sil(mc, h, g, c, m, 0.01, imag)
+            it, ref = oracle.sil_step(N, M, h, g, m, 0.01, imag, c)
+            assert rel_err(coef, ref) < 1e-10
+            if imag:  # cnext is the combination before renormalisation
+                assert rel_err(cnext / np.linalg.norm(cnext), ref) < 1e-10
+            oit, odiag, ooffd, _ = oracle.lanczos(N, M, h, g, m, c)
+            assert rel_err(dd[:oit], odiag[:oit]) < 1e-10
+    finally:
+        D.destroy(mc)
+
+
+# ---------------------------------------------------------------------------
+# full size (N=30, M=8): size-independent properties + sampled rows
+# ---------------------------------------------------------------------------
+def test_hc_large_properties(gpu, oracle):
+    import torch
+
+    N, M = 30, 8
+    rng = np.random.default_rng(99)
+    sp = gpu.Space(N, M)
+    nc = sp.dim
+    assert nc == 10295472
+    h, g = rand_hob(rng, M), phys_hint(rng, M)
+    sp.set_matrices(dev(h), dev(g))
+    u = torch.randn(nc, dtype=torch.complex128, device="cuda", generator=None)
+    u /= torch.linalg.vector_norm(u)
+    v = torch.randn(nc, dtype=torch.complex128, device="cuda")
+    v /= torch.linalg.vector_norm(v)
+    hu = torch.empty_like(u)
+    hv = torch.empty_like(v)
+    sp.apply_hamiltonian(u, hu)
+    sp.apply_hamiltonian(v, hv)
+    # hermiticity: <u|Hv> = conj <v|Hu>
+    a = torch.vdot(u, hv).item()
+    b = torch.vdot(v, hu).item()
+    assert abs(a - np.conj(b)) < 1e-11 * max(abs(a), 1.0)
+    # energy identity <u|Hu> = Tr(rho1 h) + 1/2 sum rho2 g
+    r1 = torch.empty(M * M, dtype=torch.complex128, device="cuda")
+    r2 = torch.empty(M ** 4, dtype=torch.complex128, device="cuda")
+    sp.density_matrices(u, r1, r2)
+    e1 = torch.vdot(u, hu).item()
+    e2 = oracle.total_energy(M, host(r1).reshape(M, M), host(r2), h, g)
+    assert abs(e1 - e2) < 1e-11 * abs(e1)
+    # rows sampled across the space against the oracle's rows
+    un = host(u)
+    hun = host(hu)
+    for r0 in (0, nc // 3, nc // 2 + 12345, nc - 2000):
+        ref = oracle.apply_hamiltonian(N, M, un, h, g, rows=(r0, r0 + 2000))
+        assert rel_err(hun[r0:r0 + 2000], ref[r0:r0 + 2000]) < TOL
