@@ -148,9 +148,18 @@ int mctdhb_step_create(mctdhb_space h, void* d_coef, void* d_rho1, void* d_rho2,
     *out = nullptr;
     std::lock_guard<std::mutex> lk(h->mu);
     if (ensure_lanczos(h, m)) return -1;
-    if (dens_prepare(h->sp.view)) return -1;
     cudaStream_t cs;
     MCTDHB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    {
+        // pick the launch variants now: a capture cannot time launches
+        HcEpilogue ep;
+        hc_variant(h->sp.view, (const double2*)d_coef, h->lw.out, h->sp.d_tab, ep, cs);
+        if (dens_prepare(h->sp.view, (const double2*)d_coef, h->sp.d_dens_part, cs)) {
+            cudaStreamDestroy(cs);
+            return -1;
+        }
+        MCTDHB_CUDA_TRY(cudaStreamSynchronize(cs));
+    }
     auto* s = new mctdhb_step_s();
     const double2 pdt = imagtime ? make_double2(0.0, -dt) : make_double2(dt, 0.0);
     int rc = 0;

@@ -1,5 +1,6 @@
 // density-matrix kernel instantiation for 6 orbitals (own translation unit)
 #include "dens_tmpl.cuh"
 namespace mctdhb {
-template int dens_launch_tmpl<6>(const SpaceView&, const double2*, double2*, int, cudaStream_t);
+template int dens_launch_tmpl<6>(const SpaceView&, const double2*, double2*, int, int,
+                                  cudaStream_t);
 }

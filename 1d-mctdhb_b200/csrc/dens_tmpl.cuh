@@ -47,20 +47,27 @@ __device__ __forceinline__ void flush8(double2 (&v)[8], double2* acc, int lane) 
     }
 }
 
-template <int M>
-__global__ void __launch_bounds__(128)
+// Rows are dealt to blocks of DENS_BLOCK threads in a block-uniform loop, so
+// SYNC > 0 can put a block barrier every SYNC elements (the warps then walk
+// the unrolled code together and share instruction-cache lines, as in the
+// H.C kernel).  The barrier changes no arithmetic: every SYNC variant sums
+// in the same order and gives the same bits.
+constexpr int DENS_BLOCK = 128;
+
+template <int M, int SYNC>
+__global__ void __launch_bounds__(DENS_BLOCK)
     dens_kernel(SpaceView sp, const double2* __restrict__ C, double2* __restrict__ partial) {
     constexpr int E = dens_nelem(M);
     constexpr int EP = (E + 7) / 8 * 8;
     extern __shared__ double2 sacc[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = DENS_BLOCK >> 5;
     double2* wacc = sacc + warp * EP;
     for (int i = lane; i < EP; i += 32) wacc[i] = make_double2(0.0, 0.0);
     __syncwarp();
 
-    const uint32_t twarps = gridDim.x * nwarps;
-    for (uint32_t base = (blockIdx.x * nwarps + warp) * 32u; base < sp.dim; base += twarps * 32u) {
-        const uint32_t row = base + lane;
+    for (uint32_t bbase = blockIdx.x * DENS_BLOCK; bbase < sp.dim;
+         bbase += gridDim.x * DENS_BLOCK) {
+        const uint32_t row = bbase + threadIdx.x;
         const bool live = row < sp.dim;
         RowState<M> st;
         double2 ci = make_double2(0.0, 0.0);
@@ -132,10 +139,11 @@ __global__ void __launch_bounds__(128)
             }
             v[e % 8] = x;
             if constexpr (e % 8 == 7) flush8(v, wacc + (e / 8) * 8, lane);
+            if constexpr (SYNC > 0 && e % SYNC == SYNC - 1) __syncthreads();
         });
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < EP; e += blockDim.x) {
+    for (int e = threadIdx.x; e < EP; e += DENS_BLOCK) {
         double2 s = sacc[e];
         for (int w = 1; w < nwarps; w++) {
             s.x += sacc[w * EP + e].x;
@@ -145,22 +153,34 @@ __global__ void __launch_bounds__(128)
     }
 }
 
-template <int M>
-int dens_launch_tmpl(const SpaceView& sp, const double2* C, double2* partial, int grid,
-                     cudaStream_t st) {
+template <int M, int SYNC>
+int dens_launch_variant(const SpaceView& sp, const double2* C, double2* partial, int grid,
+                        cudaStream_t st) {
     constexpr int EP = (dens_nelem(M) + 7) / 8 * 8;
-    const size_t smem = (size_t)4 * EP * sizeof(double2);
+    const size_t smem = (size_t)(DENS_BLOCK / 32) * EP * sizeof(double2);
     static bool attr = false;
     if (!attr) {
-        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(dens_kernel<M>,
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(dens_kernel<M, SYNC>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem));
         attr = true;
     }
     if (grid == 0) return 0;  // attribute only (before graph capture)
-    dens_kernel<M><<<grid, 128, smem, st>>>(sp, C, partial);
+    dens_kernel<M, SYNC><<<grid, DENS_BLOCK, smem, st>>>(sp, C, partial);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
+}
+
+// kDensVariants (kernels.h) barrier intervals; variant 0 is the default
+template <int M>
+int dens_launch_tmpl(const SpaceView& sp, const double2* C, double2* partial, int grid,
+                     int variant, cudaStream_t st) {
+    switch (variant) {
+        case 1: return dens_launch_variant<M, 32>(sp, C, partial, grid, st);
+        case 2: return dens_launch_variant<M, 128>(sp, C, partial, grid, st);
+        case 3: return dens_launch_variant<M, 0>(sp, C, partial, grid, st);
+        default: return dens_launch_variant<M, 64>(sp, C, partial, grid, st);
+    }
 }
 
 }  // namespace mctdhb

@@ -205,17 +205,50 @@ size_t dens_partial_elems(const SpaceView& sp) {
     return (size_t)dens_slices(sp) * dens_ep(sp.M);
 }
 
-int dens_prepare(const SpaceView& sp) {
+static int dens_launch_v(const SpaceView& sp, const double2* C, double2* partial, int grid,
+                         int v, cudaStream_t st) {
     switch (sp.M) {
-        case 2: return dens_launch_tmpl<2>(sp, nullptr, nullptr, 0, 0);
-        case 3: return dens_launch_tmpl<3>(sp, nullptr, nullptr, 0, 0);
-        case 4: return dens_launch_tmpl<4>(sp, nullptr, nullptr, 0, 0);
-        case 5: return dens_launch_tmpl<5>(sp, nullptr, nullptr, 0, 0);
-        case 6: return dens_launch_tmpl<6>(sp, nullptr, nullptr, 0, 0);
-        case 7: return dens_launch_tmpl<7>(sp, nullptr, nullptr, 0, 0);
-        case 8: return dens_launch_tmpl<8>(sp, nullptr, nullptr, 0, 0);
-        default: return 0;
+        case 2: return dens_launch_tmpl<2>(sp, C, partial, grid, v, st);
+        case 3: return dens_launch_tmpl<3>(sp, C, partial, grid, v, st);
+        case 4: return dens_launch_tmpl<4>(sp, C, partial, grid, v, st);
+        case 5: return dens_launch_tmpl<5>(sp, C, partial, grid, v, st);
+        case 6: return dens_launch_tmpl<6>(sp, C, partial, grid, v, st);
+        case 7: return dens_launch_tmpl<7>(sp, C, partial, grid, v, st);
+        case 8: return dens_launch_tmpl<8>(sp, C, partial, grid, v, st);
+        default:
+            dens_generic_kernel<<<grid, 128, 0, st>>>(sp, C, partial, dens_ep(sp.M));
+            MCTDHB_CUDA_TRY(cudaGetLastError());
+            return 0;
     }
+}
+
+// the variants differ only in the barrier interval (dens_tmpl.cuh): same
+// blocks, same row order, same sums -- the tuner changes speed, not bits
+namespace {
+struct DensTuneCtx {
+    const SpaceView* sp;
+    const double2* C;
+    double2* partial;
+    int grid;
+};
+int dens_tune_launch(void* p, int v, cudaStream_t st) {
+    auto* c = (DensTuneCtx*)p;
+    return dens_launch_v(*c->sp, c->C, c->partial, c->grid, v, st);
+}
+int dens_variant(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st) {
+    if (!dens_templated(sp.M) || sp.dim < 4096) return 0;
+    DensTuneCtx ctx{&sp, C, partial, dens_grid(sp)};
+    return tune_pick("dens", sp.N, sp.M, kDensVariants, st, dens_tune_launch, &ctx);
+}
+}  // namespace
+
+int dens_prepare(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st) {
+    if (!dens_templated(sp.M)) return 0;
+    for (int v = 0; v < kDensVariants; v++)
+        if (dens_launch_v(sp, nullptr, nullptr, 0, v, st)) return -1;  // attributes only
+    dens_variant(sp, C, partial, st);
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(st));
+    return 0;
 }
 
 int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
@@ -223,20 +256,8 @@ int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2*
     const int grid = dens_grid(sp);
     const int M = sp.M;
     const int EP = dens_ep(M);
-    int rc = 0;
-    switch (M) {
-        case 2: rc = dens_launch_tmpl<2>(sp, C, partial, grid, st); break;
-        case 3: rc = dens_launch_tmpl<3>(sp, C, partial, grid, st); break;
-        case 4: rc = dens_launch_tmpl<4>(sp, C, partial, grid, st); break;
-        case 5: rc = dens_launch_tmpl<5>(sp, C, partial, grid, st); break;
-        case 6: rc = dens_launch_tmpl<6>(sp, C, partial, grid, st); break;
-        case 7: rc = dens_launch_tmpl<7>(sp, C, partial, grid, st); break;
-        case 8: rc = dens_launch_tmpl<8>(sp, C, partial, grid, st); break;
-        default:
-            dens_generic_kernel<<<grid, 128, 0, st>>>(sp, C, partial, EP);
-            MCTDHB_CUDA_TRY(cudaGetLastError());
-    }
-    if (rc) return rc;
+    const int v = dens_variant(sp, C, partial, st);
+    if (int rc = dens_launch_v(sp, C, partial, grid, v, st)) return rc;
     const int E = dens_nelem(M);
     dens_finalize_kernel<<<(E + 127) / 128, 128, 0, st>>>(M, E, EP, dens_slices(sp), partial,
                                                           d_desc, rho1, rho2);

@@ -18,7 +18,6 @@ struct SpaceCtx {
     uint32_t* d_T = nullptr;
     double* d_sq = nullptr;
     double2* d_tab = nullptr;       // H.C coefficient table (moves.cuh layout)
-    double2* d_hc_part = nullptr;   // per-block <v, Hv> partials
     int* d_dens_desc = nullptr;     // density element descriptors
     double2* d_dens_part = nullptr; // density partial sums
 };

@@ -17,6 +17,12 @@
 //   * for M <= 8 the move loops are fully unrolled so occupations, rank
 //     offsets and sqrt factors stay in registers;  larger M use a generic
 //     runtime-loop kernel.
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "moves.cuh"
@@ -75,7 +81,6 @@ __global__ void __launch_bounds__(128)
     if (ep.flag != nullptr && *ep.flag != 0) return;
     const int M = sp.M, N = sp.N;
     const int ND = hc_ndiag(M), NS = hc_nsingle(M);
-    double2 dot_acc = make_double2(0.0, 0.0);
     for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < sp.dim;
          row += gridDim.x * blockDim.x) {
         int n[kMaxOrb], L[kMaxOrb];
@@ -157,13 +162,11 @@ __global__ void __launch_bounds__(128)
             acc.y -= b * pv.y;
         }
         HC[row] = acc;
-        if (ep.dot_partial != nullptr) dot_acc = cfma_conj(ci, acc, dot_acc);
     }
-    if (ep.dot_partial != nullptr) block_reduce_store(dot_acc, ep.dot_partial);
 }
 
 // ---------------------------------------------------------------------------
-// launchers
+// launchers and autotuner
 // ---------------------------------------------------------------------------
 int hc_prep(int M, const double2* d_hob, const double2* d_hint, double2* d_tab,
             cudaStream_t st) {
@@ -172,33 +175,56 @@ int hc_prep(int M, const double2* d_hob, const double2* d_hint, double2* d_tab,
     return 0;
 }
 
-int hc_grid(const SpaceView& sp) {
-    if (sp.M >= 2 && sp.M <= kMaxTemplOrb) {
-        uint64_t need = ((uint64_t)sp.dim + 255) / 256;
-        uint64_t cap = (uint64_t)num_sms() * 2;
-        return (int)(need < cap ? (need ? need : 1) : cap);
+static bool hc_templated(int M) { return M >= 2 && M <= kMaxTemplOrb; }
+
+static int hc_launch_v(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+                       const HcEpilogue& ep, int v, cudaStream_t st) {
+    switch (sp.M) {
+        case 2: return hc_launch_tmpl<2>(sp, C, HC, tab, ep, v, st);
+        case 3: return hc_launch_tmpl<3>(sp, C, HC, tab, ep, v, st);
+        case 4: return hc_launch_tmpl<4>(sp, C, HC, tab, ep, v, st);
+        case 5: return hc_launch_tmpl<5>(sp, C, HC, tab, ep, v, st);
+        case 6: return hc_launch_tmpl<6>(sp, C, HC, tab, ep, v, st);
+        case 7: return hc_launch_tmpl<7>(sp, C, HC, tab, ep, v, st);
+        case 8: return hc_launch_tmpl<8>(sp, C, HC, tab, ep, v, st);
+        default: {
+            uint64_t need = ((uint64_t)sp.dim + 127) / 128;
+            uint64_t cap = (uint64_t)num_sms() * 8;
+            const int grid = (int)(need < cap ? (need ? need : 1) : cap);
+            hc_generic_kernel<<<grid, 128, 0, st>>>(sp, C, HC, tab, ep);
+            MCTDHB_CUDA_TRY(cudaGetLastError());
+            return 0;
+        }
     }
-    uint64_t need = ((uint64_t)sp.dim + 127) / 128;
-    uint64_t cap = (uint64_t)num_sms() * 8;
-    return (int)(need < cap ? (need ? need : 1) : cap);
+}
+
+// launch variant (block size x barrier interval, hc_tmpl.cuh) chosen by the
+// autotuner (tune.cu) on the caller's own data; small spaces use variant 0
+namespace {
+struct HcTuneCtx {
+    const SpaceView* sp;
+    const double2* C;
+    double2* HC;
+    const double2* tab;
+    const HcEpilogue* ep;
+};
+int hc_tune_launch(void* p, int v, cudaStream_t st) {
+    auto* c = (HcTuneCtx*)p;
+    return hc_launch_v(*c->sp, c->C, c->HC, c->tab, *c->ep, v, st);
+}
+}  // namespace
+
+int hc_variant(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+               const HcEpilogue& ep, cudaStream_t st) {
+    if (!hc_templated(sp.M) || sp.dim < 4096) return 0;
+    HcTuneCtx ctx{&sp, C, HC, tab, &ep};
+    return tune_pick("hc", sp.N, sp.M, kHcVariants, st, hc_tune_launch, &ctx);
 }
 
 int hc_apply(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
              const HcEpilogue& ep, cudaStream_t st) {
-    const int grid = hc_grid(sp);
-    switch (sp.M) {
-        case 2: return hc_launch_tmpl<2>(sp, C, HC, tab, ep, grid, st);
-        case 3: return hc_launch_tmpl<3>(sp, C, HC, tab, ep, grid, st);
-        case 4: return hc_launch_tmpl<4>(sp, C, HC, tab, ep, grid, st);
-        case 5: return hc_launch_tmpl<5>(sp, C, HC, tab, ep, grid, st);
-        case 6: return hc_launch_tmpl<6>(sp, C, HC, tab, ep, grid, st);
-        case 7: return hc_launch_tmpl<7>(sp, C, HC, tab, ep, grid, st);
-        case 8: return hc_launch_tmpl<8>(sp, C, HC, tab, ep, grid, st);
-        default:
-            hc_generic_kernel<<<grid, 128, 0, st>>>(sp, C, HC, tab, ep);
-            MCTDHB_CUDA_TRY(cudaGetLastError());
-            return 0;
-    }
+    const int v = hc_variant(sp, C, HC, tab, ep, st);
+    return hc_launch_v(sp, C, HC, tab, ep, v, st);
 }
 
 }  // namespace mctdhb

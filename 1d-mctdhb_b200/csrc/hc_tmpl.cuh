@@ -2,6 +2,14 @@
 // explicit instantiation per translation unit (hc_m*.cu).  See
 // hamiltonian.cu for the design notes and moves.cuh for the coefficient
 // folding.
+//
+// Instruction supply.  The fully unrolled move list is the lowest
+// instruction count per row (every orbital index, rank offset and table
+// offset is an immediate), but at M = 8 it is ~180 KB of code: warps that
+// drift apart stream different parts of it and stall on instruction fetch.
+// SYNC > 0 puts a block barrier every SYNC moves so the warps of a block
+// walk the code together and share instruction-cache lines; BLOCK and SYNC
+// are picked per (N, M) by the autotuner (hamiltonian.cu).
 #pragma once
 #include "common.cuh"
 #include "kernels.h"
@@ -23,28 +31,41 @@ __device__ __forceinline__ uint32_t jumpc(const RowState<M>& st, uint32_t row) {
 }
 
 template <int M>
-__global__ void __launch_bounds__(256, 2)
+__device__ __forceinline__ void zero_row(RowState<M>& st) {
+    static_for<M>([&](auto mi) { st.n[decltype(mi)::value] = 0; });
+    static_for<(M > 1 ? M - 1 : 1)>([&](auto mi) {
+        constexpr int m = decltype(mi)::value;
+        st.F[m][0] = st.F[m][1] = st.F[m][2] = st.F[m][3] = 0;
+    });
+}
+
+template <int M, int BLOCK, int SYNC>
+__global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     hc_kernel(SpaceView sp, const double2* __restrict__ C, double2* __restrict__ HC,
               const double2* __restrict__ tab_g, HcEpilogue ep) {
     constexpr int TAB = hc_table_size(M);
     constexpr int NMOVE = HcMoveList<M>::N;
     __shared__ double2 tab[TAB];
-    for (int i = threadIdx.x; i < TAB; i += blockDim.x) tab[i] = tab_g[i];
+    for (int i = threadIdx.x; i < TAB; i += BLOCK) tab[i] = tab_g[i];
     __syncthreads();
     if (ep.flag != nullptr && *ep.flag != 0) return;  // Lanczos breakdown: no-op
 
-    double2 dot_acc = make_double2(0.0, 0.0);
-    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < sp.dim;
-         row += gridDim.x * blockDim.x) {
+    // block-uniform trip count: every thread reaches every barrier
+    for (uint32_t base = blockIdx.x * BLOCK; base < sp.dim; base += gridDim.x * BLOCK) {
+        const uint32_t row = base + threadIdx.x;
+        const bool live = row < sp.dim;
         RowState<M> st;
-        load_row<M>(sp, row, st);
+        if (live)
+            load_row<M>(sp, row, st);
+        else
+            zero_row<M>(st);
         double sq0[M], sq1[M];
         static_for<M>([&](auto mi) {
             constexpr int m = decltype(mi)::value;
             sq0[m] = __ldg(sp.sq + st.n[m]);
             sq1[m] = __ldg(sp.sq + st.n[m] + 1);
         });
-        const double2 ci = __ldg(C + row);
+        const double2 ci = live ? __ldg(C + row) : make_double2(0.0, 0.0);
 
         // diagonal: h_kk n_k + 1/2 g_kkkk n_k (n_k - 1) + 2 g_ksks n_k n_s
         double2 dg = make_double2(0.0, 0.0);
@@ -66,7 +87,8 @@ __global__ void __launch_bounds__(256, 2)
         double sa = 0.0;
         double2 as = make_double2(0.0, 0.0);
         static_for<NMOVE>([&](auto ei) {
-            constexpr HcMove mv = kHcMoves<M>.m[decltype(ei)::value];
+            constexpr int e = decltype(ei)::value;
+            constexpr HcMove mv = kHcMoves<M>.m[e];
             constexpr int k = mv.k, s = mv.s, q = mv.q, l = mv.l;
             if constexpr (s < 0) {
                 // single move k -> q
@@ -104,27 +126,43 @@ __global__ void __launch_bounds__(256, 2)
                 }
                 if constexpr (mv.last) acc = cadd(acc, cscale(as, sa));
             }
+            if constexpr (SYNC > 0 && e % SYNC == SYNC - 1) __syncthreads();
         });
 
-        // Lanczos epilogue: out = HC - beta * prev; dot += conj(C) * out
-        if (ep.prev != nullptr) {
+        // Lanczos epilogue: out = HC - beta * prev
+        if (ep.prev != nullptr && live) {
             const double2 pv = __ldg(ep.prev + row);
             const double b = *ep.beta;
             acc.x -= b * pv.x;
             acc.y -= b * pv.y;
         }
-        HC[row] = acc;
-        if (ep.dot_partial != nullptr) dot_acc = cfma_conj(ci, acc, dot_acc);
+        if (live) HC[row] = acc;
     }
-    if (ep.dot_partial != nullptr) block_reduce_store(dot_acc, ep.dot_partial);
 }
 
-template <int M>
-int hc_launch_tmpl(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
-                   const HcEpilogue& ep, int grid, cudaStream_t st) {
-    hc_kernel<M><<<grid, 256, 0, st>>>(sp, C, HC, tab, ep);
+template <int M, int BLOCK, int SYNC>
+int hc_launch_variant(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+                      const HcEpilogue& ep, int blocks_per_sm, cudaStream_t st) {
+    const uint64_t need = ((uint64_t)sp.dim + BLOCK - 1) / BLOCK;
+    const uint64_t cap = (uint64_t)num_sms() * blocks_per_sm;
+    const int grid = (int)(need < cap ? (need ? need : 1) : cap);
+    hc_kernel<M, BLOCK, SYNC><<<grid, BLOCK, 0, st>>>(sp, C, HC, tab, ep);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
+}
+
+// the tuned variants (kHcVariants of them, kernels.h), in autotuner order
+template <int M>
+int hc_launch_tmpl(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+                   const HcEpilogue& ep, int variant, cudaStream_t st) {
+    // variant 0 is the default outside the tuner (best measured at N=30, M=8)
+    switch (variant) {
+        case 1: return hc_launch_variant<M, 512, 32>(sp, C, HC, tab, ep, 1, st);
+        case 2: return hc_launch_variant<M, 512, 128>(sp, C, HC, tab, ep, 1, st);
+        case 3: return hc_launch_variant<M, 256, 32>(sp, C, HC, tab, ep, 2, st);
+        case 4: return hc_launch_variant<M, 256, 0>(sp, C, HC, tab, ep, 2, st);
+        default: return hc_launch_variant<M, 512, 64>(sp, C, HC, tab, ep, 1, st);
+    }
 }
 
 }  // namespace mctdhb

@@ -9,14 +9,13 @@
 namespace mctdhb {
 
 // Optional fused epilogue of the H.C kernel, used by the Lanczos recurrence
-// (multiconfig_lanczos.c:40-41, 78-83): out = H v - beta * prev and the
-// per-block partials of <v, out>.  `flag` != 0 turns the launch into a no-op
-// (a breakdown detected on the device earlier in the same step).
+// (multiconfig_lanczos.c:78-82): out = H v - beta * prev.  `flag` != 0 turns
+// the launch into a no-op (a breakdown detected on the device earlier in the
+// same step).
 struct HcEpilogue {
     const int* flag = nullptr;
     const double2* prev = nullptr;
     const double* beta = nullptr;
-    double2* dot_partial = nullptr;
 };
 
 // Deterministic block reduction of one complex value per thread; thread 0
@@ -44,18 +43,31 @@ __device__ __forceinline__ void block_reduce_store(double2 v, double2* out) {
 }
 
 // per-M register-resident kernels (hc_tmpl.cuh / dens_tmpl.cuh, explicit
-// instantiations in hc_m*.cu / dens_m*.cu)
+// instantiations in hc_m*.cu / dens_m*.cu); H.C has kHcVariants launch
+// variants (block size x barrier interval) chosen by the autotuner
+constexpr int kHcVariants = 5;
+constexpr int kDensVariants = 4;
 template <int M>
 int hc_launch_tmpl(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
-                   const HcEpilogue& ep, int grid, cudaStream_t st);
+                   const HcEpilogue& ep, int variant, cudaStream_t st);
 template <int M>
 int dens_launch_tmpl(const SpaceView& sp, const double2* C, double2* partial, int grid,
-                     cudaStream_t st);
+                     int variant, cudaStream_t st);
+
+// tune.cu: autotuner.  The launch variant of `kernel` for (current device,
+// N, M): the cached choice, else -- outside a stream capture -- each variant
+// is timed on the caller's own data with `launch(v)` and the fastest kept;
+// inside a capture (no timing possible) variant 0.  MCTDHB_TUNE_CACHE names
+// an optional text file persisting choices across processes.
+int tune_pick(const char* kernel, int N, int M, int nvariants, cudaStream_t st,
+              int (*launch)(void* ctx, int v, cudaStream_t st), void* ctx);
+int tune_lookup(const char* kernel, int N, int M);  // -1 when not tuned
 
 // hamiltonian.cu
 int hc_prep(int M, const double2* d_hob, const double2* d_hint, double2* d_tab,
             cudaStream_t st);
-int hc_grid(const SpaceView& sp);
+int hc_variant(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
+               const HcEpilogue& ep, cudaStream_t st);
 int hc_apply(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
              const HcEpilogue& ep, cudaStream_t st);
 
@@ -64,8 +76,9 @@ int dens_grid(const SpaceView& sp);
 size_t dens_partial_elems(const SpaceView& sp);  // doubles2 in the partial buffer
 int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
                double2* rho2, const int* d_desc, cudaStream_t st);
-int dens_descriptors(int M, int* host_desc);
-int dens_prepare(const SpaceView& sp);  // one-time launch attributes  // returns count; desc = 5 ints/elem
+int dens_descriptors(int M, int* host_desc);  // returns count; desc = 5 ints/elem
+// one-time launch attributes and the tuned variant, before any capture
+int dens_prepare(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st);
 
 // space.cu (map kernels)
 int build_hash_table(const SpaceView& sp, uint16_t* d_ht, cudaStream_t st);

@@ -314,8 +314,7 @@ int lanczos_alloc(LanczosWork& w, const SpaceCtx& s, int mmax) {
     w.mmax = mmax;
     w.dim = s.dim;
     w.vec_grid = vec_grid_for(s.dim);
-    const size_t part_elems =
-        std::max<size_t>((size_t)kDotChunk * w.vec_grid, (size_t)hc_grid(s.view));
+    const size_t part_elems = (size_t)kDotChunk * w.vec_grid;
     MCTDHB_CUDA_TRY(cudaMalloc(&w.V, (size_t)mmax * s.dim * sizeof(double2)));
     MCTDHB_CUDA_TRY(cudaMalloc(&w.out, (size_t)s.dim * sizeof(double2)));
     MCTDHB_CUDA_TRY(cudaMalloc(&w.part, part_elems * sizeof(double2)));
@@ -342,13 +341,14 @@ int lanczos_run(const SpaceCtx& s, LanczosWork& w, int m, cudaStream_t st) {
         return -1;
     }
     const uint32_t n = s.dim;
-    const int vg = w.vec_grid, hg = hc_grid(s.view);
+    const int vg = w.vec_grid;
     lz_init_kernel<<<1, 32, 0, st>>>(w.scal, w.iflag, m);
     HcEpilogue ep;
     ep.flag = w.iflag;
-    ep.dot_partial = w.part;
     if (hc_apply(s.view, w.V, w.out, s.d_tab, ep, st)) return -1;
-    if (reduce_rows(w.part, 1, hg, w.scal + S_DIAG, st)) return -1;
+    // a_0 = <v0, H v0>: fixed-geometry reduction, independent of the H.C
+    // launch variant
+    if (vec_dot(w.V, w.out, n, w.part, vg, w.scal + S_DIAG, st)) return -1;
     for (int i = 0; i < m - 1; i++) {
         for (int k0 = 0; k0 <= i; k0 += kDotChunk) {
             const int k1 = std::min(i, k0 + kDotChunk - 1);
@@ -365,10 +365,10 @@ int lanczos_run(const SpaceCtx& s, LanczosWork& w, int m, cudaStream_t st) {
         e2.flag = w.iflag;
         e2.prev = w.V + (size_t)i * n;
         e2.beta = &(w.scal + S_OFFD + i)->x;
-        e2.dot_partial = w.part;
         if (hc_apply(s.view, w.V + (size_t)(i + 1) * n, w.out, s.d_tab, e2, st)) return -1;
-        // a_{i+1}; skipped values are never read (iterations done < i+2)
-        if (reduce_rows(w.part, 1, hg, w.scal + S_DIAG + i + 1, st)) return -1;
+        // a_{i+1}; after a breakdown the value is never read (iterations < i+2)
+        if (vec_dot(w.V + (size_t)(i + 1) * n, w.out, n, w.part, vg, w.scal + S_DIAG + i + 1, st))
+            return -1;
     }
     return 0;
 }

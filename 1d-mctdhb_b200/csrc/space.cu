@@ -65,9 +65,8 @@ int space_init(SpaceCtx& s, int N, int M) {
     s.view.dim = s.dim;
     s.view.T = s.d_T;
     s.view.sq = s.d_sq;
-    // H.C coefficient table + dot partials
+    // H.C coefficient table
     MCTDHB_CUDA_TRY(cudaMalloc(&s.d_tab, (size_t)hc_table_size(M) * sizeof(double2)));
-    MCTDHB_CUDA_TRY(cudaMalloc(&s.d_hc_part, (size_t)hc_grid(s.view) * sizeof(double2)));
     // density descriptors + partials
     const int E = dens_descriptors(M, nullptr);
     std::vector<int> desc((size_t)5 * E);
@@ -83,7 +82,6 @@ void space_release(SpaceCtx& s) {
     cudaFree(s.d_T);
     cudaFree(s.d_sq);
     cudaFree(s.d_tab);
-    cudaFree(s.d_hc_part);
     cudaFree(s.d_dens_desc);
     cudaFree(s.d_dens_part);
     s = SpaceCtx();

@@ -255,6 +255,68 @@ def test_propagate_coef_sil_dropin(gpu, oracle):
         D.destroy(mc)
 
 
+def test_step_graph_matches_calls(gpu, oracle):
+    """the captured step (SIL + rho1/rho2) equals the same calls made one by one"""
+    import torch
+
+    rng = np.random.default_rng(55)
+    N, M, m = 14, 6, 6
+    sp = gpu.Space(N, M)
+    c, h, g = rand_coef(rng, sp.dim), rand_hob(rng, M), phys_hint(rng, M)
+    g = g * (0.05 / np.abs(g).max())
+    sp.set_matrices(dev(h), dev(g))
+    cg = dev(c)
+    r1 = torch.empty(M * M, dtype=torch.complex128, device="cuda")
+    r2 = torch.empty(M ** 4, dtype=torch.complex128, device="cuda")
+    step = gpu.Step(sp, cg, r1, r2, m, 0.01, False)
+    assert step.kernels > 10
+    step.launch()
+    step.launch()
+    cc = dev(c)
+    s1 = torch.empty_like(r1)
+    s2 = torch.empty_like(r2)
+    for _ in range(2):
+        sp.sil_step(cc, m, 0.01, False)
+    sp.density_matrices(cc, s1, s2)
+    assert np.array_equal(host(cg), host(cc))
+    assert np.array_equal(host(r1), host(s1)) and np.array_equal(host(r2), host(s2))
+    _, ref = oracle.sil_step(N, M, h, g, m, 0.01, False, c)
+    _, ref = oracle.sil_step(N, M, h, g, m, 0.01, False, ref)
+    assert rel_err(host(cg), ref) < 1e-10
+    step.close()
+
+
+def test_sync_density_matrices_dropin(gpu, oracle):
+    import ctypes as C
+
+    import mctdhb_types as T
+
+    rng = np.random.default_rng(56)
+    N, M = 12, 5
+    D = gpu.DropIn()
+    mc = D.multiconf(N, M)
+    try:
+        nc = mc.contents.dim
+        c = rand_coef(rng, nc)
+        st = T.ManyBodyStateS()
+        st.npar, st.norb, st.space_dim = N, M, nc
+        coef = np.ascontiguousarray(c)
+        r2 = np.zeros(M ** 4, np.complex128)
+        R1 = T.RowMatrix(np.zeros((M, M), np.complex128))
+        RI = T.RowMatrix(np.zeros((M, M), np.complex128))
+        st.coef, st.tb_denmat, st.ob_denmat, st.inv_ob_denmat = (T.carray(coef), T.carray(r2),
+                                                                 R1.ptr, RI.ptr)
+        D.lib.mctdhb_gpu_clear_error()
+        D.lib.sync_density_matrices(mc, C.pointer(st))
+        assert gpu.last_error() == ""
+        o1, o2, oi = oracle.sync_density_matrices(N, M, c)
+        assert rel_err(R1.a, o1) < TOL and rel_err(r2, o2) < TOL
+        assert rel_err(RI.a, oi) < 1e-10
+        assert np.allclose(RI.a @ R1.a, np.eye(M), atol=1e-10)
+    finally:
+        D.destroy(mc)
+
+
 # ---------------------------------------------------------------------------
 # full size (N=30, M=8): size-independent properties + sampled rows
 # ---------------------------------------------------------------------------
