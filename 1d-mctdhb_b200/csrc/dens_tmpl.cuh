@@ -2,6 +2,8 @@
 // orbitals, one explicit instantiation per translation unit (dens_m*.cu).
 // See density.cu for the design notes.
 #pragma once
+#include <algorithm>
+
 #include "common.cuh"
 #include "hc_tmpl.cuh"
 #include "kernels.h"
@@ -54,8 +56,13 @@ __device__ __forceinline__ void flush8(double2 (&v)[8], double2* acc, int lane) 
 // in the same order and gives the same bits.
 constexpr int DENS_BLOCK = 128;
 
-template <int M, int SYNC>
-__global__ void __launch_bounds__(DENS_BLOCK)
+// The reduction layout is fixed by the grid, which is a function of the space
+// size only (min(888, dim/128) blocks; 888 = 6 x 148 runs in whole waves at
+// two or three resident blocks per SM): block b owns rows
+// b*128 + k*grid*128 + t and one partial slice, so the sums do not depend on
+// the launch variant.
+template <int M, int SYNC, int MINB>
+__global__ void __launch_bounds__(DENS_BLOCK, MINB)
     dens_kernel(SpaceView sp, const double2* __restrict__ C, double2* __restrict__ partial) {
     constexpr int E = dens_nelem(M);
     constexpr int EP = (E + 7) / 8 * 8;
@@ -153,33 +160,34 @@ __global__ void __launch_bounds__(DENS_BLOCK)
     }
 }
 
-template <int M, int SYNC>
+template <int M, int SYNC, int MINB>
 int dens_launch_variant(const SpaceView& sp, const double2* C, double2* partial, int grid,
                         cudaStream_t st) {
     constexpr int EP = (dens_nelem(M) + 7) / 8 * 8;
     const size_t smem = (size_t)(DENS_BLOCK / 32) * EP * sizeof(double2);
     static bool attr = false;
     if (!attr) {
-        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(dens_kernel<M, SYNC>,
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(dens_kernel<M, SYNC, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem));
         attr = true;
     }
-    if (grid == 0) return 0;  // attribute only (before graph capture)
-    dens_kernel<M, SYNC><<<grid, DENS_BLOCK, smem, st>>>(sp, C, partial);
+    if (grid == 0) return 0;  // attributes only (before graph capture)
+    dens_kernel<M, SYNC, MINB><<<grid, DENS_BLOCK, smem, st>>>(sp, C, partial);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
-// kDensVariants (kernels.h) barrier intervals; variant 0 is the default
+// kDensVariants (kernels.h): barrier interval x register budget (MINB
+// resident blocks per SM); variant 0 is the default
 template <int M>
 int dens_launch_tmpl(const SpaceView& sp, const double2* C, double2* partial, int grid,
                      int variant, cudaStream_t st) {
     switch (variant) {
-        case 1: return dens_launch_variant<M, 32>(sp, C, partial, grid, st);
-        case 2: return dens_launch_variant<M, 128>(sp, C, partial, grid, st);
-        case 3: return dens_launch_variant<M, 0>(sp, C, partial, grid, st);
-        default: return dens_launch_variant<M, 64>(sp, C, partial, grid, st);
+        case 1: return dens_launch_variant<M, 32, 0>(sp, C, partial, grid, st);
+        case 2: return dens_launch_variant<M, 64, 3>(sp, C, partial, grid, st);
+        case 3: return dens_launch_variant<M, 128, 0>(sp, C, partial, grid, st);
+        default: return dens_launch_variant<M, 64, 0>(sp, C, partial, grid, st);
     }
 }
 

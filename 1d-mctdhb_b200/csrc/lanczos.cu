@@ -410,6 +410,14 @@ int sil_step(const SpaceCtx& s, LanczosWork& w, double2* d_C, int m, double2 pro
     return 0;
 }
 
+int sil_norm2(const LanczosWork& w, double* out) {
+    double2 v;
+    MCTDHB_CUDA_TRY(cudaDeviceSynchronize());
+    MCTDHB_CUDA_TRY(cudaMemcpy(&v, w.scal + S_MISC + 3, sizeof(v), cudaMemcpyDeviceToHost));
+    *out = v.x;
+    return 0;
+}
+
 int lowest_state(const SpaceCtx& s, LanczosWork& w, double2* d_C, int m, double* d_energy,
                  cudaStream_t st) {
     const uint32_t n = s.dim;

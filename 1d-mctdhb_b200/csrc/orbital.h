@@ -1,0 +1,52 @@
+// orbital.h -- device objects of the orbital side (orbital.cu) and of the
+// full MCTDHB step (solver.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace mctdhb {
+
+// grid, equation coefficients and Simpson weights (device pointers)
+struct OrbView {
+    int M, G, periodic;
+    double dx, a2;  // a2: coefficient of d^2/dx^2 (d2coef), a1: of d/dx (d1coef)
+    double2 a1, tf;  // tf: time factor, 1 (real time) or -i (imaginary time)
+    const double* w;
+    const double* pot;
+};
+
+struct OrbCtx {
+    int M = 0, G = 0;
+    OrbView view{};
+    double* d_w = nullptr;
+    double* d_pot = nullptr;
+    double* d_g = nullptr;         // contact interaction strength (device scalar)
+    double2* d_k[8] = {};          // Runge-Kutta stages + stage input
+    double2* d_H = nullptr;        // H phi
+    double2* d_P = nullptr;        // projector overlaps
+    double2* d_Q = nullptr;        // g rho1^{-1} rho2
+    double2* d_work = nullptr;     // small dense work (rho1 synchronisation)
+};
+
+std::vector<double> simpson_weights(int n, double h);
+int orb_init(OrbCtx& c, int M, int G, double xi, double xf, double a2, double2 a1, int periodic,
+             int imagtime);
+void orb_release(OrbCtx& c);
+int orb_matrices(const OrbCtx& c, const double2* orb, double2* hob, double2* hint,
+                 cudaStream_t st);
+int orb_rhs_eval(const OrbCtx& c, const double2* rinv, const double2* rho2, const double2* y,
+                 double2* out, cudaStream_t st);
+int orb_rk_step(const OrbCtx& c, int order, double dt, const double2* rinv, const double2* rho2,
+                const double2* y, double2* ynext, cudaStream_t st);
+int orb_periodic(const OrbCtx& c, double2* orb, cudaStream_t st);
+int orb_orthonormalize(const OrbCtx& c, double2* orb, cudaStream_t st);
+int orb_sync_rho1(const OrbCtx& c, double2* rho1, double2* rinv, double reg_fac, int* d_info,
+                  cudaStream_t st);
+int orb_energy(int M, const double2* rho1, const double2* rho2, const double2* hob,
+               const double2* hint, double2* E, cudaStream_t st);
+
+}  // namespace mctdhb

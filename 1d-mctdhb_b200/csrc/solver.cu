@@ -1,0 +1,354 @@
+// solver.cu -- one full MCTDHB time step on the device (driver.c:159-201):
+//   orbitals:  Runge-Kutta step of the orbital equation with the current
+//              rho1^{-1} and rho2; Gram-Schmidt in imaginary time
+//   matrices:  h_kl and g_ksql of the new orbitals
+//   coefficients: short-iterative-Lanczos step with the new h, g
+//   densities: rho1, rho2 of the new coefficients; regularised rho1^{-1}
+// Everything stays in HBM; the step is captured once into a CUDA graph and
+// replayed, so a step costs one graph launch and no host round trip.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/mctdhb_gpu.h"
+#include "common.cuh"
+#include "engine.h"
+#include "kernels.h"
+#include "orbital.h"
+
+using namespace mctdhb;
+
+struct mctdhb_solver_s {
+    mctdhb_space sp = nullptr;
+    OrbCtx orb;
+    int N = 0, M = 0, G = 0, imagtime = 0, rk_order = 5, lanczos_m = 5;
+    double dt = 0.0, reg_fac = 1e-9, t = 0.0;
+    double2 *d_orb = nullptr, *d_orb_next = nullptr, *d_coef = nullptr, *d_hob = nullptr,
+            *d_hint = nullptr, *d_rho1 = nullptr, *d_rho2 = nullptr, *d_rinv = nullptr,
+            *d_E = nullptr;
+    int* d_info = nullptr;
+    cudaStream_t cs = nullptr;
+    // phase 0: orbital step; phase 1: matrices, SIL, densities
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int kernels = 0;
+    bool has_state = false;
+    std::mutex mu;
+};
+
+namespace {
+
+// phase 0 (orbital_integration.c:284-349): orbitals advanced with the
+// current rho1^{-1} and rho2
+int phase_orbitals(mctdhb_solver_s* s, cudaStream_t st) {
+    const OrbCtx& o = s->orb;
+    const size_t n = (size_t)s->M * s->G;
+    if (o.view.periodic && orb_periodic(o, s->d_orb, st)) return -1;
+    if (orb_rk_step(o, s->rk_order, s->dt, s->d_rinv, s->d_rho2, s->d_orb, s->d_orb_next, st))
+        return -1;
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(s->d_orb, s->d_orb_next, n * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, st));
+    if (s->imagtime && orb_orthonormalize(o, s->d_orb, st)) return -1;
+    return 0;
+}
+
+// phase 1 (driver.c:179-200): matrices of the new orbitals (with the trap
+// and interaction of the new time), SIL step, density matrices
+int phase_coefficients(mctdhb_solver_s* s, cudaStream_t st) {
+    const OrbCtx& o = s->orb;
+    if (o.view.periodic && orb_periodic(o, s->d_orb, st)) return -1;
+    if (orb_matrices(o, s->d_orb, s->d_hob, s->d_hint, st)) return -1;
+    if (s->M == 1) return 0;  // Gross-Pitaevskii: the coefficient is trivial
+    SpaceCtx& sc = s->sp->sp;
+    if (hc_prep(s->M, s->d_hob, s->d_hint, sc.d_tab, st)) return -1;
+    const double2 pdt = s->imagtime ? make_double2(0.0, -s->dt) : make_double2(s->dt, 0.0);
+    if (sil_step(sc, s->sp->lw, s->d_coef, s->lanczos_m, pdt, s->imagtime, st)) return -1;
+    if (dens_apply(sc.view, s->d_coef, sc.d_dens_part, s->d_rho1, s->d_rho2, sc.d_dens_desc, st))
+        return -1;
+    return orb_sync_rho1(o, s->d_rho1, s->d_rinv, s->reg_fac, s->d_info, st);
+}
+
+int count_kernels(cudaGraph_t g) {
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    cudaGraphGetNodes(g, nodes.data(), &nn);
+    int k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nd, &t);
+        if (t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
+}
+
+int build_graphs(mctdhb_solver_s* s) {
+    if (s->exec[0] && s->exec[1]) return 0;
+    s->kernels = 0;
+    for (int p = 0; p < 2; p++) {
+        cudaError_t e = cudaStreamBeginCapture(s->cs, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            set_error("solver: capture: %s", cudaGetErrorString(e));
+            return -1;
+        }
+        const int rc = p == 0 ? phase_orbitals(s, s->cs) : phase_coefficients(s, s->cs);
+        e = cudaStreamEndCapture(s->cs, &s->graph[p]);
+        if (rc) return -1;
+        if (e != cudaSuccess || cudaGraphInstantiate(&s->exec[p], s->graph[p], 0) != cudaSuccess) {
+            set_error("solver: graph capture failed: %s", cudaGetErrorString(e));
+            return -1;
+        }
+        s->kernels += count_kernels(s->graph[p]);
+    }
+    return 0;
+}
+
+void drop_graphs(mctdhb_solver_s* s) {
+    for (int p = 0; p < 2; p++) {
+        if (s->exec[p]) cudaGraphExecDestroy(s->exec[p]);
+        if (s->graph[p]) cudaGraphDestroy(s->graph[p]);
+        s->exec[p] = nullptr;
+        s->graph[p] = nullptr;
+    }
+}
+
+}  // namespace
+
+// one phase of a step, for callers that change the trap or the interaction
+// between the two phases (the reference's sync_equation_params)
+int mctdhb_solver_phase(mctdhb_solver s, int phase, cudaStream_t st) {
+    if (build_graphs(s)) return -1;
+    MCTDHB_CUDA_TRY(cudaGraphLaunch(s->exec[phase], st));
+    return 0;
+}
+
+double2* mctdhb_solver_orb_next(mctdhb_solver s) { return s->d_orb_next; }
+mctdhb_space mctdhb_solver_space(mctdhb_solver s) { return s->sp; }
+
+extern "C" {
+
+int mctdhb_solver_create(uint16_t npar, uint16_t norb, uint16_t grid_size, double xi, double xf,
+                         double d2coef, double d1coef_re, double d1coef_im, int periodic,
+                         int imagtime, int rk_order, int lanczos_iter, double dt,
+                         mctdhb_solver* out) {
+    if (!out) {
+        set_error("mctdhb_solver_create: null output");
+        return -1;
+    }
+    *out = nullptr;
+    if (rk_order != 2 && rk_order != 4 && rk_order != 5) {
+        set_error("mctdhb_solver_create: Runge-Kutta order %d not in {2, 4, 5}", rk_order);
+        return -1;
+    }
+    if (lanczos_iter < 2 || lanczos_iter > 64) {
+        set_error("mctdhb_solver_create: Lanczos dimension %d outside 2..64", lanczos_iter);
+        return -1;
+    }
+    auto* s = new mctdhb_solver_s();
+    s->N = npar;
+    s->M = norb;
+    s->G = grid_size;
+    s->imagtime = imagtime ? 1 : 0;
+    s->rk_order = rk_order;
+    s->lanczos_m = lanczos_iter;
+    s->dt = dt;
+    auto fail = [&]() {
+        mctdhb_solver_destroy(s);
+        return -1;
+    };
+    if (mctdhb_space_create(npar, norb, &s->sp)) return fail();
+    if (orb_init(s->orb, norb, grid_size, xi, xf, d2coef, make_double2(d1coef_re, d1coef_im),
+                 periodic, imagtime))
+        return fail();
+    const size_t n = (size_t)norb * grid_size, M2 = (size_t)norb * norb, M4 = M2 * M2;
+    const size_t nc = mctdhb_space_dim(s->sp);
+    if (cudaMalloc(&s->d_orb, n * sizeof(double2)) || cudaMalloc(&s->d_orb_next, n * sizeof(double2)) ||
+        cudaMalloc(&s->d_coef, nc * sizeof(double2)) || cudaMalloc(&s->d_hob, M2 * sizeof(double2)) ||
+        cudaMalloc(&s->d_hint, M4 * sizeof(double2)) || cudaMalloc(&s->d_rho1, M2 * sizeof(double2)) ||
+        cudaMalloc(&s->d_rho2, M4 * sizeof(double2)) || cudaMalloc(&s->d_rinv, M2 * sizeof(double2)) ||
+        cudaMalloc(&s->d_E, sizeof(double2)) || cudaMalloc(&s->d_info, sizeof(int)) ||
+        cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking)) {
+        set_error("mctdhb_solver_create: device allocation failed");
+        return fail();
+    }
+    int rc = 0;
+    {
+        std::lock_guard<std::mutex> lk(s->sp->mu);
+        if (s->sp->lw.mmax < lanczos_iter) {
+            lanczos_free(s->sp->lw);
+            rc = lanczos_alloc(s->sp->lw, s->sp->sp, std::max(lanczos_iter, 16));
+        }
+    }
+    if (rc) return fail();
+    *out = s;
+    return 0;
+}
+
+void mctdhb_solver_destroy(mctdhb_solver s) {
+    if (!s) return;
+    drop_graphs(s);
+    cudaFree(s->d_orb);
+    cudaFree(s->d_orb_next);
+    cudaFree(s->d_coef);
+    cudaFree(s->d_hob);
+    cudaFree(s->d_hint);
+    cudaFree(s->d_rho1);
+    cudaFree(s->d_rho2);
+    cudaFree(s->d_rinv);
+    cudaFree(s->d_E);
+    cudaFree(s->d_info);
+    if (s->cs) cudaStreamDestroy(s->cs);
+    orb_release(s->orb);
+    mctdhb_space_destroy(s->sp);
+    delete s;
+}
+
+int mctdhb_solver_set_potential(mctdhb_solver s, const double* pot) {
+    if (!s || !pot) {
+        set_error("mctdhb_solver_set_potential: null argument");
+        return -1;
+    }
+    MCTDHB_CUDA_TRY(cudaMemcpy(s->orb.d_pot, pot, s->G * sizeof(double), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int mctdhb_solver_set_interaction(mctdhb_solver s, double g) {
+    if (!s) {
+        set_error("mctdhb_solver_set_interaction: null solver");
+        return -1;
+    }
+    MCTDHB_CUDA_TRY(cudaMemcpy(s->orb.d_g, &g, sizeof(double), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int mctdhb_solver_set_regularization(mctdhb_solver s, double reg_fac) {
+    if (!s || reg_fac > 1e-6 || reg_fac < 1e-13) {
+        set_error("mctdhb_solver_set_regularization: factor outside [1E-13, 1E-6]");
+        return -1;
+    }
+    s->reg_fac = reg_fac;
+    drop_graphs(s);  // the factor is a launch argument: capture again
+    return 0;
+}
+
+// Initial state: orbitals (M x G row-major) and coefficients (host), then the
+// synchronisation the reference performs before integrating
+// (dataio.c full_setup: sync_density_matrices + sync_orbital_matrices).
+int mctdhb_solver_set_state(mctdhb_solver s, const void* orb, const void* coef) {
+    if (!s || !orb || !coef) {
+        set_error("mctdhb_solver_set_state: null argument");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    const size_t n = (size_t)s->M * s->G;
+    const size_t nc = mctdhb_space_dim(s->sp);
+    cudaStream_t st = s->cs;
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(s->d_orb, orb, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(s->d_coef, coef, nc * sizeof(double2), cudaMemcpyHostToDevice, st));
+    SpaceCtx& sc = s->sp->sp;
+    if (dens_prepare(sc.view, s->d_coef, sc.d_dens_part, st)) return -1;
+    if (dens_apply(sc.view, s->d_coef, sc.d_dens_part, s->d_rho1, s->d_rho2, sc.d_dens_desc, st))
+        return -1;
+    if (orb_sync_rho1(s->orb, s->d_rho1, s->d_rinv, s->reg_fac, s->d_info, st)) return -1;
+    if (orb_matrices(s->orb, s->d_orb, s->d_hob, s->d_hint, st)) return -1;
+    if (s->M > 1) {
+        if (hc_prep(s->M, s->d_hob, s->d_hint, sc.d_tab, st)) return -1;
+        HcEpilogue ep;  // tune H.C on this state before the graph is captured
+        hc_variant(sc.view, s->d_coef, s->sp->lw.out, sc.d_tab, ep, st);
+    }
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(st));
+    s->has_state = true;
+    s->t = 0.0;
+    return 0;
+}
+
+int mctdhb_solver_step(mctdhb_solver s, int nsteps, void* stream) {
+    if (!s || !s->has_state) {
+        set_error("mctdhb_solver_step: solver without state");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (build_graphs(s)) return -1;
+    for (int i = 0; i < nsteps; i++) {
+        MCTDHB_CUDA_TRY(cudaGraphLaunch(s->exec[0], (cudaStream_t)stream));
+        MCTDHB_CUDA_TRY(cudaGraphLaunch(s->exec[1], (cudaStream_t)stream));
+        s->t += s->dt;
+    }
+    return 0;
+}
+
+int mctdhb_solver_kernel_count(mctdhb_solver s) {
+    if (!s) return -1;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (build_graphs(s)) return -1;
+    return s->kernels;
+}
+
+// Copies the state to host buffers (NULL skips a field); synchronises.
+int mctdhb_solver_get(mctdhb_solver s, void* orb, void* coef, void* hob, void* hint, void* rho1,
+                      void* rho2, void* rinv) {
+    if (!s) {
+        set_error("mctdhb_solver_get: null solver");
+        return -1;
+    }
+    const size_t n = (size_t)s->M * s->G, M2 = (size_t)s->M * s->M, M4 = M2 * M2;
+    const size_t nc = mctdhb_space_dim(s->sp);
+    MCTDHB_CUDA_TRY(cudaDeviceSynchronize());
+    struct {
+        void* h;
+        const void* d;
+        size_t b;
+    } cp[] = {{orb, s->d_orb, n}, {coef, s->d_coef, nc}, {hob, s->d_hob, M2},
+              {hint, s->d_hint, M4}, {rho1, s->d_rho1, M2}, {rho2, s->d_rho2, M4},
+              {rinv, s->d_rinv, M2}};
+    for (auto& c : cp)
+        if (c.h) MCTDHB_CUDA_TRY(cudaMemcpy(c.h, c.d, c.b * sizeof(double2), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+// Replaces the parts of the state a caller may change between steps
+// (NULL keeps a field): orbitals, coefficients, rho2, rho1^{-1}.
+int mctdhb_solver_put(mctdhb_solver s, const void* orb, const void* coef, const void* rho2,
+                      const void* rinv) {
+    if (!s) {
+        set_error("mctdhb_solver_put: null solver");
+        return -1;
+    }
+    const size_t n = (size_t)s->M * s->G, M2 = (size_t)s->M * s->M, M4 = M2 * M2;
+    const size_t nc = mctdhb_space_dim(s->sp);
+    MCTDHB_CUDA_TRY(cudaDeviceSynchronize());
+    struct {
+        void* d;
+        const void* h;
+        size_t b;
+    } cp[] = {{s->d_orb, orb, n}, {s->d_coef, coef, nc}, {s->d_rho2, rho2, M4},
+              {s->d_rinv, rinv, M2}};
+    for (auto& c : cp)
+        if (c.h) MCTDHB_CUDA_TRY(cudaMemcpy(c.d, c.h, c.b * sizeof(double2), cudaMemcpyHostToDevice));
+    s->has_state = true;
+    return 0;
+}
+
+// E = Tr(rho1 h) + 1/2 sum rho2 g of the current state (integrator_monitor.c:56)
+int mctdhb_solver_energy(mctdhb_solver s, double* e) {
+    if (!s || !e) {
+        set_error("mctdhb_solver_energy: null argument");
+        return -1;
+    }
+    if (orb_energy(s->M, s->d_rho1, s->d_rho2, s->d_hob, s->d_hint, s->d_E, s->cs)) return -1;
+    double2 v;
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(&v, s->d_E, sizeof(v), cudaMemcpyDeviceToHost, s->cs));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(s->cs));
+    e[0] = v.x;
+    e[1] = v.y;
+    return 0;
+}
+
+void* mctdhb_solver_device_coef(mctdhb_solver s) { return s ? s->d_coef : nullptr; }
+void* mctdhb_solver_device_orbitals(mctdhb_solver s) { return s ? s->d_orb : nullptr; }
+double mctdhb_solver_time(mctdhb_solver s) { return s ? s->t : NAN; }
+
+}  // extern "C"

@@ -39,6 +39,12 @@ EXPORTED = [
     "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
     "mctdhb_step_create", "mctdhb_step_launch", "mctdhb_step_kernel_count",
     "mctdhb_step_destroy",
+    "set_orbital_hob", "set_orbital_hint", "sync_orbital_matrices", "mctdhb_propagate_step",
+    "mctdhb_solver_create", "mctdhb_solver_destroy", "mctdhb_solver_set_potential",
+    "mctdhb_solver_set_interaction", "mctdhb_solver_set_regularization",
+    "mctdhb_solver_set_state", "mctdhb_solver_step", "mctdhb_solver_kernel_count",
+    "mctdhb_solver_get", "mctdhb_solver_put", "mctdhb_solver_energy",
+    "mctdhb_solver_device_coef", "mctdhb_solver_device_orbitals", "mctdhb_solver_time",
 ]
 
 _lib = None
@@ -119,6 +125,38 @@ def load(path=LIB_PATH):
     L.mctdhb_step_kernel_count.restype = i
     L.mctdhb_step_kernel_count.argtypes = [vp]
     L.mctdhb_step_destroy.argtypes = [vp]
+    L.set_orbital_hob.argtypes = [T.OrbitalEquation, u16, T.Cmatrix, T.Cmatrix]
+    L.set_orbital_hint.argtypes = [T.OrbitalEquation, u16, T.Cmatrix, T.Carray]
+    L.sync_orbital_matrices.argtypes = [T.OrbitalEquation, T.ManyBodyState]
+    L.mctdhb_propagate_step.argtypes = [T.MCTDHBDataStruct, T.Carray, T.Carray, u32]
+    d = C.c_double
+    L.mctdhb_solver_create.restype = i
+    L.mctdhb_solver_create.argtypes = [u16, u16, u16, d, d, d, d, d, i, i, i, i, d,
+                                       C.POINTER(vp)]
+    L.mctdhb_solver_destroy.argtypes = [vp]
+    for f in ("set_potential", "set_interaction", "set_regularization"):
+        getattr(L, "mctdhb_solver_" + f).restype = i
+    L.mctdhb_solver_set_potential.argtypes = [vp, C.POINTER(d)]
+    L.mctdhb_solver_set_interaction.argtypes = [vp, d]
+    L.mctdhb_solver_set_regularization.argtypes = [vp, d]
+    L.mctdhb_solver_set_state.restype = i
+    L.mctdhb_solver_set_state.argtypes = [vp, vp, vp]
+    L.mctdhb_solver_step.restype = i
+    L.mctdhb_solver_step.argtypes = [vp, i, vp]
+    L.mctdhb_solver_kernel_count.restype = i
+    L.mctdhb_solver_kernel_count.argtypes = [vp]
+    L.mctdhb_solver_get.restype = i
+    L.mctdhb_solver_get.argtypes = [vp] + [vp] * 7
+    L.mctdhb_solver_put.restype = i
+    L.mctdhb_solver_put.argtypes = [vp] + [vp] * 4
+    L.mctdhb_solver_energy.restype = i
+    L.mctdhb_solver_energy.argtypes = [vp, C.POINTER(d)]
+    L.mctdhb_solver_device_coef.restype = vp
+    L.mctdhb_solver_device_coef.argtypes = [vp]
+    L.mctdhb_solver_device_orbitals.restype = vp
+    L.mctdhb_solver_device_orbitals.argtypes = [vp]
+    L.mctdhb_solver_time.restype = d
+    L.mctdhb_solver_time.argtypes = [vp]
     _lib = L
     return L
 
@@ -229,6 +267,72 @@ class Step:
             self.close()
         except Exception:
             pass
+
+
+class Solver:
+    """A whole MCTDHB system resident on the device (include/mctdhb_gpu.h,
+    mctdhb_solver_*): orbitals, coefficients and their matrices; one step is
+    the reference's mctdhb_propagate_step as two replayed CUDA graphs."""
+
+    def __init__(self, npar, norb, grid, xi, xf, dt, imagtime, rk_order=5, lanczos_iter=5,
+                 d2coef=-0.5, d1coef=0j, periodic=True):
+        L = load()
+        h = C.c_void_p()
+        _check(L.mctdhb_solver_create(npar, norb, grid, xi, xf, d2coef, complex(d1coef).real,
+                                      complex(d1coef).imag, int(periodic), int(imagtime),
+                                      rk_order, lanczos_iter, dt, C.byref(h)),
+               "mctdhb_solver_create")
+        self.h = h
+        self.npar, self.norb, self.grid = npar, norb, grid
+        self.dim = int(L.space_dimension(npar, norb))
+
+    def close(self):
+        if self.h:
+            load().mctdhb_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_potential(self, pot):
+        pot = np.ascontiguousarray(pot, np.float64)
+        _check(load().mctdhb_solver_set_potential(self.h, pot.ctypes.data_as(C.POINTER(C.c_double))),
+               "mctdhb_solver_set_potential")
+
+    def set_interaction(self, g):
+        _check(load().mctdhb_solver_set_interaction(self.h, g), "mctdhb_solver_set_interaction")
+
+    def set_state(self, orb, coef):
+        orb = np.ascontiguousarray(orb, np.complex128)
+        coef = np.ascontiguousarray(coef, np.complex128)
+        _check(load().mctdhb_solver_set_state(self.h, orb.ctypes.data, coef.ctypes.data),
+               "mctdhb_solver_set_state")
+
+    def step(self, n=1, stream=None):
+        _check(load().mctdhb_solver_step(self.h, n, _stream_ptr(stream)), "mctdhb_solver_step")
+
+    @property
+    def kernels(self):
+        return int(load().mctdhb_solver_kernel_count(self.h))
+
+    def get(self):
+        M, G = self.norb, self.grid
+        out = {"orb": np.zeros((M, G), np.complex128), "coef": np.zeros(self.dim, np.complex128),
+               "hob": np.zeros((M, M), np.complex128), "hint": np.zeros(M ** 4, np.complex128),
+               "rho1": np.zeros((M, M), np.complex128), "rho2": np.zeros(M ** 4, np.complex128),
+               "rinv": np.zeros((M, M), np.complex128)}
+        k = ("orb", "coef", "hob", "hint", "rho1", "rho2", "rinv")
+        _check(load().mctdhb_solver_get(self.h, *[out[x].ctypes.data for x in k]),
+               "mctdhb_solver_get")
+        return out
+
+    def energy(self):
+        e = (C.c_double * 2)()
+        _check(load().mctdhb_solver_energy(self.h, e), "mctdhb_solver_energy")
+        return complex(e[0], e[1])
 
 
 class DropIn:

@@ -93,6 +93,24 @@ void set_regulatization_factor(double reg_fac);
 /* synchronize.h:41 (synchronize.c:28) */
 double get_current_regularization_factor(void);
 
+/* include/function_tools/orbital_matrices.h:25 (orbital_matrices.c:22):
+ * h_kl on the GPU (finite-difference derivative, Simpson weights) */
+void set_orbital_hob(OrbitalEquation eq_desc, uint16_t norb, Cmatrix orb, Cmatrix hob);
+/* orbital_matrices.h:30 (orbital_matrices.c:73): g_ksql on the GPU, one
+ * complex (M^2 x G)(G x M^2) contraction on the FP64 tensor cores */
+void set_orbital_hint(OrbitalEquation eq_desc, uint16_t norb, Cmatrix orb, Carray hint);
+/* include/integrator/synchronize.h:45 (synchronize.c:35) */
+void sync_orbital_matrices(OrbitalEquation eq_desc, ManyBodyState psi);
+/* include/integrator/driver.h:67 (driver.c:159): one full step on the GPU.
+ * Supported integrator settings: FULLSTEP_RUNGEKUTTA orbitals with
+ * FINITEDIFF derivatives (RK2 / RK4 / RK5 as the named tableaux Heun,
+ * classical RK4 and Butcher RK5), LANCZOS coefficients, the simple
+ * projector.  Other settings are reported as errors.  orb_works receives
+ * the orbitals after the Runge-Kutta step, coef_works the Lanczos
+ * combination before the imaginary-time renormalisation. */
+void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coef_works,
+                           uint32_t curr_step);
+
 /* include/assistant/integrator_monitor.h:53 (integrator_monitor.c:56) */
 dcomplex total_energy(ManyBodyState psi);
 /* integrator_monitor.h:26 (integrator_monitor.c:10) */
@@ -137,6 +155,36 @@ int  mctdhb_step_create(mctdhb_space sp, void* d_coef, void* d_rho1, void* d_rho
 int  mctdhb_step_launch(mctdhb_step st, void* stream);
 int  mctdhb_step_kernel_count(mctdhb_step st); /* kernels launched per replay */
 void mctdhb_step_destroy(mctdhb_step st);
+
+/* A whole MCTDHB system resident on the device: orbitals (norb x grid),
+ * coefficients, h, g, rho1, rho2, rho1^{-1}.  One step (driver.c:159-201:
+ * orbital Runge-Kutta step, Gram-Schmidt in imaginary time, h and g of the
+ * new orbitals, SIL step of the coefficients, density matrices, regularised
+ * rho1^{-1}) is two captured CUDA graphs replayed per step.  Trap and
+ * interaction are read from device memory at replay time: set them between
+ * steps to follow time-dependent parameters.  Host buffers below are
+ * complex128 row-major (orbitals norb x grid). */
+typedef struct mctdhb_solver_s* mctdhb_solver;
+int  mctdhb_solver_create(uint16_t npar, uint16_t norb, uint16_t grid_size, double xi, double xf,
+                          double d2coef, double d1coef_re, double d1coef_im, int periodic,
+                          int imagtime, int rk_order, int lanczos_iter, double dt,
+                          mctdhb_solver* out);
+void mctdhb_solver_destroy(mctdhb_solver s);
+int  mctdhb_solver_set_potential(mctdhb_solver s, const double* pot); /* grid values */
+int  mctdhb_solver_set_interaction(mctdhb_solver s, double g);
+int  mctdhb_solver_set_regularization(mctdhb_solver s, double reg_fac);
+/* initial orbitals + coefficients, then rho1, rho2, rho1^{-1}, h, g */
+int  mctdhb_solver_set_state(mctdhb_solver s, const void* orb, const void* coef);
+int  mctdhb_solver_step(mctdhb_solver s, int nsteps, void* stream);
+int  mctdhb_solver_kernel_count(mctdhb_solver s); /* kernels per step */
+int  mctdhb_solver_get(mctdhb_solver s, void* orb, void* coef, void* hob, void* hint, void* rho1,
+                       void* rho2, void* rinv);
+int  mctdhb_solver_put(mctdhb_solver s, const void* orb, const void* coef, const void* rho2,
+                       const void* rinv);
+int  mctdhb_solver_energy(mctdhb_solver s, double* e_re_im); /* Tr(rho1 h) + rho2 g / 2 */
+void*  mctdhb_solver_device_coef(mctdhb_solver s);
+void*  mctdhb_solver_device_orbitals(mctdhb_solver s);
+double mctdhb_solver_time(mctdhb_solver s);
 
 /* Index tables on the device, bit-exact with the reference's: hash table
  * (dim x M uint16), single-jump map (M^2 dim uint32). */

@@ -375,3 +375,85 @@ class Reference:
 
     def fn(self, name):
         return C.cast(getattr(self.lib, name), C.c_void_p).value
+
+    def make_mctdhb(self, N, M, G, xi, xf, imagtime, rk_order, lanczos_m, dt, omega, g,
+                    periodic=True):
+        """A reference MCTDHBDataStruct from its own constructor
+        (types_definition.c:247): FULLSTEP_RUNGEKUTTA orbitals, FINITEDIFF
+        derivatives, LANCZOS coefficients, harmonic trap
+        (builtin_potential.c:37) and constant g (builtin_time_parameter.c:7).
+        Returns (struct pointer, keep-alive list)."""
+        L = self.lib
+        pot_args = (C.c_double * 3)(omega, omega, 0.0)
+        g_args = (C.c_double * 3)(g, g, 0.0)
+        ms = L.get_mctdhb_struct(
+            T.IMAGTIME if imagtime else T.REALTIME, T.LANCZOS, T.FULLSTEP_RUNGEKUTTA,
+            T.FINITEDIFF, rk_order, lanczos_m, N, M, b"harmonic",
+            T.PERIODIC_BOUNDS if periodic else T.ZERO_BOUNDS, xi, xf, G, dt, 1.0, -0.5,
+            T.dcomplex(0.0, 0.0), C.cast(pot_args, C.c_void_p), C.cast(g_args, C.c_void_p),
+            self.fn("potfunc_harmonic"), self.fn("timeparam_linear_ramp"))
+        return ms, [pot_args, g_args]
+
+    def set_state(self, ms, orb, coef):
+        """orbitals and coefficients into the struct, then the reference's
+        own initial synchronisation (dataio.c full_setup)"""
+        st = ms.contents.state.contents
+        M, G = orb.shape
+        for k in range(M):
+            row = C.cast(st.orbitals[k], C.POINTER(C.c_double * (2 * G))).contents
+            np.frombuffer(row, np.complex128)[:] = orb[k]
+        cbuf = C.cast(st.coef, C.POINTER(C.c_double * (2 * len(coef)))).contents
+        np.frombuffer(cbuf, np.complex128)[:] = coef
+        self.lib.sync_orbital_matrices(ms.contents.orb_eq, ms.contents.state)
+        self.lib.sync_density_matrices(ms.contents.multiconfig_space, ms.contents.state)
+
+    def get_state(self, ms):
+        st = ms.contents.state.contents
+        M, G, nc = st.norb, st.grid_size, st.space_dim
+        return {
+            "orb": T.cmatrix_to_numpy(st.orbitals, M, G),
+            "coef": T.carray_to_numpy(st.coef, nc),
+            "hob": T.cmatrix_to_numpy(st.hob, M, M),
+            "hint": T.carray_to_numpy(st.hint, M ** 4),
+            "rho1": T.cmatrix_to_numpy(st.ob_denmat, M, M),
+            "rho2": T.carray_to_numpy(st.tb_denmat, M ** 4),
+            "rinv": T.cmatrix_to_numpy(st.inv_ob_denmat, M, M),
+            "pot": np.ctypeslib.as_array(ms.contents.orb_eq.contents.pot_grid, shape=(G,)).copy(),
+        }
+
+    def step(self, ms, k):
+        st = ms.contents.state.contents
+        ow = np.zeros(st.norb * st.grid_size, np.complex128)
+        cw = np.zeros(st.space_dim, np.complex128)
+        self.lib.mctdhb_propagate_step(ms, T.carray(ow), T.carray(cw), k)
+        return ow, cw
+
+    def destroy_mctdhb(self, ms):
+        self.lib.destroy_mctdhb_struct(ms)
+
+
+def hermite_orbitals(M, G, xi, xf):
+    """Hermite-Gaussian orbitals n = 0..M-1 on the grid, Gram-Schmidt in
+    the Simpson metric (the synthetic initial orbitals of the workloads)"""
+    x = np.linspace(xi, xf, G)
+    dx = x[1] - x[0]
+    w = np.zeros(G)
+    if G % 2 == 0:
+        for i in range(0, G - 4, 2):
+            w[i:i + 3] += [1, 4, 1]
+        w[: G - 3] *= dx / 3
+        w[G - 4:] += np.array([1, 3, 3, 1]) * 3 * dx / 8
+    else:
+        for i in range(0, G - 2, 2):
+            w[i:i + 3] += [1, 4, 1]
+        w *= dx / 3
+    phi = np.zeros((M, G), np.complex128)
+    hm, hc = np.zeros(G), np.exp(-x ** 2 / 2)
+    for n in range(M):
+        phi[n] = hc
+        hm, hc = hc, (np.sqrt(2.0) * x * hc - np.sqrt(n) * hm) / np.sqrt(n + 1)
+    for i in range(M):
+        for j in range(i):
+            phi[i] -= np.sum(w * phi[j].conj() * phi[i]) * phi[j]
+        phi[i] /= np.sqrt(np.sum(w * np.abs(phi[i]) ** 2))
+    return phi, dx

@@ -1,0 +1,93 @@
+"""The oracle's orbital side and full step pinned against the reference's
+own mctdhb_propagate_step (driver.c:159-201), compiled from its sources with
+the named Runge-Kutta tableaux of oracle/shim/odesys_rk.c.  Runs where
+oracle/_ref is built."""
+import numpy as np
+import pytest
+
+from helpers import rand_coef, rel_err
+from oracle import hermite_orbitals
+
+
+def oracle_state(ref_state, coef):
+    return {
+        "orb": np.ascontiguousarray(ref_state["orb"]),
+        "coef": np.ascontiguousarray(coef.copy()),
+        "hob": np.ascontiguousarray(ref_state["hob"]),
+        "hint": np.ascontiguousarray(ref_state["hint"]),
+        "rho1": np.ascontiguousarray(ref_state["rho1"]),
+        "rho2": np.ascontiguousarray(ref_state["rho2"]),
+        "rinv": np.ascontiguousarray(ref_state["rinv"]),
+    }
+
+
+CASES = [  # N, M, G, imag, rk, lanczos m, dt, g
+    (4, 3, 64, True, 5, 5, 0.01, 0.5),
+    (4, 3, 64, False, 5, 5, 0.005, 0.5),
+    (6, 4, 96, True, 4, 4, 0.01, 1.0),
+    (5, 2, 64, False, 2, 3, 0.005, 0.3),
+]
+
+
+@pytest.mark.parametrize("N,M,G,imag,rk,m,dt,g", CASES)
+def test_full_step_oracle_vs_reference(oracle, reference, N, M, G, imag, rk, m, dt, g):
+    xi, xf = -8.0, 8.0
+    ms, keep = reference.make_mctdhb(N, M, G, xi, xf, imag, rk, m, dt, 1.0, g)
+    try:
+        orb, dx = hermite_orbitals(M, G, xi, xf)
+        rng = np.random.default_rng(N * 10 + M)
+        coef = rand_coef(rng, oracle.dim(N, M))
+        reference.set_state(ms, orb, coef)
+        r0 = reference.get_state(ms)
+        # initial synchronisation agrees
+        assert rel_err(oracle.orbital_hob(r0["orb"], dx, -0.5, 0.0, r0["pot"]), r0["hob"]) < 1e-12
+        assert rel_err(oracle.orbital_hint(r0["orb"], dx, g), r0["hint"]) < 1e-12
+        r1, r2, ri = oracle.sync_density_matrices(N, M, coef)
+        assert rel_err(r1, r0["rho1"]) < 1e-13 and rel_err(r2, r0["rho2"]) < 1e-13
+        assert rel_err(ri, r0["rinv"]) < 1e-10
+        st = oracle_state(r0, coef)
+        for k in range(3):
+            reference.step(ms, k)
+            oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, imag, rk, m, r0["pot"])
+        rs = reference.get_state(ms)
+        assert rel_err(st["orb"], rs["orb"]) < 1e-10
+        assert rel_err(st["coef"], rs["coef"]) < 1e-10
+        assert rel_err(st["rho1"], rs["rho1"]) < 1e-10
+        e_ref = oracle.total_energy(M, rs["rho1"], rs["rho2"], rs["hob"], rs["hint"])
+        e_orc = oracle.total_energy(M, st["rho1"], st["rho2"], st["hob"], st["hint"])
+        assert abs(e_ref - e_orc) < 1e-10 * abs(e_ref)
+    finally:
+        reference.destroy_mctdhb(ms)
+
+
+def test_orthonormalize_vs_reference(oracle, reference):
+    import mctdhb_types as T
+
+    rng = np.random.default_rng(3)
+    M, G = 4, 65
+    f = rng.normal(size=(M, G)) + 1j * rng.normal(size=(M, G))
+    dx = 0.1
+    R = T.RowMatrix(f.copy())
+    reference.lib.orthonormalize(G, dx, M, R.ptr)
+    assert rel_err(oracle.orthonormalize(f, dx), R.a) < 1e-12
+
+
+def test_rk5_is_fifth_order(oracle):
+    """Butcher's tableau of the shim: y' = i y over one step of size h has
+    local error O(h^6)"""
+    import importlib
+
+    errs = []
+    for h in (0.2, 0.1):
+        # integrate with the oracle's tableau via a 1x1 'orbital' equation is
+        # not exposed; check the tableau arithmetic directly
+        k1 = 1j
+        k2 = 1j * (1 + h * 0.25 * k1)
+        k3 = 1j * (1 + h * (0.125 * k1 + 0.125 * k2))
+        k4 = 1j * (1 + h * (-0.5 * k2 + k3))
+        k5 = 1j * (1 + h * (3 / 16 * k1 + 9 / 16 * k4))
+        k6 = 1j * (1 + h * (-3 / 7 * k1 + 2 / 7 * k2 + 12 / 7 * k3 - 12 / 7 * k4 + 8 / 7 * k5))
+        y = 1 + h * (7 * k1 + 32 * k3 + 12 * k4 + 32 * k5 + 7 * k6) / 90
+        errs.append(abs(y - np.exp(1j * h)))
+    assert 50 < errs[0] / errs[1] < 80  # 2^6 = 64
+    importlib.invalidate_caches()
