@@ -79,6 +79,13 @@ int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2*
 int dens_descriptors(int M, int* host_desc);  // returns count; desc = 5 ints/elem
 // one-time launch attributes and the tuned variant, before any capture
 int dens_prepare(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st);
+// kernels of density.cu also launched by noalloc.cu on its own scratch
+__global__ void dens_generic_kernel(SpaceView sp, const double2* __restrict__ C,
+                                    double2* __restrict__ partial, int EP);
+__global__ void dens_finalize_kernel(int M, int E, int EP, int nblocks,
+                                     const double2* __restrict__ partial,
+                                     const int* __restrict__ desc, double2* __restrict__ rho1,
+                                     double2* __restrict__ rho2);
 
 // space.cu (map kernels)
 int build_hash_table(const SpaceView& sp, uint16_t* d_ht, cudaStream_t st);

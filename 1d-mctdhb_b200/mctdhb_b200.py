@@ -36,6 +36,7 @@ EXPORTED = [
     "mctdhb_dev_set_matrices", "mctdhb_dev_apply_hamiltonian", "mctdhb_dev_density_matrices",
     "mctdhb_dev_sil_step", "mctdhb_dev_hash_table", "mctdhb_dev_single_jump_map",
     "mctdhb_dev_double_jump_chunks", "mctdhb_dev_double_jump_map",
+    "mctdhb_dev_density_matrices_noalloc",
     "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
     "mctdhb_step_create", "mctdhb_step_launch", "mctdhb_step_kernel_count",
     "mctdhb_step_destroy",
@@ -115,6 +116,8 @@ def load(path=LIB_PATH):
     L.mctdhb_dev_double_jump_chunks.argtypes = [vp, i, C.POINTER(C.c_uint64)]
     L.mctdhb_dev_double_jump_map.restype = i
     L.mctdhb_dev_double_jump_map.argtypes = [vp, i, vp, vp, vp]
+    L.mctdhb_dev_density_matrices_noalloc.restype = i
+    L.mctdhb_dev_density_matrices_noalloc.argtypes = [u16, u16, vp, vp, vp, vp]
     L.sync_density_matrices.argtypes = [T.MultiConfiguration, T.ManyBodyState]
     L.set_regulatization_factor.argtypes = [C.c_double]
     L.get_current_regularization_factor.restype = C.c_double

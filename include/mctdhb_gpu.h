@@ -198,6 +198,27 @@ int mctdhb_dev_double_jump_chunks(mctdhb_space sp, int diff, uint64_t* n_chunks)
 int mctdhb_dev_double_jump_map(mctdhb_space sp, int diff, void* d_strides, void* d_map,
                                void* stream);
 
+/* rho1 and rho2 of C, as mctdhb_dev_density_matrices computes them, with no
+ * device allocation at all.  This entry point has no counterpart in the
+ * reference.  It is for callers that cannot let a library call cudaMalloc
+ * or cudaFree: a process whose device memory is owned by its own pool
+ * allocator (PyTorch's caching allocator, an arena reserved at start-up),
+ * or a loop that cannot pay for the device-wide synchronisation that
+ * cudaMalloc and cudaFree imply.  No mctdhb_space is needed (creating one
+ * allocates): the space is named by (npar, norb), and its tables and the
+ * partial sums live in one static device array of
+ * MCTDHB_NOALLOC_SCRATCH_BYTES (8 MiB), held by every GPU that loads the
+ * library until the process exits.  Spaces that do not fit are rejected
+ * with an error: every space with norb <= 8 fits, and norb up to 25 on a
+ * smaller grid.  The first call on each device looks up the array's device
+ * address and sets kernel launch attributes; make it before any stream
+ * capture.  All calls on one device share the array: calls that overlap on
+ * the GPU (streams with no ordering between them) race and give undefined
+ * results.  Each call rewrites every part of the array it reads. */
+#define MCTDHB_NOALLOC_SCRATCH_BYTES 8388608u
+int mctdhb_dev_density_matrices_noalloc(uint16_t npar, uint16_t norb, const void* d_coef,
+                                        void* d_rho1, void* d_rho2, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
