@@ -1,0 +1,810 @@
+// batch.cu -- host side of the batched engine (include/mctdhb_gpu.h, part 5):
+// many independent MCTDHB systems of uneven (N, M, grid) resident in one HBM
+// arena and advanced together, one CUDA graph launch per step of the whole
+// batch.
+//
+//   admission   a job's exact footprint (mctdhb_batch_job_bytes) is carved
+//               from the arena (first fit); the job is refused (not queued)
+//               when no free slot or range is left, so a serving loop admits
+//               by memory footprint.  Admission uploads the state and runs
+//               the set-up the single-system solver runs before integrating
+//               (rho1, rho2, regularised rho1^{-1}, h, g, energy).
+//   work lists  per-slot tiles (vector rows, H.C rows and density slices per
+//               orbital count, whole slots) live in device memory; the step
+//               graph's persistent kernels read them at run time, so the
+//               graph is captured once per set of orbital counts present and
+//               systems join and leave between launches without a capture.
+//   stopping    each slot stops on the device (step limit, or the
+//               imaginary-time energy rule of driver.c:47-67) and is then
+//               skipped by every kernel; poll/fetch/release hand it back.
+// Every slot's arithmetic depends only on that slot's data and sizes, so a
+// system gives the same bits alone and in any mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "../../include/mctdhb_gpu.h"
+#include "batch.h"
+#include "batch_kernels.h"
+#include "common.cuh"
+#include "engine.h"
+#include "kernels.h"
+#include "moves.cuh"
+#include "orbital.h"
+
+using namespace mctdhb;
+
+namespace {
+
+size_t al256(size_t b) { return (b + 255) / 256 * 256; }
+
+// sizes of one job's parts, in the arena order
+struct JobLayout {
+    uint32_t nc = 0;
+    int vtiles = 0, dslices = 0, dchunks = 0, E = 0, EP = 0;
+    size_t o_orb, o_stage, o_H, o_pot, o_w, o_Q, o_hob, o_hint, o_tab, o_rho1, o_rho2, o_rinv,
+        o_work, o_T, o_sq, o_g, o_V, o_out, o_part, o_dpart, total;
+};
+
+int job_layout(int N, int M, int G, int lz, JobLayout& L) {
+    if (M < kBatchMinOrb || M > kBatchMaxOrb) {
+        set_error("batch: %d orbitals outside %d..%d", M, kBatchMinOrb, kBatchMaxOrb);
+        return -1;
+    }
+    if (N < 1 || N > 10000) {
+        set_error("batch: %d particles outside 1..10000", N);
+        return -1;
+    }
+    if (G < 5 || G > kBatchMaxGrid) {
+        set_error("batch: grid of %d points outside 5..%d", G, kBatchMaxGrid);
+        return -1;
+    }
+    const uint64_t dim = fock_dimension(N, M);
+    if (dim == 0 || dim >= (uint64_t)UINT32_MAX) {
+        set_error("batch: %d particles in %d orbitals exceed 32-bit configuration indices", N, M);
+        return -1;
+    }
+    L.nc = (uint32_t)dim;
+    L.vtiles = (int)((dim + kBatchVecRows - 1) / kBatchVecRows);
+    const uint64_t chunks = (dim + kBatchDensThreads - 1) / kBatchDensThreads;
+    L.dchunks = (int)std::max<uint64_t>(8, (chunks + kBatchMaxSlices - 1) / kBatchMaxSlices);
+    L.dslices = (int)((chunks + L.dchunks - 1) / L.dchunks);
+    L.E = dens_nelem(M);
+    L.EP = (L.E + 7) / 8 * 8;
+    const size_t n = (size_t)M * G, M2 = (size_t)M * M, M4 = M2 * M2, z = sizeof(double2);
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o += al256(bytes);
+        return at;
+    };
+    L.o_orb = take(n * z);
+    L.o_stage = take(7 * n * z);
+    L.o_H = take(n * z);
+    L.o_pot = take((size_t)G * sizeof(double));
+    L.o_w = take((size_t)G * sizeof(double));
+    L.o_Q = take(M4 * z);
+    L.o_hob = take(M2 * z);
+    L.o_hint = take(M4 * z);
+    L.o_tab = take((size_t)hc_table_size(M) * z);
+    L.o_rho1 = take(M2 * z);
+    L.o_rho2 = take(M4 * z);
+    L.o_rinv = take(M2 * z);
+    L.o_work = take((3 * M2 + M + 2) * z);
+    L.o_T = take((size_t)(M - 1) * (N + 1) * sizeof(uint32_t));
+    L.o_sq = take((size_t)(N + 3) * sizeof(double));
+    L.o_g = take(sizeof(double));
+    L.o_V = take((size_t)lz * dim * z);
+    L.o_out = take((size_t)dim * z);
+    L.o_part = take((size_t)kBatchMaxLz * L.vtiles * z);
+    L.o_dpart = take((size_t)L.dslices * L.EP * z);
+    L.total = o;
+    return 0;
+}
+
+struct HostSlot {
+    bool used = false;
+    bool running = false;
+    size_t off = 0, bytes = 0;
+    BatchSlot d{};
+    JobLayout L{};
+};
+
+constexpr int kNumM = kBatchMaxOrb + 1;  // lists indexed by M
+
+}  // namespace
+
+struct mctdhb_batch_s {
+    int max_slots = 0, lz = 0;
+    size_t arena_bytes = 0;
+    char* arena = nullptr;
+    std::map<size_t, size_t> free_ranges;  // offset -> bytes
+    std::vector<HostSlot> hs;
+    BatchSlot* d_slots = nullptr;
+    double2* d_scal = nullptr;  // max_slots x BS_TOTAL
+    int* d_flags = nullptr;     // max_slots x BF_TOTAL
+    int* d_desc[kNumM] = {};
+    // work lists (device) and their pinned host images
+    size_t cap_vec = 0, cap_hc = 0, cap_dn = 0;
+    int* d_list = nullptr;  // [0] count, [1..] slots
+    BatchTile *d_vec = nullptr, *d_hc = nullptr, *d_dn = nullptr;
+    int* d_cnt = nullptr;  // [0] vec count, [1..9] hc off, [10..18] hc cnt, [19..27] dn off, [28..36] dn cnt
+    int* h_list = nullptr;
+    BatchTile *h_vec = nullptr, *h_hc = nullptr, *h_dn = nullptr;
+    int* h_cnt = nullptr;
+    // single-slot lists of the admission set-up
+    int* d_pro = nullptr;  // [0] 1, [1] slot, then 1 + 2 kNumM ints of offsets / counts
+    BatchTile* d_pro_dn = nullptr;
+    int* h_pro = nullptr;
+    BatchTile* h_pro_dn = nullptr;
+    int* h_flags = nullptr;
+    double2* h_scal = nullptr;
+    unsigned present_mask = 0;  // orbital counts present in the lists
+    bool lists_dirty = true;
+    cudaStream_t st = nullptr;
+    cudaStream_t side[kNumM] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kNumM] = {};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned graph_mask = 0;
+    int kernels = 0;
+    std::mutex mu;
+};
+
+namespace {
+
+int* cnt_vec(int* c) { return c; }
+int* hc_off(int* c) { return c + 1; }
+int* hc_cnt(int* c) { return c + 1 + kNumM; }
+int* dn_off(int* c) { return c + 1 + 2 * kNumM; }
+int* dn_cnt(int* c) { return c + 1 + 3 * kNumM; }
+constexpr int kCntInts = 1 + 4 * kNumM;
+
+void drop_graph(mctdhb_batch_s* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+// arena first fit
+bool arena_take(mctdhb_batch_s* b, size_t bytes, size_t* off) {
+    for (auto it = b->free_ranges.begin(); it != b->free_ranges.end(); ++it) {
+        if (it->second >= bytes) {
+            *off = it->first;
+            const size_t rest = it->second - bytes;
+            const size_t at = it->first + bytes;
+            b->free_ranges.erase(it);
+            if (rest) b->free_ranges[at] = rest;
+            return true;
+        }
+    }
+    return false;
+}
+
+void arena_give(mctdhb_batch_s* b, size_t off, size_t bytes) {
+    auto it = b->free_ranges.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != b->free_ranges.end() && it->first + it->second == nx->first) {
+        it->second += nx->second;
+        b->free_ranges.erase(nx);
+    }
+    if (it != b->free_ranges.begin()) {
+        auto pv = std::prev(it);
+        if (pv->first + pv->second == it->first) {
+            pv->second += it->second;
+            b->free_ranges.erase(it);
+        }
+    }
+}
+
+// the step's work lists from the running slots, uploaded on the engine stream
+int rebuild_lists(mctdhb_batch_s* b) {
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(b->st));  // the pinned images are free to rewrite
+    int ns = 0;
+    size_t nv = 0;
+    std::memset(b->h_cnt, 0, kCntInts * sizeof(int));
+    unsigned mask = 0;
+    for (int s = 0; s < b->max_slots; s++) {
+        const HostSlot& h = b->hs[s];
+        if (!h.used || !h.running) continue;
+        b->h_list[1 + ns++] = s;
+        for (int t = 0; t < h.L.vtiles; t++) b->h_vec[nv++] = BatchTile{s, (uint32_t)t};
+        mask |= 1u << h.d.M;
+    }
+    b->h_list[0] = ns;
+    cnt_vec(b->h_cnt)[0] = (int)nv;
+    size_t nh = 0, nd = 0;
+    for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++) {
+        hc_off(b->h_cnt)[M] = (int)nh;
+        dn_off(b->h_cnt)[M] = (int)nd;
+        for (int q = 0; q < ns; q++) {
+            const int s = b->h_list[1 + q];
+            const HostSlot& h = b->hs[s];
+            if (h.d.M != M) continue;
+            for (uint32_t r = 0; r < h.L.nc; r += kBatchHcRows) b->h_hc[nh++] = BatchTile{s, r};
+            for (int sl = 0; sl < h.L.dslices; sl++) b->h_dn[nd++] = BatchTile{s, (uint32_t)sl};
+        }
+        hc_cnt(b->h_cnt)[M] = (int)nh - hc_off(b->h_cnt)[M];
+        dn_cnt(b->h_cnt)[M] = (int)nd - dn_off(b->h_cnt)[M];
+    }
+    if (nv > b->cap_vec || nh > b->cap_hc || nd > b->cap_dn) {
+        set_error("batch: work lists exceed their capacity");
+        return -1;
+    }
+    cudaStream_t st = b->st;
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_list, b->h_list, (1 + ns) * sizeof(int),
+                                    cudaMemcpyHostToDevice, st));
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_cnt, b->h_cnt, kCntInts * sizeof(int),
+                                    cudaMemcpyHostToDevice, st));
+    if (nv)
+        MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_vec, b->h_vec, nv * sizeof(BatchTile),
+                                        cudaMemcpyHostToDevice, st));
+    if (nh)
+        MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_hc, b->h_hc, nh * sizeof(BatchTile),
+                                        cudaMemcpyHostToDevice, st));
+    if (nd)
+        MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_dn, b->h_dn, nd * sizeof(BatchTile),
+                                        cudaMemcpyHostToDevice, st));
+    b->present_mask = mask;
+    b->lists_dirty = false;
+    return 0;
+}
+
+int hc_group(int M, const BatchSlot* slots, const BatchTile* tiles, const int* off,
+             const int* cnt, int iter, cudaStream_t st) {
+    switch (M) {
+        case 2: return hc_batch_launch<2>(slots, tiles, off, cnt, iter, st);
+        case 3: return hc_batch_launch<3>(slots, tiles, off, cnt, iter, st);
+        case 4: return hc_batch_launch<4>(slots, tiles, off, cnt, iter, st);
+        case 5: return hc_batch_launch<5>(slots, tiles, off, cnt, iter, st);
+        case 6: return hc_batch_launch<6>(slots, tiles, off, cnt, iter, st);
+        case 7: return hc_batch_launch<7>(slots, tiles, off, cnt, iter, st);
+        case 8: return hc_batch_launch<8>(slots, tiles, off, cnt, iter, st);
+    }
+    return 0;
+}
+
+int dens_group(int M, const BatchSlot* slots, const BatchTile* tiles, const int* off,
+               const int* cnt, cudaStream_t st) {
+    switch (M) {
+        case 2: return dens_batch_launch<2>(slots, tiles, off, cnt, st);
+        case 3: return dens_batch_launch<3>(slots, tiles, off, cnt, st);
+        case 4: return dens_batch_launch<4>(slots, tiles, off, cnt, st);
+        case 5: return dens_batch_launch<5>(slots, tiles, off, cnt, st);
+        case 6: return dens_batch_launch<6>(slots, tiles, off, cnt, st);
+        case 7: return dens_batch_launch<7>(slots, tiles, off, cnt, st);
+        case 8: return dens_batch_launch<8>(slots, tiles, off, cnt, st);
+    }
+    return 0;
+}
+
+// one launch per orbital count present, on parallel branches of the graph
+template <class F>
+int per_group(mctdhb_batch_s* b, unsigned mask, F&& launch) {
+    int groups = 0;
+    for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++)
+        if (mask >> M & 1) groups++;
+    if (groups <= 1) {
+        for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++)
+            if (mask >> M & 1)
+                if (launch(M, b->st)) return -1;
+        return 0;
+    }
+    MCTDHB_CUDA_TRY(cudaEventRecord(b->ev_fork, b->st));
+    for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++) {
+        if (!(mask >> M & 1)) continue;
+        MCTDHB_CUDA_TRY(cudaStreamWaitEvent(b->side[M], b->ev_fork, 0));
+        if (launch(M, b->side[M])) return -1;
+        MCTDHB_CUDA_TRY(cudaEventRecord(b->ev_join[M], b->side[M]));
+    }
+    for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++)
+        if (mask >> M & 1) MCTDHB_CUDA_TRY(cudaStreamWaitEvent(b->st, b->ev_join[M], 0));
+    return 0;
+}
+
+// the launch sequence of one batch step (captured into the step graph)
+int enqueue_step(mctdhb_batch_s* b, unsigned mask) {
+    cudaStream_t st = b->st;
+    const BatchSlot* S = b->d_slots;
+    const int* nL = b->d_list;  // count in element 0, slots from element 1
+    const int* sl = b->d_list + 1;
+    const BatchTile* V = b->d_vec;
+    const int* nV = cnt_vec(b->d_cnt);
+    const int vgrid = num_sms() * 8, sgrid = b->max_slots;
+    const int lz = b->lz;
+    bt_orbital_kernel<<<sgrid, kBatchOrbThreads, kBatchMaxGrid * sizeof(double), st>>>(S, sl, nL, 0);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    auto hc = [&](int iter) {
+        return per_group(b, mask, [&](int M, cudaStream_t s) {
+            return hc_group(M, S, b->d_hc, hc_off(b->d_cnt), hc_cnt(b->d_cnt), iter, s);
+        });
+    };
+    // Lanczos (multiconfig_lanczos.c:12-90)
+    if (hc(0)) return -1;
+    bt_dot_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV, 0);
+    bt_reduce_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 1, BS_DIAG, 0);
+    for (int i = 0; i < lz - 1; i++) {
+        bt_subdots_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV, i);
+        bt_reduce_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, i + 1, BS_ORTHO, 1);
+        bt_orth_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV, i);
+        bt_norm_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, i);
+        bt_scale_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV, i);
+        MCTDHB_CUDA_TRY(cudaGetLastError());
+        if (hc(i + 1)) return -1;
+        bt_dot_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV, i + 1);
+        bt_reduce_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 1, BS_DIAG + i + 1, 1);
+    }
+    // SIL combination and renormalisation (coefficients_integration.c:59-160)
+    bt_small_kernel<<<sgrid, 32, 0, st>>>(S, sl, nL);
+    bt_combine_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV);
+    bt_norm2_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV);
+    bt_reduce_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 1, BS_MISC + 2, 0);
+    bt_renorm_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    // densities, rho1 synchronisation, energy, stop rules
+    if (per_group(b, mask, [&](int M, cudaStream_t s) {
+            return dens_group(M, S, b->d_dn, dn_off(b->d_cnt), dn_cnt(b->d_cnt), s);
+        }))
+        return -1;
+    bt_dens_finalize_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL);
+    bt_tail_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 0);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int count_graph_kernels(cudaGraph_t g) {
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    cudaGraphGetNodes(g, nodes.data(), &nn);
+    int k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nd, &t);
+        if (t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
+}
+
+int ensure_graph(mctdhb_batch_s* b) {
+    if (b->exec && b->graph_mask == b->present_mask) return 0;
+    drop_graph(b);
+    for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++)
+        if (b->present_mask >> M & 1)
+            if (dens_group(M, nullptr, nullptr, nullptr, nullptr, b->st)) return -1;
+    cudaError_t e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        set_error("batch: capture: %s", cudaGetErrorString(e));
+        return -1;
+    }
+    const int rc = enqueue_step(b, b->present_mask);
+    e = cudaStreamEndCapture(b->st, &b->graph);
+    if (rc) {
+        if (b->graph) cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+        return -1;
+    }
+    if (e != cudaSuccess || cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
+        set_error("batch: graph capture failed: %s", cudaGetErrorString(e));
+        drop_graph(b);
+        return -1;
+    }
+    b->graph_mask = b->present_mask;
+    b->kernels = count_graph_kernels(b->graph);
+    return 0;
+}
+
+uint32_t binom_u32(int n, int k) {
+    if (k > n) return 0;
+    if (k > n - k) k = n - k;
+    uint64_t r = 1;
+    for (int i = 1; i <= k; i++) r = r * (uint64_t)(n - k + i) / (uint64_t)i;
+    return (uint32_t)r;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t mctdhb_batch_job_bytes(const mctdhb_job* job, int lanczos_iter) {
+    if (!job) return 0;
+    JobLayout L;
+    if (job_layout(job->npar, job->norb, job->grid_size, lanczos_iter, L)) return 0;
+    return L.total;
+}
+
+int mctdhb_batch_create(int max_slots, size_t arena_bytes, int lanczos_iter, mctdhb_batch* out) {
+    if (!out) {
+        set_error("mctdhb_batch_create: null output");
+        return -1;
+    }
+    *out = nullptr;
+    if (max_slots < 1 || max_slots > 65536) {
+        set_error("mctdhb_batch_create: %d slots outside 1..65536", max_slots);
+        return -1;
+    }
+    if (lanczos_iter < 2 || lanczos_iter > kBatchMaxLz) {
+        set_error("mctdhb_batch_create: Lanczos dimension %d outside 2..%d", lanczos_iter,
+                  kBatchMaxLz);
+        return -1;
+    }
+    auto* b = new mctdhb_batch_s();
+    b->max_slots = max_slots;
+    b->lz = lanczos_iter;
+    b->arena_bytes = arena_bytes / 256 * 256;
+    b->hs.resize(max_slots);
+    auto fail = [&]() {
+        mctdhb_batch_destroy(b);
+        return -1;
+    };
+    // every job holds at least (lz + 1) nc complex numbers: bounds the tiles
+    const size_t max_rows = b->arena_bytes / ((size_t)(lanczos_iter + 1) * sizeof(double2));
+    b->cap_vec = max_rows / kBatchVecRows + max_slots;
+    b->cap_hc = max_rows / kBatchHcRows + max_slots;
+    b->cap_dn = max_rows / (kBatchDensThreads * 8) + max_slots;
+    if (cudaMalloc(&b->arena, std::max<size_t>(b->arena_bytes, 256)) ||
+        cudaMalloc(&b->d_slots, max_slots * sizeof(BatchSlot)) ||
+        cudaMalloc(&b->d_scal, (size_t)max_slots * BS_TOTAL * sizeof(double2)) ||
+        cudaMalloc(&b->d_flags, (size_t)max_slots * BF_TOTAL * sizeof(int)) ||
+        cudaMalloc(&b->d_list, (max_slots + 1) * sizeof(int)) ||
+        cudaMalloc(&b->d_vec, b->cap_vec * sizeof(BatchTile)) ||
+        cudaMalloc(&b->d_hc, b->cap_hc * sizeof(BatchTile)) ||
+        cudaMalloc(&b->d_dn, b->cap_dn * sizeof(BatchTile)) ||
+        cudaMalloc(&b->d_cnt, kCntInts * sizeof(int)) ||
+        cudaMalloc(&b->d_pro, (2 + kCntInts) * sizeof(int)) ||
+        cudaMalloc(&b->d_pro_dn, kBatchMaxSlices * sizeof(BatchTile)) ||
+        cudaMallocHost(&b->h_list, (max_slots + 1) * sizeof(int)) ||
+        cudaMallocHost(&b->h_vec, b->cap_vec * sizeof(BatchTile)) ||
+        cudaMallocHost(&b->h_hc, b->cap_hc * sizeof(BatchTile)) ||
+        cudaMallocHost(&b->h_dn, b->cap_dn * sizeof(BatchTile)) ||
+        cudaMallocHost(&b->h_cnt, kCntInts * sizeof(int)) ||
+        cudaMallocHost(&b->h_pro, (2 + kCntInts) * sizeof(int)) ||
+        cudaMallocHost(&b->h_pro_dn, kBatchMaxSlices * sizeof(BatchTile)) ||
+        cudaMallocHost(&b->h_flags, (size_t)max_slots * BF_TOTAL * sizeof(int)) ||
+        cudaMallocHost(&b->h_scal, (size_t)max_slots * BS_TOTAL * sizeof(double2)) ||
+        cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) {
+        set_error("mctdhb_batch_create: device allocation of %zu bytes failed", b->arena_bytes);
+        return fail();
+    }
+    for (int M = 0; M < kNumM; M++)
+        if (cudaStreamCreateWithFlags(&b->side[M], cudaStreamNonBlocking) ||
+            cudaEventCreateWithFlags(&b->ev_join[M], cudaEventDisableTiming)) {
+            set_error("mctdhb_batch_create: stream creation failed");
+            return fail();
+        }
+    if (cudaMemset(b->d_flags, 0, (size_t)max_slots * BF_TOTAL * sizeof(int)) ||
+        cudaMemset(b->d_scal, 0, (size_t)max_slots * BS_TOTAL * sizeof(double2)) ||
+        cudaMemset(b->d_slots, 0, max_slots * sizeof(BatchSlot))) {
+        set_error("mctdhb_batch_create: initialisation failed");
+        return fail();
+    }
+    for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++) {
+        const int E = dens_descriptors(M, nullptr);
+        std::vector<int> desc((size_t)5 * E);
+        dens_descriptors(M, desc.data());
+        if (cudaMalloc(&b->d_desc[M], desc.size() * sizeof(int)) ||
+            cudaMemcpy(b->d_desc[M], desc.data(), desc.size() * sizeof(int),
+                       cudaMemcpyHostToDevice)) {
+            set_error("mctdhb_batch_create: descriptor upload failed");
+            return fail();
+        }
+    }
+    if (b->arena_bytes) b->free_ranges[0] = b->arena_bytes;
+    if (rebuild_lists(b)) return fail();
+    *out = b;
+    return 0;
+}
+
+void mctdhb_batch_destroy(mctdhb_batch b) {
+    if (!b) return;
+    if (b->st) cudaStreamSynchronize(b->st);
+    drop_graph(b);
+    cudaFree(b->arena);
+    cudaFree(b->d_slots);
+    cudaFree(b->d_scal);
+    cudaFree(b->d_flags);
+    cudaFree(b->d_list);
+    cudaFree(b->d_vec);
+    cudaFree(b->d_hc);
+    cudaFree(b->d_dn);
+    cudaFree(b->d_cnt);
+    cudaFree(b->d_pro);
+    cudaFree(b->d_pro_dn);
+    for (int M = 0; M < kNumM; M++) {
+        cudaFree(b->d_desc[M]);
+        if (b->side[M]) cudaStreamDestroy(b->side[M]);
+        if (b->ev_join[M]) cudaEventDestroy(b->ev_join[M]);
+    }
+    cudaFreeHost(b->h_list);
+    cudaFreeHost(b->h_vec);
+    cudaFreeHost(b->h_hc);
+    cudaFreeHost(b->h_dn);
+    cudaFreeHost(b->h_cnt);
+    cudaFreeHost(b->h_pro);
+    cudaFreeHost(b->h_pro_dn);
+    cudaFreeHost(b->h_flags);
+    cudaFreeHost(b->h_scal);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
+    if (!b || !job || !slot || !job->pot || !job->orbitals || !job->coef) {
+        set_error("mctdhb_batch_admit: null argument");
+        return -1;
+    }
+    *slot = -1;
+    if (job->rk_order != 2 && job->rk_order != 4 && job->rk_order != 5) {
+        set_error("mctdhb_batch_admit: Runge-Kutta order %d not in {2, 4, 5}", job->rk_order);
+        return -1;
+    }
+    if (!(job->dt > 0) || job->max_steps < 1) {
+        set_error("mctdhb_batch_admit: need dt > 0 and at least one step");
+        return -1;
+    }
+    const double reg = job->reg_fac > 0 ? job->reg_fac : 1e-9;
+    std::lock_guard<std::mutex> lk(b->mu);
+    JobLayout L;
+    if (job_layout(job->npar, job->norb, job->grid_size, b->lz, L)) return -1;
+    int s = -1;
+    for (int i = 0; i < b->max_slots; i++)
+        if (!b->hs[i].used) {
+            s = i;
+            break;
+        }
+    size_t off = 0;
+    if (s < 0 || !arena_take(b, L.total, &off)) return 1;  // no room now
+    HostSlot& h = b->hs[s];
+    h = HostSlot();
+    h.used = true;
+    h.running = true;
+    h.off = off;
+    h.bytes = L.total;
+    h.L = L;
+    const int N = job->npar, M = job->norb, G = job->grid_size;
+    const size_t n = (size_t)M * G;
+    char* base = b->arena + off;
+    auto P = [&](size_t o) { return (void*)(base + o); };
+    BatchSlot& d = h.d;
+    d.N = N;
+    d.M = M;
+    d.G = G;
+    d.imag = job->imagtime ? 1 : 0;
+    d.rk = job->rk_order;
+    d.check_every = job->check_every;
+    d.lz = b->lz;
+    d.nc = L.nc;
+    d.max_steps = job->max_steps;
+    d.vtiles = L.vtiles;
+    d.dslices = L.dslices;
+    d.dchunks = L.dchunks;
+    d.dt = job->dt;
+    d.etol = job->energy_tol;
+    d.reg_fac = reg;
+    d.pdt = d.imag ? make_double2(0.0, -job->dt) : make_double2(job->dt, 0.0);
+    d.ov.M = M;
+    d.ov.G = G;
+    d.ov.periodic = job->periodic ? 1 : 0;
+    d.ov.dx = (job->xf - job->xi) / (G - 1);
+    d.ov.a2 = job->d2coef;
+    d.ov.a1 = make_double2(job->d1coef_re, job->d1coef_im);
+    d.ov.tf = d.imag ? make_double2(0.0, -1.0) : make_double2(1.0, 0.0);
+    d.ov.w = (const double*)P(L.o_w);
+    d.ov.pot = (const double*)P(L.o_pot);
+    d.sp.N = N;
+    d.sp.M = M;
+    d.sp.dim = L.nc;
+    d.sp.T = (const uint32_t*)P(L.o_T);
+    d.sp.sq = (const double*)P(L.o_sq);
+    d.g = (const double*)P(L.o_g);
+    d.desc = b->d_desc[M];
+    d.orb = (double2*)P(L.o_orb);
+    d.stage = (double2*)P(L.o_stage);
+    d.H = (double2*)P(L.o_H);
+    d.Q = (double2*)P(L.o_Q);
+    d.hob = (double2*)P(L.o_hob);
+    d.hint = (double2*)P(L.o_hint);
+    d.tab = (double2*)P(L.o_tab);
+    d.rho1 = (double2*)P(L.o_rho1);
+    d.rho2 = (double2*)P(L.o_rho2);
+    d.rinv = (double2*)P(L.o_rinv);
+    d.work = (double2*)P(L.o_work);
+    d.V = (double2*)P(L.o_V);
+    d.out = (double2*)P(L.o_out);
+    d.part = (double2*)P(L.o_part);
+    d.dpart = (double2*)P(L.o_dpart);
+    d.scal = b->d_scal + (size_t)s * BS_TOTAL;
+    d.flags = b->d_flags + (size_t)s * BF_TOTAL;
+    // host-side tables (the rank table of space_init, Simpson weights)
+    std::vector<uint32_t> T((size_t)(M - 1) * (N + 1));
+    for (int m = 0; m < M - 1; m++)
+        for (int l = 0; l <= N; l++) T[(size_t)m * (N + 1) + l] = binom_u32(l + m, m + 1);
+    std::vector<double> sq(N + 3);
+    for (int x = 0; x < N + 3; x++) sq[x] = std::sqrt((double)x);
+    const std::vector<double> w = simpson_weights(G, d.ov.dx);
+    int fl[BF_TOTAL] = {0};
+    fl[BF_STATE] = SLOT_RUNNING;
+    cudaStream_t st = b->st;
+    auto undo = [&]() {
+        arena_give(b, h.off, h.bytes);
+        h = HostSlot();
+        return -1;
+    };
+    if (cudaStreamSynchronize(st) ||
+        cudaMemcpyAsync(d.orb, job->orbitals, n * sizeof(double2), cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d.V, job->coef, (size_t)L.nc * sizeof(double2), cudaMemcpyHostToDevice,
+                        st) ||
+        cudaMemcpyAsync((void*)d.ov.pot, job->pot, G * sizeof(double), cudaMemcpyHostToDevice,
+                        st) ||
+        cudaMemcpyAsync((void*)d.ov.w, w.data(), G * sizeof(double), cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync((void*)d.sp.T, T.data(), T.size() * sizeof(uint32_t),
+                        cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync((void*)d.sp.sq, sq.data(), sq.size() * sizeof(double),
+                        cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync((void*)d.g, &job->g, sizeof(double), cudaMemcpyHostToDevice, st) ||
+        cudaMemsetAsync(d.scal, 0, BS_TOTAL * sizeof(double2), st) ||
+        cudaMemcpyAsync(d.flags, fl, sizeof(fl), cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(b->d_slots + s, &d, sizeof(BatchSlot), cudaMemcpyHostToDevice, st)) {
+        set_error("mctdhb_batch_admit: upload failed");
+        return undo();
+    }
+    // set-up (mctdhb_solver_set_state): rho1, rho2 and rho1^{-1} of the
+    // initial coefficients, h and g of the initial orbitals, the energy
+    int* hp = b->h_pro;
+    std::memset(hp, 0, (2 + kCntInts) * sizeof(int));
+    hp[0] = 1;
+    hp[1] = s;
+    int* pc = hp + 2;
+    dn_off(pc)[M] = 0;
+    dn_cnt(pc)[M] = L.dslices;
+    for (int q = 0; q < L.dslices; q++) b->h_pro_dn[q] = BatchTile{s, (uint32_t)q};
+    const int* pl = b->d_pro;
+    int* dpc = b->d_pro + 2;
+    if (cudaMemcpyAsync(b->d_pro, hp, (2 + kCntInts) * sizeof(int), cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(b->d_pro_dn, b->h_pro_dn, L.dslices * sizeof(BatchTile),
+                        cudaMemcpyHostToDevice, st)) {
+        set_error("mctdhb_batch_admit: upload failed");
+        return undo();
+    }
+    bt_orbital_kernel<<<1, kBatchOrbThreads, kBatchMaxGrid * sizeof(double), st>>>(
+        b->d_slots, pl + 1, pl, 1);
+    if (dens_group(M, nullptr, nullptr, nullptr, nullptr, st) ||
+        dens_group(M, b->d_slots, b->d_pro_dn, dn_off(dpc), dn_cnt(dpc), st))
+        return undo();
+    bt_dens_finalize_kernel<<<1, kBatchVecThreads, 0, st>>>(b->d_slots, pl + 1, pl);
+    bt_tail_kernel<<<1, kBatchVecThreads, 0, st>>>(b->d_slots, pl + 1, pl, 1);
+    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        set_error("mctdhb_batch_admit: set-up failed: %s",
+                  cudaGetErrorString(e != cudaSuccess ? e : e2));
+        return undo();
+    }
+    b->lists_dirty = true;
+    *slot = s;
+    return 0;
+}
+
+int mctdhb_batch_step(mctdhb_batch b, int nsteps) {
+    if (!b || nsteps < 0) {
+        set_error("mctdhb_batch_step: invalid argument");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (b->lists_dirty && rebuild_lists(b)) return -1;
+    if (b->present_mask == 0) return 0;  // nothing running
+    if (ensure_graph(b)) return -1;
+    for (int i = 0; i < nsteps; i++) MCTDHB_CUDA_TRY(cudaGraphLaunch(b->exec, b->st));
+    return 0;
+}
+
+int mctdhb_batch_sync(mctdhb_batch b) {
+    if (!b) {
+        set_error("mctdhb_batch_sync: null batch");
+        return -1;
+    }
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(b->st));
+    return 0;
+}
+
+int mctdhb_batch_poll(mctdhb_batch b, int* state, uint32_t* steps, double* energy) {
+    if (!b) {
+        set_error("mctdhb_batch_poll: null batch");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    const int S = b->max_slots;
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->h_flags, b->d_flags, (size_t)S * BF_TOTAL * sizeof(int),
+                                    cudaMemcpyDeviceToHost, b->st));
+    if (energy)
+        MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->h_scal, b->d_scal,
+                                        (size_t)S * BS_TOTAL * sizeof(double2),
+                                        cudaMemcpyDeviceToHost, b->st));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(b->st));
+    int running = 0;
+    for (int s = 0; s < S; s++) {
+        HostSlot& h = b->hs[s];
+        const int* f = b->h_flags + (size_t)s * BF_TOTAL;
+        const int stt = h.used ? f[BF_STATE] : SLOT_EMPTY;
+        if (h.used && h.running && stt != SLOT_RUNNING) {
+            h.running = false;
+            b->lists_dirty = true;  // drop the stopped slot's tiles
+        }
+        if (stt == SLOT_RUNNING) running++;
+        if (state) state[s] = stt;
+        if (steps) steps[s] = h.used ? (uint32_t)f[BF_STEPS] : 0u;
+        if (energy) energy[s] = h.used ? b->h_scal[(size_t)s * BS_TOTAL + BS_MISC + 3].x : 0.0;
+    }
+    return running;
+}
+
+int mctdhb_batch_fetch(mctdhb_batch b, int slot, void* orbitals, void* coef, void* rho1,
+                       void* rho2, double* energy, uint32_t* steps, int* converged) {
+    if (!b || slot < 0 || slot >= b->max_slots || !b->hs[slot].used) {
+        set_error("mctdhb_batch_fetch: no job in slot %d", slot);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    const HostSlot& h = b->hs[slot];
+    const BatchSlot& d = h.d;
+    cudaStream_t st = b->st;
+    const size_t n = (size_t)d.M * d.G, M2 = (size_t)d.M * d.M;
+    int fl[BF_TOTAL];
+    double2 sc[BS_TOTAL];
+    if (orbitals)
+        MCTDHB_CUDA_TRY(cudaMemcpyAsync(orbitals, d.orb, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    if (coef)
+        MCTDHB_CUDA_TRY(cudaMemcpyAsync(coef, d.V, (size_t)d.nc * sizeof(double2),
+                                        cudaMemcpyDeviceToHost, st));
+    if (rho1)
+        MCTDHB_CUDA_TRY(cudaMemcpyAsync(rho1, d.rho1, M2 * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    if (rho2)
+        MCTDHB_CUDA_TRY(cudaMemcpyAsync(rho2, d.rho2, M2 * M2 * sizeof(double2),
+                                        cudaMemcpyDeviceToHost, st));
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(fl, d.flags, sizeof(fl), cudaMemcpyDeviceToHost, st));
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(sc, d.scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (energy) *energy = sc[BS_MISC + 3].x;
+    if (steps) *steps = (uint32_t)fl[BF_STEPS];
+    if (converged) *converged = fl[BF_CONV];
+    return 0;
+}
+
+int mctdhb_batch_release(mctdhb_batch b, int slot) {
+    if (!b || slot < 0 || slot >= b->max_slots || !b->hs[slot].used) {
+        set_error("mctdhb_batch_release: no job in slot %d", slot);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    HostSlot& h = b->hs[slot];
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(b->st));  // no step in flight reads the region
+    const int fl[BF_TOTAL] = {0};
+    MCTDHB_CUDA_TRY(cudaMemcpy(b->d_flags + (size_t)slot * BF_TOTAL, fl, sizeof(fl),
+                               cudaMemcpyHostToDevice));
+    arena_give(b, h.off, h.bytes);
+    h = HostSlot();
+    b->lists_dirty = true;
+    return 0;
+}
+
+size_t mctdhb_batch_free_bytes(mctdhb_batch b) {
+    if (!b) return 0;
+    std::lock_guard<std::mutex> lk(b->mu);
+    size_t best = 0;
+    for (auto& r : b->free_ranges) best = std::max(best, r.second);
+    return best;
+}
+
+int mctdhb_batch_kernel_count(mctdhb_batch b) { return b ? b->kernels : 0; }
+
+void* mctdhb_batch_stream(mctdhb_batch b) { return b ? (void*)b->st : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,545 @@
+// batch_kernels.cu -- the slot-level and vector kernels of the batched engine
+// (batch.h).  Per slot, one step is the full step of the single-system
+// solver (driver.c:159-201):
+//   bt_orbital_kernel   one block per slot: Runge-Kutta step of the orbital
+//                       equation with the slot's rho1^{-1} and rho2,
+//                       Gram-Schmidt in imaginary time, h_kl and g_ksql of the
+//                       new orbitals, the packed H.C table, Lanczos set-up
+//   Lanczos             hc_batch_kernel (per M) and the vector kernels below,
+//                       multiconfig_lanczos.c:12-90 operation for operation
+//   SIL                 tridiagonal eigenproblem, C = V U exp(-i D dt) U^T e1,
+//                       renormalisation in imaginary time
+//                       (coefficients_integration.c:59-160)
+//   densities           dens_batch_kernel (per M) + bt_dens_finalize_kernel
+//   bt_tail_kernel      rho1 regularisation and inverse (synchronize.c:42-57),
+//                       energy (integrator_monitor.c:56-88), step count and
+//                       the imaginary-time stop rule (driver.c:47-67)
+// Vector kernels walk tiles of kBatchVecRows rows; every per-slot sum is
+// formed from per-tile partials in tile order.
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "batch_kernels.h"
+#include "common.cuh"
+#include "moves.cuh"
+#include "orbital_dev.cuh"
+#include "small_linalg.cuh"
+
+namespace mctdhb {
+
+namespace {
+
+__device__ __forceinline__ bool slot_running(const BatchSlot& S) {
+    return S.flags[BF_STATE] == SLOT_RUNNING;
+}
+
+// ---------------------------------------------------------------------------
+// orbital side, one block per slot
+// ---------------------------------------------------------------------------
+
+// dy/dt of the orbital equation (orbital_integration.c:179-240) for all
+// orbitals y (M x G): H = linear part + interacting part, overlaps
+// P[s][k] = <y_s|H_k> (simple projector, :95-131), out = -i tf (H - sum_s y_s P[s][k]).
+__device__ void bt_rhs(const BatchSlot& S, const double2* __restrict__ y, double2* __restrict__ out,
+                       double2* sP) {
+    const OrbView& o = S.ov;
+    const int M = o.M, G = o.G, n = M * G;
+    double2* H = S.H;
+    const double2* Q = S.Q;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int k = t / G, x = t % G;
+        const double2 lin = linear_at(o, y + (size_t)k * G, x);
+        double2 fx[kBatchMaxOrb];
+        for (int a = 0; a < M; a++) fx[a] = y[(size_t)a * G + x];
+        const double2* Qk = Q + (size_t)k * M * M * M;
+        double2 red = make_double2(0.0, 0.0);
+        for (int s = 0; s < M; s++) {
+            double2 ts = make_double2(0.0, 0.0);
+            for (int l = 0; l < M; l++) {
+                double2 tl = make_double2(0.0, 0.0);
+                for (int q = 0; q < M; q++) tl = cfma(Qk[s + q * M + l * M * M], fx[q], tl);
+                ts = cfma(tl, fx[l], ts);
+            }
+            red = cfma(make_double2(fx[s].x, -fx[s].y), ts, red);
+        }
+        H[t] = cadd(red, lin);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int p = warp; p < M * M; p += nw) {
+        const int s = p / M, k = p % M;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int x = lane; x < G; x += 32) {
+            const double2 t = cfma_conj(y[(size_t)s * G + x], H[(size_t)k * G + x],
+                                        make_double2(0.0, 0.0));
+            acc.x += o.w[x] * t.x;
+            acc.y += o.w[x] * t.y;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) sP[p] = acc;
+    }
+    __syncthreads();
+    const double2 mi_tf = make_double2(o.tf.y, -o.tf.x);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int k = t / G, x = t % G;
+        double2 proj = make_double2(0.0, 0.0);
+        for (int s = 0; s < M; s++) proj = cfma(y[(size_t)s * G + x], sP[s * M + k], proj);
+        const double2 d = make_double2(H[t].x - proj.x, H[t].y - proj.y);
+        out[t] = cmul(mi_tf, d);
+    }
+    __syncthreads();
+}
+
+// out = y + dt sum_j c_j k_j
+struct Combo {
+    int n;
+    int j[5];
+    double c[5];
+};
+
+// (out may be y itself: each point is read before it is written)
+__device__ void bt_combo(const BatchSlot& S, const double2* y, const Combo& cb, double2* out) {
+    const int n = S.ov.M * S.ov.G;
+    const double dt = S.dt;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int q = 0; q < cb.n; q++) {
+            const double2 kv = S.stage[(size_t)cb.j[q] * n + t];
+            s.x += cb.c[q] * kv.x;
+            s.y += cb.c[q] * kv.y;
+        }
+        out[t] = make_double2(y[t].x + dt * s.x, y[t].y + dt * s.y);
+    }
+    __syncthreads();
+}
+
+// Runge-Kutta step of the orbitals in place (orbital_integration.c:284-349)
+// with the named tableaux Heun (2), classical RK4 (4) and Butcher RK5 (5).
+// Stage j lives in stage[j], the stage input in stage[6].
+__device__ void bt_rk_step(const BatchSlot& S, double2* sP) {
+    const int n = S.ov.M * S.ov.G;
+    double2* y = S.orb;
+    double2* w = S.stage + (size_t)6 * n;
+    auto k = [&](int j) { return S.stage + (size_t)j * n; };
+    auto C1 = [](int a, double ca) { Combo c{1, {a}, {ca}}; return c; };
+    switch (S.rk) {
+        case 2:
+            bt_rhs(S, y, k(0), sP);
+            bt_combo(S, y, C1(0, 1.0), w);
+            bt_rhs(S, w, k(1), sP);
+            bt_combo(S, y, Combo{2, {0, 1}, {0.5, 0.5}}, y);
+            break;
+        case 4:
+            bt_rhs(S, y, k(0), sP);
+            bt_combo(S, y, C1(0, 0.5), w);
+            bt_rhs(S, w, k(1), sP);
+            bt_combo(S, y, C1(1, 0.5), w);
+            bt_rhs(S, w, k(2), sP);
+            bt_combo(S, y, C1(2, 1.0), w);
+            bt_rhs(S, w, k(3), sP);
+            bt_combo(S, y, Combo{4, {0, 1, 2, 3}, {1.0 / 6, 2.0 / 6, 2.0 / 6, 1.0 / 6}}, y);
+            break;
+        default:  // 5
+            bt_rhs(S, y, k(0), sP);
+            bt_combo(S, y, C1(0, 0.25), w);
+            bt_rhs(S, w, k(1), sP);
+            bt_combo(S, y, Combo{2, {0, 1}, {0.125, 0.125}}, w);
+            bt_rhs(S, w, k(2), sP);
+            bt_combo(S, y, Combo{2, {1, 2}, {-0.5, 1.0}}, w);
+            bt_rhs(S, w, k(3), sP);
+            bt_combo(S, y, Combo{2, {0, 3}, {3.0 / 16, 9.0 / 16}}, w);
+            bt_rhs(S, w, k(4), sP);
+            bt_combo(S, y,
+                     Combo{5, {0, 1, 2, 3, 4}, {-3.0 / 7, 2.0 / 7, 12.0 / 7, -12.0 / 7, 8.0 / 7}},
+                     w);
+            bt_rhs(S, w, k(5), sP);
+            bt_combo(S, y,
+                     Combo{5, {0, 2, 3, 4, 5}, {7.0 / 90, 32.0 / 90, 12.0 / 90, 32.0 / 90, 7.0 / 90}},
+                     y);
+            break;
+    }
+}
+
+__device__ void bt_periodic(const BatchSlot& S) {
+    const int M = S.ov.M, G = S.ov.G;
+    if (S.ov.periodic && threadIdx.x < M) S.orb[(size_t)threadIdx.x * G + G - 1] = S.orb[(size_t)threadIdx.x * G];
+    __syncthreads();
+}
+
+// h_kl (orbital_matrices.c:22-70): one warp per pair k <= l;
+// g_ksql: one warp per 8 x 8 tensor-core tile (hint_tile)
+__device__ void bt_matrices(const BatchSlot& S) {
+    const OrbView& o = S.ov;
+    const int M = o.M, G = o.G;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const double r = 1.0 / (12 * o.dx);
+    const int npair = M * (M + 1) / 2;
+    for (int p = warp; p < npair; p += nw) {
+        int q = p, k = 0;
+        while (q >= M - k) {
+            q -= M - k;
+            k++;
+        }
+        const int l = k + q;
+        const double2* fk = S.orb + (size_t)k * G;
+        const double2* fl = S.orb + (size_t)l * G;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int x = lane; x < G; x += 32) {
+            const double2 t = hob_integrand(o, fk, fl, x, r);
+            acc.x += o.w[x] * t.x;
+            acc.y += o.w[x] * t.y;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) {
+            if (k == l) {
+                S.hob[k * M + k] = make_double2(acc.x, 0.0);
+            } else {
+                S.hob[k * M + l] = acc;
+                S.hob[l * M + k] = make_double2(acc.x, -acc.y);
+            }
+        }
+    }
+    const int tiles = (M * M + 7) / 8;
+    for (int t = warp; t < tiles * tiles; t += nw) hint_tile(o, S.orb, S.g, S.hint, t, lane);
+    __syncthreads();
+}
+
+}  // namespace
+
+// mode 0: one full orbital step (periodic copy, Runge-Kutta, Gram-Schmidt,
+// periodic copy), then the matrices of the new orbitals;
+// mode 1: the matrices of the orbitals as given (set-up of a new slot)
+__global__ void __launch_bounds__(kBatchOrbThreads)
+    bt_orbital_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                      const int* __restrict__ nlist, int mode) {
+    if ((int)blockIdx.x >= *nlist) return;
+    const BatchSlot& S = slots[list[blockIdx.x]];
+    if (!slot_running(S)) return;
+    extern __shared__ double scan[];  // G doubles (Gram-Schmidt)
+    __shared__ double2 sP[kBatchMaxOrb * kBatchMaxOrb];
+    const int M = S.M;
+    if (mode == 0) {
+        bt_periodic(S);
+        // Q[k][s + qM + lM^2] = g sum_a rinv[k][a] rho2[a, s, q, l]
+        const int M3 = M * M * M, M4 = M3 * M;
+        const double g = *S.g;
+        for (int e = threadIdx.x; e < M4; e += blockDim.x) {
+            const int k = e / M3, sql = e % M3;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int a = 0; a < M; a++) acc = cfma(S.rinv[k * M + a], S.rho2[a + M * sql], acc);
+            S.Q[e] = cscale(acc, g);
+        }
+        __syncthreads();
+        bt_rk_step(S, sP);
+        if (S.imag) {
+            orthonormalize_block(S.ov, S.orb, scan);
+            __syncthreads();
+        }
+        bt_periodic(S);
+    }
+    bt_matrices(S);
+    if (threadIdx.x == 0) {
+        hc_pack_table(M, S.hob, S.hint, S.tab);
+        // Lanczos set-up of this step (multiconfig_lanczos.c:30-41)
+        S.flags[BF_BREAK] = 0;
+        S.flags[BF_ITERS] = S.lz;
+        S.flags[BF_QL] = 0;
+        S.scal[BS_MISC + 0] = make_double2(0.0, 0.0);
+        S.scal[BS_OFFD + S.lz - 1] = make_double2(0.0, 0.0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// vector kernels over tiles of kBatchVecRows rows
+// ---------------------------------------------------------------------------
+#define BT_TILE_LOOP                                                              \
+    const int nt = *ntiles;                                                       \
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {                            \
+        const BatchTile tl = tiles[t];                                            \
+        const BatchSlot& S = slots[tl.slot];                                      \
+        const uint32_t nc = S.nc;                                                 \
+        const uint32_t r0 = tl.idx * (uint32_t)kBatchVecRows;
+#define BT_ROWS(r)                                                                \
+    for (uint32_t r = r0 + threadIdx.x; r < nc && r < r0 + kBatchVecRows; r += kBatchVecThreads)
+
+// part[tile] = <V[i], out>   (alpha_i, multiconfig_lanczos.c:40-41, :83)
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_dot_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                  const int* __restrict__ ntiles, int i) {
+    BT_TILE_LOOP
+    if (!slot_running(S) || S.flags[BF_BREAK]) continue;
+    const double2* v = S.V + (size_t)i * nc;
+    double2 acc = make_double2(0.0, 0.0);
+    BT_ROWS(r) acc = cfma_conj(v[r], S.out[r], acc);
+    const double2 s = block_sum(acc);
+    if (threadIdx.x == 0) S.part[tl.idx] = s;
+    }
+}
+
+// out -= alpha_i V[i]; part[k * vtiles + tile] = <V[k], out>, k <= i
+// (multiconfig_lanczos.c:46, :57-62)
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_subdots_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                      const int* __restrict__ ntiles, int i) {
+    BT_TILE_LOOP
+    if (!slot_running(S) || S.flags[BF_BREAK]) continue;
+    const double2 alpha = S.scal[BS_DIAG + i];
+    double2 acc[kBatchMaxLz];
+#pragma unroll
+    for (int k = 0; k < kBatchMaxLz; k++) acc[k] = make_double2(0.0, 0.0);
+    BT_ROWS(r) {
+        double2 o = S.out[r];
+        const double2 av = cmul(alpha, S.V[(size_t)i * nc + r]);
+        o.x -= av.x;
+        o.y -= av.y;
+        S.out[r] = o;
+#pragma unroll
+        for (int k = 0; k < kBatchMaxLz; k++)
+            if (k <= i) acc[k] = cfma_conj(S.V[(size_t)k * nc + r], o, acc[k]);
+    }
+    for (int k = 0; k <= i; k++) {
+        const double2 s = block_sum(acc[k]);
+        if (threadIdx.x == 0) S.part[(size_t)k * S.vtiles + tl.idx] = s;
+    }
+    }
+}
+
+// out -= sum_{k<=i} o_k V[k]; part[tile] = |out|^2 (multiconfig_lanczos.c:57-64)
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_orth_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                   const int* __restrict__ ntiles, int i) {
+    BT_TILE_LOOP
+    if (!slot_running(S) || S.flags[BF_BREAK]) continue;
+    double acc = 0.0;
+    BT_ROWS(r) {
+        double2 o = S.out[r];
+        for (int k = 0; k <= i; k++) {
+            const double2 tv = cmul(S.V[(size_t)k * nc + r], S.scal[BS_ORTHO + k]);
+            o.x -= tv.x;
+            o.y -= tv.y;
+        }
+        S.out[r] = o;
+        acc += o.x * o.x + o.y * o.y;
+    }
+    const double2 s = block_sum(make_double2(acc, 0.0));
+    if (threadIdx.x == 0) S.part[tl.idx] = s;
+    }
+}
+
+// V[i+1] = out / beta_i (multiconfig_lanczos.c:74)
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_scale_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                    const int* __restrict__ ntiles, int i) {
+    BT_TILE_LOOP
+    if (!slot_running(S) || S.flags[BF_BREAK]) continue;
+    const double inv = S.scal[BS_MISC + 1].x;
+    BT_ROWS(r) {
+        const double2 o = S.out[r];
+        S.V[(size_t)(i + 1) * nc + r] = make_double2(o.x * inv, o.y * inv);
+    }
+    }
+}
+
+// C = sum_j y_j V[j] over the vectors built (coefficients_integration.c:127-154);
+// C is V[0], overwritten row by row after its own rows are read
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_combine_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                      const int* __restrict__ ntiles) {
+    BT_TILE_LOOP
+    if (!slot_running(S)) continue;
+    const int it = S.flags[BF_ITERS];
+    BT_ROWS(r) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int j = 0; j < it; j++) s = cfma(S.V[(size_t)j * nc + r], S.scal[BS_Y + j], s);
+        S.V[r] = s;
+    }
+    }
+}
+
+// part[tile] = |C|^2
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_norm2_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                    const int* __restrict__ ntiles) {
+    BT_TILE_LOOP
+    if (!slot_running(S) || !S.imag) continue;
+    double acc = 0.0;
+    BT_ROWS(r) acc += S.V[r].x * S.V[r].x + S.V[r].y * S.V[r].y;
+    const double2 s = block_sum(make_double2(acc, 0.0));
+    if (threadIdx.x == 0) S.part[tl.idx] = s;
+    }
+}
+
+// C /= |C| (imaginary time, coefficients_integration.c:156-159)
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_renorm_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                     const int* __restrict__ ntiles) {
+    BT_TILE_LOOP
+    if (!slot_running(S) || !S.imag) continue;
+    const double rn = 1.0 / sqrt(S.scal[BS_MISC + 2].x);
+    BT_ROWS(r) {
+        S.V[r].x *= rn;
+        S.V[r].y *= rn;
+    }
+    }
+}
+
+#undef BT_TILE_LOOP
+#undef BT_ROWS
+
+// ---------------------------------------------------------------------------
+// slot kernels: one block per slot of the list
+// ---------------------------------------------------------------------------
+#define BT_SLOT                                                                   \
+    if ((int)blockIdx.x >= *nlist) return;                                        \
+    const BatchSlot& S = slots[list[blockIdx.x]];                                 \
+    if (!slot_running(S)) return;
+
+// fixed-order sum of part[k * vtiles + t] over t, for k < nvals, into
+// scal[dst + k]: threads take strided partial sums, then a tree (256 threads)
+__device__ double2 bt_sum_parts(const double2* part, int ntile) {
+    __shared__ double2 sh[kBatchVecThreads];
+    double2 s = make_double2(0.0, 0.0);
+    for (int b = threadIdx.x; b < ntile; b += blockDim.x) {
+        s.x += part[b].x;
+        s.y += part[b].y;
+    }
+    __syncthreads();
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sh[threadIdx.x].x += sh[threadIdx.x + o].x;
+            sh[threadIdx.x].y += sh[threadIdx.x + o].y;
+        }
+        __syncthreads();
+    }
+    return sh[0];
+}
+
+// scal[dst + k] = sum_t part[k * vtiles + t], k < nvals.  skip_break: the
+// value belongs to a Lanczos iteration a breakdown has cancelled.
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_reduce_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                     const int* __restrict__ nlist, int nvals, int dst, int skip_break) {
+    BT_SLOT
+    if (skip_break && S.flags[BF_BREAK]) return;
+    for (int k = 0; k < nvals; k++) {
+        const double2 s = bt_sum_parts(S.part + (size_t)k * S.vtiles, S.vtiles);
+        if (threadIdx.x == 0) S.scal[dst + k] = s;
+        __syncthreads();
+    }
+}
+
+// beta_i = |out|; breakdown when beta_i / max beta < 1e-14 (or beta_i = 0);
+// 1/beta_i for the scaling (multiconfig_lanczos.c:64-74)
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_norm_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                   const int* __restrict__ nlist, int i) {
+    BT_SLOT
+    if (S.flags[BF_BREAK]) return;
+    const double2 s = bt_sum_parts(S.part, S.vtiles);
+    if (threadIdx.x != 0) return;
+    const double beta = sqrt(s.x);
+    S.scal[BS_OFFD + i] = make_double2(beta, 0.0);
+    double mx = S.scal[BS_MISC + 0].x;
+    if (mx < beta) mx = beta;
+    S.scal[BS_MISC + 0].x = mx;
+    if (beta == 0.0 || beta / mx < 1e-14) {
+        S.flags[BF_BREAK] = 1;
+        S.flags[BF_ITERS] = i + 1;
+        return;
+    }
+    S.scal[BS_MISC + 1] = make_double2(1.0 / beta, 0.0);
+}
+
+// y = U exp(-i D pdt) U^T e1 of the tridiagonal (alpha, beta) (implicit QL)
+__global__ void bt_small_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                                const int* __restrict__ nlist) {
+    BT_SLOT
+    if (threadIdx.x != 0) return;
+    const int n = S.flags[BF_ITERS];
+    double d[kBatchMaxLz], e[kBatchMaxLz];
+    for (int k = 0; k < n; k++) {
+        d[k] = S.scal[BS_DIAG + k].x;
+        e[k] = S.scal[BS_OFFD + k].x;
+    }
+    double* z = (double*)(S.scal + BS_Z);
+    S.flags[BF_QL] = tridiag_ql(n, d, e, z);
+    const double2 pdt = S.pdt;
+    double2 aux[kBatchMaxLz];
+    for (int k = 0; k < n; k++) {
+        const double re = d[k] * pdt.y, im = -d[k] * pdt.x;
+        const double mag = exp(re);
+        double sn, cs;
+        sincos(im, &sn, &cs);
+        const double u = z[0 * n + k];
+        aux[k] = make_double2(u * mag * cs, u * mag * sn);
+    }
+    for (int k = 0; k < n; k++) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int j = 0; j < n; j++) {
+            s.x += z[k * n + j] * aux[j].x;
+            s.y += z[k * n + j] * aux[j].y;
+        }
+        S.scal[BS_Y + k] = s;
+    }
+}
+
+// rho1 / rho2: fixed-order sum of the slices, the reference's symmetric fill
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_dens_finalize_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                            const int* __restrict__ nlist) {
+    BT_SLOT
+    const int M = S.M;
+    const int E = dens_nelem(M), EP = (E + 7) / 8 * 8;
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        double2 v = S.dpart[e];
+        for (int b = 1; b < S.dslices; b++) {
+            const double2 p = S.dpart[(size_t)b * EP + e];
+            v.x += p.x;
+            v.y += p.y;
+        }
+        const int* d = S.desc + 5 * e;
+        dens_fill(d[0], d[1], d[2], d[3], d[4], v, M, S.rho1, S.rho2);
+    }
+}
+
+// rho1 regularisation and inverse, energy, step count, stop rules.
+// prologue: set-up of a new slot (no step counted; the energy seeds the
+// imaginary-time stop rule as driver.c:229 does).
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_tail_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                   const int* __restrict__ nlist, int prologue) {
+    BT_SLOT
+    const int M = S.M;
+    if (threadIdx.x == 0) {
+        double* wd = (double*)(S.work + 3 * M * M);
+        S.flags[BF_INFO] = sync_rho1(M, S.rho1, S.rinv, S.reg_fac, S.work, wd);
+    }
+    __syncthreads();
+    const double2 E = energy_block(M, S.rho1, S.rho2, S.hob, S.hint);
+    if (threadIdx.x != 0) return;
+    S.scal[BS_MISC + 3] = E;
+    if (prologue) {
+        S.scal[BS_MISC + 4] = make_double2(E.x / S.N, 0.0);
+        return;
+    }
+    const int steps = S.flags[BF_STEPS] + 1;
+    S.flags[BF_STEPS] = steps;
+    int state = SLOT_RUNNING;
+    if (S.imag && S.check_every > 0 && steps % S.check_every == 0) {
+        // driver.c:47-67: |E/N - prev| < tol * prev
+        const double curr = E.x / S.N, prev = S.scal[BS_MISC + 4].x;
+        if (fabs(curr - prev) < S.etol * prev) {
+            state = SLOT_DONE;
+            S.flags[BF_CONV] = 1;
+        }
+        S.scal[BS_MISC + 4] = make_double2(curr, 0.0);
+    }
+    if ((uint32_t)steps >= S.max_steps) state = SLOT_DONE;
+    S.flags[BF_STATE] = state;
+}
+
+#undef BT_SLOT
+
+}  // namespace mctdhb

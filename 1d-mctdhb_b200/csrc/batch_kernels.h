@@ -1,0 +1,44 @@
+// batch_kernels.h -- launch interface of batch_kernels.cu (slot and vector
+// kernels of the batched engine).  Tile kernels take a tile list and its
+// device count; slot kernels a slot list and its device count.
+#pragma once
+#include "batch.h"
+
+namespace mctdhb {
+
+__global__ void bt_orbital_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                                  const int* __restrict__ nlist, int mode);
+__global__ void bt_dot_kernel(const BatchSlot* __restrict__ slots,
+                              const BatchTile* __restrict__ tiles, const int* __restrict__ ntiles,
+                              int i);
+__global__ void bt_subdots_kernel(const BatchSlot* __restrict__ slots,
+                                  const BatchTile* __restrict__ tiles,
+                                  const int* __restrict__ ntiles, int i);
+__global__ void bt_orth_kernel(const BatchSlot* __restrict__ slots,
+                               const BatchTile* __restrict__ tiles, const int* __restrict__ ntiles,
+                               int i);
+__global__ void bt_scale_kernel(const BatchSlot* __restrict__ slots,
+                                const BatchTile* __restrict__ tiles,
+                                const int* __restrict__ ntiles, int i);
+__global__ void bt_combine_kernel(const BatchSlot* __restrict__ slots,
+                                  const BatchTile* __restrict__ tiles,
+                                  const int* __restrict__ ntiles);
+__global__ void bt_norm2_kernel(const BatchSlot* __restrict__ slots,
+                                const BatchTile* __restrict__ tiles,
+                                const int* __restrict__ ntiles);
+__global__ void bt_renorm_kernel(const BatchSlot* __restrict__ slots,
+                                 const BatchTile* __restrict__ tiles,
+                                 const int* __restrict__ ntiles);
+__global__ void bt_reduce_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                                 const int* __restrict__ nlist, int nvals, int dst, int skip_break);
+__global__ void bt_norm_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                               const int* __restrict__ nlist, int i);
+__global__ void bt_small_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                                const int* __restrict__ nlist);
+__global__ void bt_dens_finalize_kernel(const BatchSlot* __restrict__ slots,
+                                        const int* __restrict__ list,
+                                        const int* __restrict__ nlist);
+__global__ void bt_tail_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                               const int* __restrict__ nlist, int prologue);
+
+}  // namespace mctdhb

@@ -1,0 +1,8 @@
+// batch_m2.cu -- batched H.C and density kernels for 2 orbitals
+#include "batch_tmpl.cuh"
+namespace mctdhb {
+template int hc_batch_launch<2>(const BatchSlot*, const BatchTile*, const int*, const int*, int,
+                                cudaStream_t);
+template int dens_batch_launch<2>(const BatchSlot*, const BatchTile*, const int*, const int*,
+                                  cudaStream_t);
+}  // namespace mctdhb

@@ -49,6 +49,90 @@ __device__ __forceinline__ void flush8(double2 (&v)[8], double2* acc, int lane) 
     }
 }
 
+// Contributions of one row to every density element, reduced across the
+// warp and added to the warp's accumulators wacc[0..EP).  Called by all
+// threads of a block together (the SYNC barriers inside); `live` is false
+// for padding threads past the last row.
+template <int M, int SYNC>
+__device__ __forceinline__ void dens_row(const SpaceView& sp, uint32_t row, bool live,
+                                         const double2* __restrict__ C, double2* wacc,
+                                         int lane) {
+    constexpr int E = dens_nelem(M);
+    constexpr int EP = (E + 7) / 8 * 8;
+    RowState<M> st;
+    double2 ci = make_double2(0.0, 0.0);
+    if (live) {
+        load_row<M>(sp, row, st);
+        ci = __ldg(C + row);
+    } else {
+        static_for<M>([&](auto mi) { st.n[decltype(mi)::value] = 0; });
+        static_for<(M > 1 ? M - 1 : 1)>([&](auto mi) {
+            constexpr int m = decltype(mi)::value;
+            st.F[m][0] = st.F[m][1] = st.F[m][2] = st.F[m][3] = 0;
+        });
+    }
+    double sq0[M], sq1[M];
+    static_for<M>([&](auto mi) {
+        constexpr int m = decltype(mi)::value;
+        sq0[m] = __ldg(sp.sq + st.n[m]);
+        sq1[m] = __ldg(sp.sq + st.n[m] + 1);
+    });
+    const double m2 = ci.x * ci.x + ci.y * ci.y;
+    double2 v[8];
+    double2 t = make_double2(0.0, 0.0);  // current single-move product
+
+    static_for<EP>([&](auto ei) {
+        constexpr int e = decltype(ei)::value;
+        double2 x = make_double2(0.0, 0.0);
+        if constexpr (e < E) {
+            constexpr DensElem d = kDensElems<M>.e[e];
+            constexpr int k = d.k, s = d.s, q = d.q, l = d.l;
+            if constexpr (d.kind == D_R1_DIAG) {
+                x.x = m2 * st.n[k];
+            } else if constexpr (d.kind == D_R2_KKKK) {
+                x.x = m2 * (st.n[k] * (st.n[k] - 1));
+            } else if constexpr (d.kind == D_R2_KSKS) {
+                x.x = m2 * (st.n[k] * st.n[s]);
+            } else if constexpr (d.kind == D_R1_OFF) {  // move k -> s
+                t = make_double2(0.0, 0.0);
+                if (st.n[k] > 0) {
+                    const uint32_t j = jumpc<M, k, -1, s, -1>(st, row);
+                    const double2 cj = __ldg(C + j);
+                    t = cscale(cfma_conj(ci, cj, make_double2(0.0, 0.0)), sq0[k] * sq1[s]);
+                }
+                x = t;
+            } else if constexpr (d.kind == D_R2_KKKL) {
+                x = cscale(t, (double)(st.n[k] - 1));
+            } else if constexpr (d.kind == D_R2_KLLL || d.kind == D_R2_KSSL) {
+                x = cscale(t, (double)st.n[s]);
+            } else {
+                bool valid;
+                double sa;
+                if constexpr (k == s) {
+                    valid = st.n[k] >= 2;
+                    sa = valid ? sq0[k] * __ldg(sp.sq + st.n[k] - 1) : 0.0;
+                } else {
+                    valid = st.n[k] >= 1 && st.n[s] >= 1;
+                    sa = sq0[k] * sq0[s];
+                }
+                if (valid) {
+                    const uint32_t j = jumpc<M, k, s, q, l>(st, row);
+                    const double2 cj = __ldg(C + j);
+                    double sb;
+                    if constexpr (q == l)
+                        sb = sq1[q] * __ldg(sp.sq + st.n[q] + 2);
+                    else
+                        sb = sq1[q] * sq1[l];
+                    x = cscale(cfma_conj(ci, cj, make_double2(0.0, 0.0)), sa * sb);
+                }
+            }
+        }
+        v[e % 8] = x;
+        if constexpr (e % 8 == 7) flush8(v, wacc + (e / 8) * 8, lane);
+        if constexpr (SYNC > 0 && e % SYNC == SYNC - 1) __syncthreads();
+    });
+}
+
 // Rows are dealt to blocks of DENS_BLOCK threads in a block-uniform loop, so
 // SYNC > 0 can put a block barrier every SYNC elements (the warps then walk
 // the unrolled code together and share instruction-cache lines, as in the
@@ -76,78 +160,7 @@ __global__ void __launch_bounds__(DENS_BLOCK, MINB)
          bbase += gridDim.x * DENS_BLOCK) {
         const uint32_t row = bbase + threadIdx.x;
         const bool live = row < sp.dim;
-        RowState<M> st;
-        double2 ci = make_double2(0.0, 0.0);
-        if (live) {
-            load_row<M>(sp, row, st);
-            ci = __ldg(C + row);
-        } else {
-            static_for<M>([&](auto mi) { st.n[decltype(mi)::value] = 0; });
-            static_for<(M > 1 ? M - 1 : 1)>([&](auto mi) {
-                constexpr int m = decltype(mi)::value;
-                st.F[m][0] = st.F[m][1] = st.F[m][2] = st.F[m][3] = 0;
-            });
-        }
-        double sq0[M], sq1[M];
-        static_for<M>([&](auto mi) {
-            constexpr int m = decltype(mi)::value;
-            sq0[m] = __ldg(sp.sq + st.n[m]);
-            sq1[m] = __ldg(sp.sq + st.n[m] + 1);
-        });
-        const double m2 = ci.x * ci.x + ci.y * ci.y;
-        double2 v[8];
-        double2 t = make_double2(0.0, 0.0);  // current single-move product
-
-        static_for<EP>([&](auto ei) {
-            constexpr int e = decltype(ei)::value;
-            double2 x = make_double2(0.0, 0.0);
-            if constexpr (e < E) {
-                constexpr DensElem d = kDensElems<M>.e[e];
-                constexpr int k = d.k, s = d.s, q = d.q, l = d.l;
-                if constexpr (d.kind == D_R1_DIAG) {
-                    x.x = m2 * st.n[k];
-                } else if constexpr (d.kind == D_R2_KKKK) {
-                    x.x = m2 * (st.n[k] * (st.n[k] - 1));
-                } else if constexpr (d.kind == D_R2_KSKS) {
-                    x.x = m2 * (st.n[k] * st.n[s]);
-                } else if constexpr (d.kind == D_R1_OFF) {  // move k -> s
-                    t = make_double2(0.0, 0.0);
-                    if (st.n[k] > 0) {
-                        const uint32_t j = jumpc<M, k, -1, s, -1>(st, row);
-                        const double2 cj = __ldg(C + j);
-                        t = cscale(cfma_conj(ci, cj, make_double2(0.0, 0.0)), sq0[k] * sq1[s]);
-                    }
-                    x = t;
-                } else if constexpr (d.kind == D_R2_KKKL) {
-                    x = cscale(t, (double)(st.n[k] - 1));
-                } else if constexpr (d.kind == D_R2_KLLL || d.kind == D_R2_KSSL) {
-                    x = cscale(t, (double)st.n[s]);
-                } else {
-                    bool valid;
-                    double sa;
-                    if constexpr (k == s) {
-                        valid = st.n[k] >= 2;
-                        sa = valid ? sq0[k] * __ldg(sp.sq + st.n[k] - 1) : 0.0;
-                    } else {
-                        valid = st.n[k] >= 1 && st.n[s] >= 1;
-                        sa = sq0[k] * sq0[s];
-                    }
-                    if (valid) {
-                        const uint32_t j = jumpc<M, k, s, q, l>(st, row);
-                        const double2 cj = __ldg(C + j);
-                        double sb;
-                        if constexpr (q == l)
-                            sb = sq1[q] * __ldg(sp.sq + st.n[q] + 2);
-                        else
-                            sb = sq1[q] * sq1[l];
-                        x = cscale(cfma_conj(ci, cj, make_double2(0.0, 0.0)), sa * sb);
-                    }
-                }
-            }
-            v[e % 8] = x;
-            if constexpr (e % 8 == 7) flush8(v, wacc + (e / 8) * 8, lane);
-            if constexpr (SYNC > 0 && e % SYNC == SYNC - 1) __syncthreads();
-        });
+        dens_row<M, SYNC>(sp, row, live, C, wacc, lane);
     }
     __syncthreads();
     for (int e = threadIdx.x; e < EP; e += DENS_BLOCK) {

@@ -135,39 +135,7 @@ __global__ void dens_finalize_kernel(int M, int E, int EP, int nblocks,
     }
     const int kind = desc[5 * e], k = desc[5 * e + 1], s = desc[5 * e + 2], q = desc[5 * e + 3],
               l = desc[5 * e + 4];
-    const double2 c = make_double2(v.x, -v.y);
-    const int M2 = M * M, M3 = M2 * M;
-    auto R = [&](int a, int b, int cc, int d) -> double2& { return rho2[a + b * M + cc * M2 + d * M3]; };
-    switch (kind) {
-        case D_R1_DIAG: rho1[k * M + k] = v; break;
-        case D_R2_KKKK: R(k, k, k, k) = v; break;
-        case D_R2_KSKS:
-            R(k, s, k, s) = v; R(s, k, k, s) = v; R(s, k, s, k) = v; R(k, s, s, k) = v;
-            break;
-        case D_R1_OFF:  // (k, l) stored as (k, s=l)
-            rho1[k * M + s] = v;
-            rho1[s * M + k] = c;
-            break;
-        case D_R2_KKKL:
-            R(k, k, k, l) = v; R(k, k, l, k) = v; R(l, k, k, k) = c; R(k, l, k, k) = c;
-            break;
-        case D_R2_KLLL:  // (k, l, l, l) stored as (k, s=l, q=l, l)
-            R(k, l, l, l) = v; R(l, k, l, l) = v; R(l, l, l, k) = c; R(l, l, k, l) = c;
-            break;
-        case D_R2_KSSL:
-            R(k, s, s, l) = v; R(s, k, s, l) = v; R(s, k, l, s) = v; R(k, s, l, s) = v;
-            R(l, s, s, k) = c; R(s, l, s, k) = c; R(s, l, k, s) = c; R(l, s, k, s) = c;
-            break;
-        case D_R2_KKQQ:
-            R(k, k, q, q) = v; R(q, q, k, k) = c;
-            break;
-        case D_R2_KKQL:
-            R(k, k, q, l) = v; R(k, k, l, q) = v; R(l, q, k, k) = c; R(q, l, k, k) = c;
-            break;
-        case D_R2_KSQL:
-            R(k, s, q, l) = v; R(s, k, q, l) = v; R(k, s, l, q) = v; R(s, k, l, q) = v;
-            break;
-    }
+    dens_fill(kind, k, s, q, l, v, M, rho1, rho2);
 }
 
 int dens_descriptors(int M, int* desc) {

@@ -35,41 +35,9 @@ namespace mctdhb {
 __global__ void hc_prep_kernel(int M, const double2* __restrict__ hob,
                                const double2* __restrict__ hint,
                                double2* __restrict__ tab) {
-    const int M2 = M * M, M3 = M2 * M;
-    auto g = [&](int a, int b, int c, int d) { return hint[a + b * M + c * M2 + d * M3]; };
-    const int nd = hc_ndiag(M), ns = hc_nsingle(M);
     // one thread does the (tiny) enumeration in order; the table is a few KB
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    int p = 0;
-    for (int k = 0; k < M; k++) tab[p++] = hob[k * M + k];
-    for (int k = 0; k < M; k++) tab[p++] = cscale(g(k, k, k, k), 0.5);
-    for (int k = 0; k < M; k++)
-        for (int s = k + 1; s < M; s++) tab[p++] = cscale(g(k, s, k, s), 2.0);
-    for (int k = 0; k < M; k++)
-        for (int l = 0; l < M; l++) {
-            if (l == k) continue;
-            double2 gk = g(k, k, k, l);
-            double2 h = hob[k * M + l];
-            tab[p++] = make_double2(h.x - gk.x, h.y - gk.y);
-            for (int s = 0; s < M; s++) {
-                if (s == k)
-                    tab[p++] = gk;
-                else if (s == l)
-                    tab[p++] = g(k, l, l, l);
-                else
-                    tab[p++] = cscale(g(k, s, s, l), 2.0);
-            }
-        }
-    (void)nd;
-    (void)ns;
-    for (int k = 0; k < M; k++)
-        for (int s = k; s < M; s++)
-            for (int q = 0; q < M; q++)
-                for (int l = q; l < M; l++) {
-                    if (q == k || q == s || l == k || l == s) continue;
-                    double f = (k == s && q == l) ? 0.5 : ((k == s || q == l) ? 1.0 : 2.0);
-                    tab[p++] = cscale(g(k, s, q, l), f);
-                }
+    hc_pack_table(M, hob, hint, tab);
 }
 
 // ---------------------------------------------------------------------------

@@ -39,12 +39,96 @@ __device__ __forceinline__ void zero_row(RowState<M>& st) {
     });
 }
 
+// H.C of one row: the diagonal plus every distinct neighbour reached by one
+// or two moves.  Called by all threads of a block together (the SYNC
+// barriers inside); `live` is false for padding threads past the last row.
+template <int M, int SYNC>
+__device__ __forceinline__ double2 hc_row(const SpaceView& sp, uint32_t row, bool live,
+                                          const double2* __restrict__ C,
+                                          const double2* __restrict__ tab) {
+    constexpr int NMOVE = HcMoveList<M>::N;
+    RowState<M> st;
+    if (live)
+        load_row<M>(sp, row, st);
+    else
+        zero_row<M>(st);
+    double sq0[M], sq1[M];
+    static_for<M>([&](auto mi) {
+        constexpr int m = decltype(mi)::value;
+        sq0[m] = __ldg(sp.sq + st.n[m]);
+        sq1[m] = __ldg(sp.sq + st.n[m] + 1);
+    });
+    const double2 ci = live ? __ldg(C + row) : make_double2(0.0, 0.0);
+
+    // diagonal: h_kk n_k + 1/2 g_kkkk n_k (n_k - 1) + 2 g_ksks n_k n_s
+    double2 dg = make_double2(0.0, 0.0);
+    static_for<M>([&](auto ki) {
+        constexpr int k = decltype(ki)::value;
+        dg = cadd(dg, cscale(tab[k], (double)st.n[k]));
+        dg = cadd(dg, cscale(tab[M + k], (double)(st.n[k] * (st.n[k] - 1))));
+        static_for<M>([&](auto si) {
+            constexpr int s = decltype(si)::value;
+            if constexpr (s > k) {
+                constexpr int p = 2 * M + k * M - k * (k + 1) / 2 + (s - k - 1);
+                dg = cadd(dg, cscale(tab[p], (double)(st.n[k] * st.n[s])));
+            }
+        });
+    });
+    double2 acc = cmul(dg, ci);
+
+    bool vs = false;
+    double sa = 0.0;
+    double2 as = make_double2(0.0, 0.0);
+    static_for<NMOVE>([&](auto ei) {
+        constexpr int e = decltype(ei)::value;
+        constexpr HcMove mv = kHcMoves<M>.m[e];
+        constexpr int k = mv.k, s = mv.s, q = mv.q, l = mv.l;
+        if constexpr (s < 0) {
+            // single move k -> q
+            if (st.n[k] > 0) {
+                const uint32_t j = jumpc<M, k, -1, q, -1>(st, row);
+                const double2 cj = __ldg(C + j);
+                double2 c = tab[mv.tab];
+                static_for<M>([&](auto xi) {
+                    constexpr int x = decltype(xi)::value;
+                    c = cadd(c, cscale(tab[mv.tab + 1 + x], (double)st.n[x]));
+                });
+                acc = cfma(cscale(c, sq0[k] * sq1[q]), cj, acc);
+            }
+        } else {
+            // double move (k, s) -> (q, l), accumulated per source pair
+            if constexpr (mv.first) {
+                if constexpr (k == s) {
+                    vs = st.n[k] >= 2;
+                    sa = vs ? sq0[k] * __ldg(sp.sq + st.n[k] - 1) : 0.0;
+                } else {
+                    vs = st.n[k] >= 1 && st.n[s] >= 1;
+                    sa = sq0[k] * sq0[s];
+                }
+                as = make_double2(0.0, 0.0);
+            }
+            if (vs) {
+                const uint32_t j = jumpc<M, k, s, q, l>(st, row);
+                const double2 cj = __ldg(C + j);
+                double sb;
+                if constexpr (q == l)
+                    sb = sq1[q] * __ldg(sp.sq + st.n[q] + 2);
+                else
+                    sb = sq1[q] * sq1[l];
+                as = cfma(tab[mv.tab], cscale(cj, sb), as);
+            }
+            if constexpr (mv.last) acc = cadd(acc, cscale(as, sa));
+        }
+        if constexpr (SYNC > 0 && e % SYNC == SYNC - 1) __syncthreads();
+    });
+    return acc;
+}
+
 template <int M, int BLOCK, int SYNC>
 __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     hc_kernel(SpaceView sp, const double2* __restrict__ C, double2* __restrict__ HC,
               const double2* __restrict__ tab_g, HcEpilogue ep) {
     constexpr int TAB = hc_table_size(M);
-    constexpr int NMOVE = HcMoveList<M>::N;
     __shared__ double2 tab[TAB];
     for (int i = threadIdx.x; i < TAB; i += BLOCK) tab[i] = tab_g[i];
     __syncthreads();
@@ -54,81 +138,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1))
     for (uint32_t base = blockIdx.x * BLOCK; base < sp.dim; base += gridDim.x * BLOCK) {
         const uint32_t row = base + threadIdx.x;
         const bool live = row < sp.dim;
-        RowState<M> st;
-        if (live)
-            load_row<M>(sp, row, st);
-        else
-            zero_row<M>(st);
-        double sq0[M], sq1[M];
-        static_for<M>([&](auto mi) {
-            constexpr int m = decltype(mi)::value;
-            sq0[m] = __ldg(sp.sq + st.n[m]);
-            sq1[m] = __ldg(sp.sq + st.n[m] + 1);
-        });
-        const double2 ci = live ? __ldg(C + row) : make_double2(0.0, 0.0);
-
-        // diagonal: h_kk n_k + 1/2 g_kkkk n_k (n_k - 1) + 2 g_ksks n_k n_s
-        double2 dg = make_double2(0.0, 0.0);
-        static_for<M>([&](auto ki) {
-            constexpr int k = decltype(ki)::value;
-            dg = cadd(dg, cscale(tab[k], (double)st.n[k]));
-            dg = cadd(dg, cscale(tab[M + k], (double)(st.n[k] * (st.n[k] - 1))));
-            static_for<M>([&](auto si) {
-                constexpr int s = decltype(si)::value;
-                if constexpr (s > k) {
-                    constexpr int p = 2 * M + k * M - k * (k + 1) / 2 + (s - k - 1);
-                    dg = cadd(dg, cscale(tab[p], (double)(st.n[k] * st.n[s])));
-                }
-            });
-        });
-        double2 acc = cmul(dg, ci);
-
-        bool vs = false;
-        double sa = 0.0;
-        double2 as = make_double2(0.0, 0.0);
-        static_for<NMOVE>([&](auto ei) {
-            constexpr int e = decltype(ei)::value;
-            constexpr HcMove mv = kHcMoves<M>.m[e];
-            constexpr int k = mv.k, s = mv.s, q = mv.q, l = mv.l;
-            if constexpr (s < 0) {
-                // single move k -> q
-                if (st.n[k] > 0) {
-                    const uint32_t j = jumpc<M, k, -1, q, -1>(st, row);
-                    const double2 cj = __ldg(C + j);
-                    double2 c = tab[mv.tab];
-                    static_for<M>([&](auto xi) {
-                        constexpr int x = decltype(xi)::value;
-                        c = cadd(c, cscale(tab[mv.tab + 1 + x], (double)st.n[x]));
-                    });
-                    acc = cfma(cscale(c, sq0[k] * sq1[q]), cj, acc);
-                }
-            } else {
-                // double move (k, s) -> (q, l), accumulated per source pair
-                if constexpr (mv.first) {
-                    if constexpr (k == s) {
-                        vs = st.n[k] >= 2;
-                        sa = vs ? sq0[k] * __ldg(sp.sq + st.n[k] - 1) : 0.0;
-                    } else {
-                        vs = st.n[k] >= 1 && st.n[s] >= 1;
-                        sa = sq0[k] * sq0[s];
-                    }
-                    as = make_double2(0.0, 0.0);
-                }
-                if (vs) {
-                    const uint32_t j = jumpc<M, k, s, q, l>(st, row);
-                    const double2 cj = __ldg(C + j);
-                    double sb;
-                    if constexpr (q == l)
-                        sb = sq1[q] * __ldg(sp.sq + st.n[q] + 2);
-                    else
-                        sb = sq1[q] * sq1[l];
-                    as = cfma(tab[mv.tab], cscale(cj, sb), as);
-                }
-                if constexpr (mv.last) acc = cadd(acc, cscale(as, sa));
-            }
-            if constexpr (SYNC > 0 && e % SYNC == SYNC - 1) __syncthreads();
-        });
-
+        double2 acc = hc_row<M, SYNC>(sp, row, live, C, tab);
         // Lanczos epilogue: out = HC - beta * prev
         if (ep.prev != nullptr && live) {
             const double2 pv = __ldg(ep.prev + row);

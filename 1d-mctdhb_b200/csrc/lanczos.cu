@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include "engine.h"
 #include "kernels.h"
+#include "small_linalg.cuh"
 
 namespace mctdhb {
 
@@ -175,61 +176,6 @@ __global__ void lz_init_kernel(double2* scal, int* iflag, int m) {
         iflag[1] = m;
         iflag[2] = 0;
     }
-}
-
-// Implicit QL with Wilkinson shifts for the symmetric tridiagonal matrix
-// (d, e); eigenvectors accumulate in the columns of row-major z (n x n).
-__device__ int tridiag_ql(int n, double* d, double* e, double* z) {
-    for (int i = 0; i < n * n; i++) z[i] = 0.0;
-    for (int i = 0; i < n; i++) z[i * n + i] = 1.0;
-    if (n < 1) return 0;
-    e[n - 1] = 0.0;
-    for (int l = 0; l < n; l++) {
-        int iter = 0;
-        for (;;) {
-            int m;
-            for (m = l; m < n - 1; m++) {
-                const double dd = fabs(d[m]) + fabs(d[m + 1]);
-                if (fabs(e[m]) <= 2.220446049250313e-16 * dd) break;
-            }
-            if (m == l) break;
-            if (++iter > 60) return l + 1;
-            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-            double r = hypot(g, 1.0);
-            g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
-            double s = 1.0, c = 1.0, p = 0.0;
-            bool deflated = false;
-            for (int i = m - 1; i >= l; i--) {
-                double f = s * e[i];
-                const double b = c * e[i];
-                r = hypot(f, g);
-                e[i + 1] = r;
-                if (r == 0.0) {
-                    d[i + 1] -= p;
-                    e[m] = 0.0;
-                    deflated = true;
-                    break;
-                }
-                s = f / r;
-                c = g / r;
-                g = d[i + 1] - p;
-                r = (d[i] - g) * s + 2.0 * c * b;
-                p = s * r;
-                d[i + 1] = g + p;
-                g = c * r - b;
-                for (int k = 0; k < n; k++) {
-                    f = z[k * n + i + 1];
-                    z[k * n + i + 1] = s * z[k * n + i] + c * f;
-                    z[k * n + i] = c * z[k * n + i] - s * f;
-                }
-            }
-            if (deflated) continue;
-            d[l] -= p;
-            e[l] = g;
-            e[m] = 0.0;
-        }
-    }
-    return 0;
 }
 
 // mode 0: SIL propagator y = U exp(-i D prop_dt) U^T e1

@@ -22,6 +22,8 @@
 #pragma once
 #include <stdint.h>
 
+#include "common.cuh"
+
 namespace mctdhb {
 
 __host__ __device__ constexpr int hc_ndiag(int M) { return 2 * M + M * (M - 1) / 2; }
@@ -89,6 +91,83 @@ __host__ __device__ void for_each_density_element(int M, Fn&& f) {
                         f(D_R2_KSQL, k, s, q, l);
                     }
                 }
+}
+
+
+// Packed H.C coefficient table (layout above) from h (M x M row-major) and
+// g (hint[k + sM + qM^2 + lM^3]); the caller runs it on one thread.
+__device__ inline void hc_pack_table(int M, const double2* __restrict__ hob,
+                                     const double2* __restrict__ hint, double2* __restrict__ tab) {
+    const int M2 = M * M, M3 = M2 * M;
+    auto g = [&](int a, int b, int c, int d) { return hint[a + b * M + c * M2 + d * M3]; };
+    int p = 0;
+    for (int k = 0; k < M; k++) tab[p++] = hob[k * M + k];
+    for (int k = 0; k < M; k++) tab[p++] = cscale(g(k, k, k, k), 0.5);
+    for (int k = 0; k < M; k++)
+        for (int s = k + 1; s < M; s++) tab[p++] = cscale(g(k, s, k, s), 2.0);
+    for (int k = 0; k < M; k++)
+        for (int l = 0; l < M; l++) {
+            if (l == k) continue;
+            double2 gk = g(k, k, k, l);
+            double2 h = hob[k * M + l];
+            tab[p++] = make_double2(h.x - gk.x, h.y - gk.y);
+            for (int s = 0; s < M; s++) {
+                if (s == k)
+                    tab[p++] = gk;
+                else if (s == l)
+                    tab[p++] = g(k, l, l, l);
+                else
+                    tab[p++] = cscale(g(k, s, s, l), 2.0);
+            }
+        }
+    for (int k = 0; k < M; k++)
+        for (int s = k; s < M; s++)
+            for (int q = 0; q < M; q++)
+                for (int l = q; l < M; l++) {
+                    if (q == k || q == s || l == k || l == s) continue;
+                    double f = (k == s && q == l) ? 0.5 : ((k == s || q == l) ? 1.0 : 2.0);
+                    tab[p++] = cscale(g(k, s, q, l), f);
+                }
+}
+
+// Store the summed density element v (descriptor kind, k, s, q, l) into
+// rho1 (M x M row-major) / rho2 (M^4) with the reference's symmetric fill
+// (density_matrices.c:33-50, 86-442).
+__device__ inline void dens_fill(int kind, int k, int s, int q, int l, double2 v, int M,
+                                 double2* __restrict__ rho1, double2* __restrict__ rho2) {
+    const double2 c = make_double2(v.x, -v.y);
+    const int M2 = M * M, M3 = M2 * M;
+    auto R = [&](int a, int b, int cc, int d) -> double2& { return rho2[a + b * M + cc * M2 + d * M3]; };
+    switch (kind) {
+        case D_R1_DIAG: rho1[k * M + k] = v; break;
+        case D_R2_KKKK: R(k, k, k, k) = v; break;
+        case D_R2_KSKS:
+            R(k, s, k, s) = v; R(s, k, k, s) = v; R(s, k, s, k) = v; R(k, s, s, k) = v;
+            break;
+        case D_R1_OFF:  // (k, l) stored as (k, s=l)
+            rho1[k * M + s] = v;
+            rho1[s * M + k] = c;
+            break;
+        case D_R2_KKKL:
+            R(k, k, k, l) = v; R(k, k, l, k) = v; R(l, k, k, k) = c; R(k, l, k, k) = c;
+            break;
+        case D_R2_KLLL:  // (k, l, l, l) stored as (k, s=l, q=l, l)
+            R(k, l, l, l) = v; R(l, k, l, l) = v; R(l, l, l, k) = c; R(l, l, k, l) = c;
+            break;
+        case D_R2_KSSL:
+            R(k, s, s, l) = v; R(s, k, s, l) = v; R(s, k, l, s) = v; R(k, s, l, s) = v;
+            R(l, s, s, k) = c; R(s, l, s, k) = c; R(s, l, k, s) = c; R(l, s, k, s) = c;
+            break;
+        case D_R2_KKQQ:
+            R(k, k, q, q) = v; R(q, q, k, k) = c;
+            break;
+        case D_R2_KKQL:
+            R(k, k, q, l) = v; R(k, k, l, q) = v; R(l, q, k, k) = c; R(q, l, k, k) = c;
+            break;
+        case D_R2_KSQL:
+            R(k, s, q, l) = v; R(s, k, q, l) = v; R(k, s, l, q) = v; R(s, k, l, q) = v;
+            break;
+    }
 }
 
 }  // namespace mctdhb

@@ -3,7 +3,9 @@
 // which calls LAPACK zheev / zhesv through lapack_interface.c:61-163):
 //   * Hermitian eigen-decomposition by cyclic Jacobi rotations,
 //   * Hermitian inverse by Gauss-Jordan elimination with partial pivoting,
-//   * the regularisation A += x exp(-A / x) (lapack_interface.c:126).
+//   * the regularisation A += x exp(-A / x) (lapack_interface.c:126);
+// and the real symmetric tridiagonal eigenproblem of the Lanczos step (in
+// place of LAPACK dstev, multiconfig_lanczos.c:143).
 // Row-major double2 storage; usable from host code and from one device
 // thread.  Results agree with LAPACK to rounding for the well-conditioned
 // one-body density matrices these are applied to.
@@ -159,6 +161,61 @@ __host__ __device__ inline int sync_rho1(int n, double2* rho1, double2* rinv, do
     }
     for (int i = 0; i < n * n; i++) a[i] = rho1[i];
     return herm_inverse(n, a, rinv);
+}
+
+// Implicit QL with Wilkinson shifts for the symmetric tridiagonal matrix
+// (d, e); eigenvectors accumulate in the columns of row-major z (n x n).
+__host__ __device__ inline int tridiag_ql(int n, double* d, double* e, double* z) {
+    for (int i = 0; i < n * n; i++) z[i] = 0.0;
+    for (int i = 0; i < n; i++) z[i * n + i] = 1.0;
+    if (n < 1) return 0;
+    e[n - 1] = 0.0;
+    for (int l = 0; l < n; l++) {
+        int iter = 0;
+        for (;;) {
+            int m;
+            for (m = l; m < n - 1; m++) {
+                const double dd = fabs(d[m]) + fabs(d[m + 1]);
+                if (fabs(e[m]) <= 2.220446049250313e-16 * dd) break;
+            }
+            if (m == l) break;
+            if (++iter > 60) return l + 1;
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = hypot(g, 1.0);
+            g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
+            double s = 1.0, c = 1.0, p = 0.0;
+            bool deflated = false;
+            for (int i = m - 1; i >= l; i--) {
+                double f = s * e[i];
+                const double b = c * e[i];
+                r = hypot(f, g);
+                e[i + 1] = r;
+                if (r == 0.0) {
+                    d[i + 1] -= p;
+                    e[m] = 0.0;
+                    deflated = true;
+                    break;
+                }
+                s = f / r;
+                c = g / r;
+                g = d[i + 1] - p;
+                r = (d[i] - g) * s + 2.0 * c * b;
+                p = s * r;
+                d[i + 1] = g + p;
+                g = c * r - b;
+                for (int k = 0; k < n; k++) {
+                    f = z[k * n + i + 1];
+                    z[k * n + i + 1] = s * z[k * n + i] + c * f;
+                    z[k * n + i] = c * z[k * n + i] - s * f;
+                }
+            }
+            if (deflated) continue;
+            d[l] -= p;
+            e[l] = g;
+            e[m] = 0.0;
+        }
+    }
+    return 0;
 }
 
 }  // namespace mctdhb

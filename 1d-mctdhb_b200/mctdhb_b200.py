@@ -37,6 +37,10 @@ EXPORTED = [
     "mctdhb_dev_sil_step", "mctdhb_dev_hash_table", "mctdhb_dev_single_jump_map",
     "mctdhb_dev_double_jump_chunks", "mctdhb_dev_double_jump_map",
     "mctdhb_dev_density_matrices_noalloc",
+    "mctdhb_batch_create", "mctdhb_batch_destroy", "mctdhb_batch_job_bytes",
+    "mctdhb_batch_free_bytes", "mctdhb_batch_admit", "mctdhb_batch_step", "mctdhb_batch_sync",
+    "mctdhb_batch_poll", "mctdhb_batch_fetch", "mctdhb_batch_release",
+    "mctdhb_batch_kernel_count", "mctdhb_batch_stream",
     "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
     "mctdhb_step_create", "mctdhb_step_launch", "mctdhb_step_kernel_count",
     "mctdhb_step_destroy",
@@ -53,6 +57,17 @@ _lib = None
 
 class MctdhbError(RuntimeError):
     pass
+
+
+class Job(C.Structure):
+    """mctdhb_job of include/mctdhb_gpu.h (one system of the batched engine)"""
+    _fields_ = [("npar", C.c_uint16), ("norb", C.c_uint16), ("grid_size", C.c_int),
+                ("xi", C.c_double), ("xf", C.c_double), ("d2coef", C.c_double),
+                ("d1coef_re", C.c_double), ("d1coef_im", C.c_double), ("periodic", C.c_int),
+                ("imagtime", C.c_int), ("rk_order", C.c_int), ("dt", C.c_double),
+                ("g", C.c_double), ("max_steps", C.c_uint32), ("energy_tol", C.c_double),
+                ("check_every", C.c_int), ("reg_fac", C.c_double),
+                ("pot", C.POINTER(C.c_double)), ("orbitals", C.c_void_p), ("coef", C.c_void_p)]
 
 
 def load(path=LIB_PATH):
@@ -160,6 +175,30 @@ def load(path=LIB_PATH):
     L.mctdhb_solver_device_orbitals.argtypes = [vp]
     L.mctdhb_solver_time.restype = d
     L.mctdhb_solver_time.argtypes = [vp]
+    L.mctdhb_batch_create.restype = i
+    L.mctdhb_batch_create.argtypes = [i, C.c_size_t, i, C.POINTER(vp)]
+    L.mctdhb_batch_destroy.argtypes = [vp]
+    L.mctdhb_batch_job_bytes.restype = C.c_size_t
+    L.mctdhb_batch_job_bytes.argtypes = [C.POINTER(Job), i]
+    L.mctdhb_batch_free_bytes.restype = C.c_size_t
+    L.mctdhb_batch_free_bytes.argtypes = [vp]
+    L.mctdhb_batch_admit.restype = i
+    L.mctdhb_batch_admit.argtypes = [vp, C.POINTER(Job), C.POINTER(i)]
+    L.mctdhb_batch_step.restype = i
+    L.mctdhb_batch_step.argtypes = [vp, i]
+    L.mctdhb_batch_sync.restype = i
+    L.mctdhb_batch_sync.argtypes = [vp]
+    L.mctdhb_batch_poll.restype = i
+    L.mctdhb_batch_poll.argtypes = [vp, vp, vp, vp]
+    L.mctdhb_batch_fetch.restype = i
+    L.mctdhb_batch_fetch.argtypes = [vp, i, vp, vp, vp, vp, C.POINTER(d), C.POINTER(u32),
+                                     C.POINTER(i)]
+    L.mctdhb_batch_release.restype = i
+    L.mctdhb_batch_release.argtypes = [vp, i]
+    L.mctdhb_batch_kernel_count.restype = i
+    L.mctdhb_batch_kernel_count.argtypes = [vp]
+    L.mctdhb_batch_stream.restype = vp
+    L.mctdhb_batch_stream.argtypes = [vp]
     _lib = L
     return L
 
@@ -446,3 +485,111 @@ class DropIn:
         if last_error():
             raise MctdhbError(last_error())
         return cnext, coef, ddiag, doffd
+
+
+class Batch:
+    """The batched engine (include/mctdhb_gpu.h, mctdhb_batch_*): independent
+    systems of uneven size resident in one HBM arena, advanced together by
+    one CUDA graph launch per step.  Jobs are dicts with the mctdhb_job
+    fields; `pot`, `orbitals` and `coef` are numpy arrays."""
+
+    def __init__(self, max_slots, arena_bytes, lanczos_iter=5):
+        L = load()
+        h = C.c_void_p()
+        _check(L.mctdhb_batch_create(max_slots, int(arena_bytes), lanczos_iter, C.byref(h)),
+               "mctdhb_batch_create")
+        self.h, self.max_slots, self.lanczos_iter = h, max_slots, lanczos_iter
+        self.jobs = {}
+
+    def close(self):
+        if self.h:
+            load().mctdhb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def make_job(job):
+        """(ctypes Job, arrays kept alive) from a dict"""
+        keep = {k: np.ascontiguousarray(job[k], dt) for k, dt in
+                (("pot", np.float64), ("orbitals", np.complex128), ("coef", np.complex128))}
+        j = Job()
+        for name, _ in Job._fields_:
+            if name in keep:
+                continue
+            if name in job:
+                setattr(j, name, job[name])
+        d1 = complex(job.get("d1coef", 0j))
+        j.d1coef_re, j.d1coef_im = d1.real, d1.imag
+        if "d2coef" not in job:
+            j.d2coef = -0.5
+        j.pot = keep["pot"].ctypes.data_as(C.POINTER(C.c_double))
+        j.orbitals = keep["orbitals"].ctypes.data
+        j.coef = keep["coef"].ctypes.data
+        return j, keep
+
+    @staticmethod
+    def job_bytes(job, lanczos_iter=5):
+        j, _ = Batch.make_job(job)
+        n = int(load().mctdhb_batch_job_bytes(C.byref(j), lanczos_iter))
+        if n == 0:
+            raise MctdhbError(f"mctdhb_batch_job_bytes: {last_error()}")
+        return n
+
+    def free_bytes(self):
+        return int(load().mctdhb_batch_free_bytes(self.h))
+
+    def admit(self, job):
+        """slot index, or None when the batch has no room now"""
+        j, keep = self.make_job(job)
+        slot = C.c_int(-1)
+        rc = load().mctdhb_batch_admit(self.h, C.byref(j), C.byref(slot))
+        if rc == 1:
+            return None
+        _check(rc, "mctdhb_batch_admit")
+        self.jobs[slot.value] = (int(job["npar"]), int(job["norb"]), int(job["grid_size"]))
+        return slot.value
+
+    def step(self, n=1):
+        _check(load().mctdhb_batch_step(self.h, n), "mctdhb_batch_step")
+
+    def sync(self):
+        _check(load().mctdhb_batch_sync(self.h), "mctdhb_batch_sync")
+
+    def poll(self):
+        """(running count, state[], steps[], energy[]) over the slots"""
+        S = self.max_slots
+        st = np.zeros(S, np.int32)
+        steps = np.zeros(S, np.uint32)
+        en = np.zeros(S, np.float64)
+        n = load().mctdhb_batch_poll(self.h, st.ctypes.data, steps.ctypes.data, en.ctypes.data)
+        if n < 0:
+            raise MctdhbError(f"mctdhb_batch_poll: {last_error()}")
+        return n, st, steps, en
+
+    def fetch(self, slot):
+        N, M, G = self.jobs[slot]
+        dim = int(load().space_dimension(N, M))
+        out = {"orb": np.zeros((M, G), np.complex128), "coef": np.zeros(dim, np.complex128),
+               "rho1": np.zeros((M, M), np.complex128), "rho2": np.zeros(M ** 4, np.complex128)}
+        e = C.c_double()
+        steps = C.c_uint32()
+        conv = C.c_int()
+        _check(load().mctdhb_batch_fetch(self.h, slot, out["orb"].ctypes.data,
+                                         out["coef"].ctypes.data, out["rho1"].ctypes.data,
+                                         out["rho2"].ctypes.data, C.byref(e), C.byref(steps),
+                                         C.byref(conv)), "mctdhb_batch_fetch")
+        out.update(energy=e.value, steps=steps.value, converged=bool(conv.value))
+        return out
+
+    def release(self, slot):
+        _check(load().mctdhb_batch_release(self.h, slot), "mctdhb_batch_release")
+        self.jobs.pop(slot, None)
+
+    @property
+    def kernels(self):
+        return int(load().mctdhb_batch_kernel_count(self.h))

@@ -198,6 +198,68 @@ int mctdhb_dev_double_jump_chunks(mctdhb_space sp, int diff, uint64_t* n_chunks)
 int mctdhb_dev_double_jump_map(mctdhb_space sp, int diff, void* d_strides, void* d_map,
                                void* stream);
 
+/* ---------------------------------------------------------------------- */
+/* Part 5: batched engine -- many independent systems on one GPU          */
+/* ---------------------------------------------------------------------- */
+/* The reference integrates one system per process (driver.c:205-330; its
+ * globals driver.c:15-19 make it single-instance).  These calls have no
+ * counterpart there: each admitted job is one such integration (the step of
+ * mctdhb_propagate_step, driver.c:159-201, FULLSTEP_RUNGEKUTTA + FINITEDIFF
+ * + LANCZOS), and all running jobs advance together, one CUDA graph launch
+ * per step of the whole batch.  A job stops on the device after max_steps
+ * steps or, in imaginary time, by the reference's energy rule checked every
+ * check_every steps (driver.c:47-67 without the eigen-residual test):
+ * |E/N - E_prev/N| < energy_tol * E_prev/N.  A job's results do not depend
+ * on the other jobs of the batch (bit for bit). */
+typedef struct {
+    uint16_t npar, norb;        /* 2 <= norb <= 8 */
+    int      grid_size;         /* 5 .. 4096 points on [xi, xf] */
+    double   xi, xf;
+    double   d2coef;            /* coefficient of d2/dx2 (-1/2 for the standard equation) */
+    double   d1coef_re, d1coef_im;
+    int      periodic;
+    int      imagtime;
+    int      rk_order;          /* 2, 4 or 5 */
+    double   dt;
+    double   g;                 /* contact interaction */
+    uint32_t max_steps;
+    double   energy_tol;        /* imaginary-time stop rule; 0 never stops early */
+    int      check_every;       /* stop-rule period in steps (monitor rate); 0: never */
+    double   reg_fac;           /* rho1 regularisation factor; 0: 1e-9 */
+    const double* pot;          /* grid_size trap values (host) */
+    const void*   orbitals;     /* norb x grid_size complex128, row-major (host) */
+    const void*   coef;         /* space_dimension(npar, norb) complex128 (host) */
+} mctdhb_job;
+
+typedef struct mctdhb_batch_s* mctdhb_batch;
+/* arena_bytes of HBM reserved once for the jobs' state; every job uses
+ * lanczos_iter (2..16) Krylov vectors per step */
+int    mctdhb_batch_create(int max_slots, size_t arena_bytes, int lanczos_iter,
+                           mctdhb_batch* out);
+void   mctdhb_batch_destroy(mctdhb_batch b);
+/* exact arena bytes one job occupies (0 and an error for an invalid job) */
+size_t mctdhb_batch_job_bytes(const mctdhb_job* job, int lanczos_iter);
+/* largest free arena range: a job fits when its bytes are at most this */
+size_t mctdhb_batch_free_bytes(mctdhb_batch b);
+/* 0: admitted into *slot (state uploaded, densities, h, g and energy set up);
+ * 1: no free slot or arena range now (nothing changed); -1: error */
+int    mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot);
+/* enqueue nsteps steps of every running job (asynchronous) */
+int    mctdhb_batch_step(mctdhb_batch b, int nsteps);
+int    mctdhb_batch_sync(mctdhb_batch b);
+/* per slot (arrays of max_slots, each may be NULL): state 0 empty,
+ * 1 running, 2 stopped; steps done; current energy.  Returns the number of
+ * running jobs (synchronises). */
+int    mctdhb_batch_poll(mctdhb_batch b, int* state, uint32_t* steps, double* energy);
+/* a job's orbitals, coefficients, rho1, rho2 (host, each may be NULL),
+ * energy, steps and whether the energy rule stopped it */
+int    mctdhb_batch_fetch(mctdhb_batch b, int slot, void* orbitals, void* coef, void* rho1,
+                          void* rho2, double* energy, uint32_t* steps, int* converged);
+/* frees the slot and its arena range */
+int    mctdhb_batch_release(mctdhb_batch b, int slot);
+int    mctdhb_batch_kernel_count(mctdhb_batch b); /* kernels per step graph */
+void*  mctdhb_batch_stream(mctdhb_batch b);       /* the engine's cudaStream_t */
+
 /* rho1 and rho2 of C, as mctdhb_dev_density_matrices computes them, with no
  * device allocation at all.  This entry point has no counterpart in the
  * reference.  It is for callers that cannot let a library call cudaMalloc

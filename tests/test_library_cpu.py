@@ -97,3 +97,24 @@ def test_invalid_space_rejected():
     assert L.mctdhb_space_create(10, 31, C.byref(h)) == -1
     assert L.mctdhb_space_create(300, 12, C.byref(h)) == -1  # > 2^32 configurations
     assert "32-bit" in mctdhb_b200.last_error()
+
+
+def test_batch_job_bytes_host():
+    """the batched engine's footprint formula is host arithmetic: it needs no
+    GPU, grows with the Fock space and rejects what the engine cannot run"""
+    import mctdhb_b200 as B
+
+    def job(N, M, G):
+        return {"npar": N, "norb": M, "grid_size": G, "xi": -8.0, "xf": 8.0, "periodic": 1,
+                "imagtime": 1, "rk_order": 5, "dt": 0.01, "g": 0.5, "max_steps": 10,
+                "pot": np.zeros(G), "orbitals": np.zeros((M, G), np.complex128),
+                "coef": np.zeros(1, np.complex128)}
+
+    small = B.Batch.job_bytes(job(10, 3, 128), 5)
+    big = B.Batch.job_bytes(job(40, 6, 128), 5)
+    nc = 1221759  # C(45, 5)
+    assert big > 6 * 16 * nc and big < 8 * 16 * nc  # 5 Krylov vectors + work vector dominate
+    assert small > 0 and small % 256 == 0 and big % 256 == 0
+    assert B.Batch.job_bytes(job(40, 6, 1024), 5) > big  # orbital buffers grow with the grid
+    with pytest.raises(B.MctdhbError):
+        B.Batch.job_bytes(job(10, 9, 128), 5)  # the engine runs 2..8 orbitals
