@@ -1,8 +1,9 @@
 """Builds libmctdhb_b200.so (the C ABI of include/mctdhb_gpu.h) for sm_100a.
 
 Every csrc/*.cu file is compiled by nvcc with
-`-gencode arch=compute_100a,code=sm_100a` in parallel, then linked into one
-shared library next to this file.  Works without a GPU (cross-compile).
+`-gencode arch=compute_100a,code=sm_100a` in parallel (an object newer than
+its source and every header is kept), then linked into one shared library
+next to this file.  Works without a GPU (cross-compile).
 
     python build.py [--verbose-ptxas] [--jobs N]
 """
@@ -32,8 +33,17 @@ def nvcc():
     raise RuntimeError("nvcc not found")
 
 
-def compile_one(src, verbose_ptxas):
+def headers_mtime():
+    hs = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+        glob.glob(os.path.join(REPO, "include", "*.h"))
+    return max((os.path.getmtime(h) for h in hs), default=0.0)
+
+
+def compile_one(src, verbose_ptxas, newest_header=0.0):
     obj = os.path.join(OBJ, os.path.basename(src).replace(".cu", ".o"))
+    if not verbose_ptxas and os.path.exists(obj) and \
+            os.path.getmtime(obj) > max(os.path.getmtime(src), newest_header):
+        return obj, ""  # up to date: newer than its source and every header
     cmd = [nvcc(), *ARCH, *FLAGS, "-c", src, "-o", obj]
     if verbose_ptxas:
         cmd += ["-Xptxas", "-v"]
@@ -48,8 +58,9 @@ def build(verbose_ptxas=False, jobs=None, quiet=False):
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
     objs = []
+    newest = headers_mtime()
     with cf.ThreadPoolExecutor(jobs) as ex:
-        for obj, log in ex.map(lambda s: compile_one(s, verbose_ptxas), srcs):
+        for obj, log in ex.map(lambda s: compile_one(s, verbose_ptxas, newest), srcs):
             objs.append(obj)
             if verbose_ptxas and log:
                 sys.stderr.write(log)

@@ -1,4 +1,4 @@
-// batch.cu -- host side of the batched engine (include/mctdhb_gpu.h, part 5):
+// batch.cu -- host side of the batched engine (include/mctdhb_gpu.h, part 3):
 // many independent MCTDHB systems of uneven (N, M, grid) resident in one HBM
 // arena and advanced together, one CUDA graph launch per step of the whole
 // batch.
@@ -804,6 +804,16 @@ size_t mctdhb_batch_free_bytes(mctdhb_batch b) {
 }
 
 int mctdhb_batch_kernel_count(mctdhb_batch b) { return b ? b->kernels : 0; }
+
+int mctdhb_batch_launch_hc(mctdhb_batch b, int norb) {
+    if (!b || norb < kBatchMinOrb || norb > kBatchMaxOrb) {
+        set_error("mctdhb_batch_launch_hc: invalid argument");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (b->lists_dirty && rebuild_lists(b)) return -1;
+    return hc_group(norb, b->d_slots, b->d_hc, hc_off(b->d_cnt), hc_cnt(b->d_cnt), 0, b->st);
+}
 
 void* mctdhb_batch_stream(mctdhb_batch b) { return b ? (void*)b->st : nullptr; }
 

@@ -31,6 +31,9 @@ struct mctdhb_solver_s {
             *d_E = nullptr;
     int* d_info = nullptr;
     cudaStream_t cs = nullptr;
+    // recorded on the caller's stream after each step or phase launch; reads
+    // of the state on `cs` wait for it
+    cudaEvent_t ev_step = nullptr;
     // phase 0: orbital step; phase 1: matrices, SIL, densities
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
@@ -122,6 +125,7 @@ void drop_graphs(mctdhb_solver_s* s) {
 int mctdhb_solver_phase(mctdhb_solver s, int phase, cudaStream_t st) {
     if (build_graphs(s)) return -1;
     MCTDHB_CUDA_TRY(cudaGraphLaunch(s->exec[phase], st));
+    MCTDHB_CUDA_TRY(cudaEventRecord(s->ev_step, st));
     return 0;
 }
 
@@ -170,7 +174,8 @@ int mctdhb_solver_create(uint16_t npar, uint16_t norb, uint16_t grid_size, doubl
         cudaMalloc(&s->d_hint, M4 * sizeof(double2)) || cudaMalloc(&s->d_rho1, M2 * sizeof(double2)) ||
         cudaMalloc(&s->d_rho2, M4 * sizeof(double2)) || cudaMalloc(&s->d_rinv, M2 * sizeof(double2)) ||
         cudaMalloc(&s->d_E, sizeof(double2)) || cudaMalloc(&s->d_info, sizeof(int)) ||
-        cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking)) {
+        cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking) ||
+        cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming)) {
         set_error("mctdhb_solver_create: device allocation failed");
         return fail();
     }
@@ -201,6 +206,7 @@ void mctdhb_solver_destroy(mctdhb_solver s) {
     cudaFree(s->d_E);
     cudaFree(s->d_info);
     if (s->cs) cudaStreamDestroy(s->cs);
+    if (s->ev_step) cudaEventDestroy(s->ev_step);
     orb_release(s->orb);
     mctdhb_space_destroy(s->sp);
     delete s;
@@ -277,6 +283,7 @@ int mctdhb_solver_step(mctdhb_solver s, int nsteps, void* stream) {
         MCTDHB_CUDA_TRY(cudaGraphLaunch(s->exec[1], (cudaStream_t)stream));
         s->t += s->dt;
     }
+    MCTDHB_CUDA_TRY(cudaEventRecord(s->ev_step, (cudaStream_t)stream));
     return 0;
 }
 
@@ -338,6 +345,9 @@ int mctdhb_solver_energy(mctdhb_solver s, double* e) {
         set_error("mctdhb_solver_energy: null argument");
         return -1;
     }
+    std::lock_guard<std::mutex> lk(s->mu);
+    // the steps may run on any caller stream: order after the last one
+    MCTDHB_CUDA_TRY(cudaStreamWaitEvent(s->cs, s->ev_step, 0));
     if (orb_energy(s->M, s->d_rho1, s->d_rho2, s->d_hob, s->d_hint, s->d_E, s->cs)) return -1;
     double2 v;
     MCTDHB_CUDA_TRY(cudaMemcpyAsync(&v, s->d_E, sizeof(v), cudaMemcpyDeviceToHost, s->cs));

@@ -40,7 +40,7 @@ EXPORTED = [
     "mctdhb_batch_create", "mctdhb_batch_destroy", "mctdhb_batch_job_bytes",
     "mctdhb_batch_free_bytes", "mctdhb_batch_admit", "mctdhb_batch_step", "mctdhb_batch_sync",
     "mctdhb_batch_poll", "mctdhb_batch_fetch", "mctdhb_batch_release",
-    "mctdhb_batch_kernel_count", "mctdhb_batch_stream",
+    "mctdhb_batch_kernel_count", "mctdhb_batch_stream", "mctdhb_batch_launch_hc",
     "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
     "mctdhb_step_create", "mctdhb_step_launch", "mctdhb_step_kernel_count",
     "mctdhb_step_destroy",
@@ -199,6 +199,8 @@ def load(path=LIB_PATH):
     L.mctdhb_batch_kernel_count.argtypes = [vp]
     L.mctdhb_batch_stream.restype = vp
     L.mctdhb_batch_stream.argtypes = [vp]
+    L.mctdhb_batch_launch_hc.restype = i
+    L.mctdhb_batch_launch_hc.argtypes = [vp, i]
     _lib = L
     return L
 
@@ -593,3 +595,13 @@ class Batch:
     @property
     def kernels(self):
         return int(load().mctdhb_batch_kernel_count(self.h))
+
+    @property
+    def stream(self):
+        """the engine's CUDA stream as a torch stream"""
+        import torch
+
+        return torch.cuda.ExternalStream(int(load().mctdhb_batch_stream(self.h)))
+
+    def launch_hc(self, norb):
+        _check(load().mctdhb_batch_launch_hc(self.h, norb), "mctdhb_batch_launch_hc")

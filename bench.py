@@ -1,27 +1,45 @@
-"""Benchmark of one MCTDHB time step on B200.
+"""Benchmark of batched MCTDHB on B200.
 
-Workload (default): the N=30 bosons, M=8 orbitals real-time quench
-(nc = 10,295,472 complex128 coefficients, 165 MB per vector), grid of 1024
-points on [-15, 15], trap V = x^2/2 + 4 exp(-x^2/0.5), g = 0.1, Lanczos
-dimension 6, dt = 0.005.  One step = the configurational part of the
-reference's mctdhb_propagate_step (driver.c:186-200): short-iterative-Lanczos
-propagation of the coefficients (6 H.C actions, full reorthogonalisation,
-tridiagonal exponential, recombination) followed by rho1 and rho2 of the new
-coefficients, with h_kl and g_ksql of Hermite-Gaussian orbitals.  The full
-step including the Runge-Kutta orbital update is timed too ("full_step"):
-at this grid and dt the explicit RK5 orbital step is unstable in the
-reference's own method (it diverges within ~5 steps), so only its cost, over
-its first steps, is reported.  Inputs are seeded synthetic data.
+Headline (the batched workload): 256 independent imaginary-time relaxations
+of uneven size -- N ~ U{10..60}, M in {3,4,5,6}, grid in {256, 512, 1024}
+points on [-10, 10], g ~ U(0.01, 1), harmonic or double-well trap by a
+seeded coin, RK5 orbitals, Lanczos dimension 5, energy rule 1e-10 checked
+every step, 5000-step limit -- resident together in the batched engine and
+advanced by one CUDA graph launch per step of the whole batch.  The unit of
+work is one full step (orbitals, h and g, SIL, rho1 and rho2) of one system,
+an "instance-step"; value = instance-steps/s.  Beside it:
+
+  plain       the same jobs advanced one at a time by the plain single-system
+              solver (two CUDA graphs per step), instance-steps/s;
+  roofline    the dominant kernel of a batch step, the batched H.C of one
+              orbital count, against the measured HBM copy bandwidth;
+  quench      the N=30 M=8 real-time quench (nc = 10,295,472, grid 1024 on
+              [-15, 15], double well, g = 0.1, Lanczos 6, dt = 0.005):
+              configurational step (SIL + rho1 + rho2, one CUDA graph) and the
+              H.C kernel's HBM GB/s;
+  serving     a Poisson stream of 70% relaxations and 30% real-time quenches
+              admitted by HBM footprint into the running batch (continuous
+              batching), p50/p99 latency and jobs/s at a sweep of arrival
+              rates, against the same arrivals served one at a time by the
+              plain solver (first come first served, each job's service time
+              measured alone on the GPU);
+  e2e         the batched workload through the public API from host memory:
+              admission (state upload), steps, fetch of every result.
+
+dt: the configured dt (0.01 imaginary, 0.005 real time) capped at
+1.5 / lambda_max, lambda_max = 4 |d2coef| / dx^2 + max V the largest
+eigenvalue of the finite-difference one-body operator, which keeps the
+explicit RK5 orbital step inside its stability region on the finer grids.
+Inputs are seeded synthetic data.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 Prints one JSON line (rank 0).  Multi-GPU: one process per GPU (torchrun),
-each rank advances its own independent system (replicas: a single system
-does not shard; no collective in the data path); value = steps/s summed over
-ranks, timed as the max over ranks.
+each rank runs its own 256-job mix (independent systems shard with no
+collective; weak scaling); value = instance-steps/s summed over ranks, timed
+as the max over ranks.
 """
 import argparse
-import ctypes as C
 import json
 import os
 import statistics
@@ -35,10 +53,18 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "1d-mctdhb_b200"))
 
-N_PAR, N_ORB, LANCZOS_M, DT = 30, 8, 6, 0.005
-GRID, XI, XF, G_INT = 1024, -15.0, 15.0, 0.1
+METRIC = "batched_mctdhb_instance_steps_per_s"
 HBM_FALLBACK = 6650.0
-METRIC = "mctdhb_steps_per_s"
+
+# batched workload
+MIX_N, MIX_SEED = 256, 2024
+BXI, BXF = -10.0, 10.0
+LZ = 5  # DEFAULT_LANCZOS_ITER of the reference
+GRIDS = (256, 512, 1024)
+
+# the N=30 M=8 quench
+N_PAR, N_ORB, Q_LZ, Q_DT = 30, 8, 6, 0.005
+Q_GRID, Q_XI, Q_XF, Q_G = 1024, -15.0, 15.0, 0.1
 
 
 # ---------------------------------------------------------------------------
@@ -60,49 +86,45 @@ def simpson_weights(n, h):
     return w
 
 
-def grid():
-    return np.linspace(XI, XF, GRID)
+_ORB = {}
 
 
-def double_well(x):
-    return 0.5 * x ** 2 + 4.0 * np.exp(-x ** 2 / 0.5)
+def hermite_orbitals(M, G, xi, xf):
+    """Hermite-Gaussian orbitals n = 0..M-1 orthonormalised by Gram-Schmidt
+    in the Simpson metric"""
+    key = (M, G, xi, xf)
+    if key not in _ORB:
+        x = np.linspace(xi, xf, G)
+        w = simpson_weights(G, x[1] - x[0])
+        phi = np.zeros((M, G), np.complex128)
+        hm, hc = np.zeros(G), np.exp(-x ** 2 / 2)
+        for n in range(M):
+            phi[n] = hc
+            hm, hc = hc, (np.sqrt(2.0) * x * hc - np.sqrt(n) * hm) / np.sqrt(n + 1)
+        for i in range(M):
+            for j in range(i):
+                phi[i] -= np.sum(w * phi[j].conj() * phi[i]) * phi[j]
+            phi[i] /= np.sqrt(np.sum(w * np.abs(phi[i]) ** 2))
+        _ORB[key] = phi
+    return _ORB[key]
 
 
-def hermite_orbitals(M=N_ORB):
-    """Hermite-Gaussian orbitals n = 0..M-1, Gram-Schmidt in the Simpson
-    metric, periodic end point equal to the first"""
-    x = grid()
-    w = simpson_weights(GRID, x[1] - x[0])
-    phi = np.zeros((M, GRID), np.complex128)
-    hm, hc = np.zeros(GRID), np.exp(-x ** 2 / 2)
-    for n in range(M):
-        phi[n] = hc
-        hm, hc = hc, (np.sqrt(2.0) * x * hc - np.sqrt(n) * hm) / np.sqrt(n + 1)
-    for i in range(M):
-        for j in range(i):
-            phi[i] -= np.sum(w * phi[j].conj() * phi[i]) * phi[j]
-        phi[i] /= np.sqrt(np.sum(w * np.abs(phi[i]) ** 2))
-    return phi
+def trap(double_well, G, xi, xf):
+    x = np.linspace(xi, xf, G)
+    v = 0.5 * x ** 2
+    return v + 4.0 * np.exp(-x ** 2 / 0.5) if double_well else v
 
 
-def orbital_matrices(phi, g=G_INT):
-    """h_kl (4th-order periodic derivative, Simpson) and g_ksql of `phi`
-    (inputs of the stand-alone kernel timings; the solver computes its own)"""
-    x = grid()
-    dx = x[1] - x[0]
-    w = simpson_weights(GRID, dx)
-    d = (np.roll(phi, 2, 1) - np.roll(phi, -2, 1) +
-         8 * (np.roll(phi, -1, 1) - np.roll(phi, 1, 1))) / (12 * dx)
-    hob = 0.5 * np.einsum("x,ax,bx->ab", w, d.conj(), d) + \
-        np.einsum("x,ax,bx->ab", w * double_well(x), phi.conj(), phi)
-    t = g * np.einsum("x,ax,bx,cx,dx->abcd", w, phi.conj(), phi.conj(), phi, phi)
-    return np.ascontiguousarray(hob), np.ascontiguousarray(t.transpose(3, 2, 1, 0)).reshape(-1)
+def stable_dt(dt, G, pot, xi, xf, d2coef=-0.5):
+    dx = (xf - xi) / (G - 1)
+    lam = 4.0 * abs(d2coef) / dx ** 2 + float(np.max(pot))
+    return min(dt, 1.5 / lam)
 
 
-def coefficients(nc, seed):
-    rng = np.random.default_rng(seed)
-    c = rng.normal(size=nc) + 1j * rng.normal(size=nc)
-    return c / np.linalg.norm(c)
+def dim(N, M):
+    from math import comb
+
+    return comb(N + M - 1, M - 1)
 
 
 def distinct_couplings(N, M):
@@ -121,6 +143,64 @@ def distinct_couplings(N, M):
             tot += cnt * (o * (M - 1) + comb(o, 2) * (M - 2) * (M - 1) // 2 +
                           d2 * (M - 1) * M // 2)
     return tot
+
+
+def coefficients(nc, rng):
+    c = rng.normal(size=nc) + 1j * rng.normal(size=nc)
+    return c / np.linalg.norm(c)
+
+
+def make_job(rng, N, M, G, imag, steps, xi=BXI, xf=BXF, big=False):
+    dw = bool(rng.random() < 0.5)
+    pot = trap(dw, G, xi, xf)
+    g = float(rng.uniform(0.01, 1.0))
+    return {"npar": int(N), "norb": int(M), "grid_size": int(G), "xi": xi, "xf": xf,
+            "periodic": 1, "imagtime": int(imag), "rk_order": 5,
+            "dt": stable_dt(0.01 if imag else 0.005, G, pot, xi, xf), "g": g,
+            "max_steps": int(steps), "energy_tol": 1e-10 if imag else 0.0,
+            "check_every": 1 if imag else 0, "pot": pot,
+            "orbitals": hermite_orbitals(M, G, xi, xf), "coef": coefficients(dim(N, M), rng),
+            "big": big}
+
+
+def mix_jobs(n=MIX_N, seed=MIX_SEED, max_steps=5000):
+    """the batched workload: n imaginary-time relaxations of uneven size"""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(n):
+        N = int(rng.integers(10, 61))
+        M = int(rng.choice([3, 4, 5, 6]))
+        G = int(rng.choice(GRIDS))
+        jobs.append(make_job(rng, N, M, G, True, max_steps))
+    return jobs
+
+
+def served_jobs(njobs, seed=77, imag_steps=5000, real_steps=500, big_frac=0.05, nmax=60):
+    """the served job sequence: [(unit-rate arrival time, job)].  Arrival
+    times are cumulative Exp(1) gaps, divided by the rate for a given rate,
+    so every rate of a sweep serves the same jobs in the same order; 70%
+    imaginary-time relaxations, 30% real-time quenches, big_frac of
+    N=30 M=8 grid 1024 jobs"""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for _ in range(njobs):
+        t += float(rng.exponential(1.0))
+        imag = bool(rng.random() < 0.7)
+        if rng.random() < big_frac:
+            job = make_job(rng, 30, 8, 1024, imag, imag_steps if imag else real_steps,
+                           Q_XI, Q_XF, big=True)
+        else:
+            job = make_job(rng, int(rng.integers(10, nmax + 1)), int(rng.choice([3, 4, 5, 6])),
+                           int(rng.choice(GRIDS)), imag, imag_steps if imag else real_steps)
+        out.append((t, job))
+    return out
+
+
+def mix_summary(jobs):
+    ncs = [dim(j["npar"], j["norb"]) for j in jobs]
+    return {"jobs": len(jobs), "sum_nc": int(sum(ncs)), "max_nc": int(max(ncs)),
+            "by_norb": {str(m): sum(1 for j in jobs if j["norb"] == m) for m in (3, 4, 5, 6)},
+            "by_grid": {str(g): sum(1 for j in jobs if j["grid_size"] == g) for g in GRIDS}}
 
 
 # ---------------------------------------------------------------------------
@@ -186,70 +266,438 @@ def peaks():
 
 
 def ncu_traffic():
-    """per-launch DRAM bytes of the H.C kernel from the committed ncu summary"""
+    """per-launch DRAM bytes of the H.C kernels from the committed ncu summary"""
     try:
         with open(os.path.join(REPO, "profiles", "hc_traffic.json")) as f:
             return json.load(f)
     except (OSError, ValueError):
-        return None
+        return {}
 
 
-def workload_config(args):
-    return {"workload": "real-time quench N=30 M=8 (nc=10295472), grid 1024 on [-15,15], "
-                        "V=x^2/2+4exp(-x^2/0.5), g=0.1, Lanczos 6, dt=0.005, RK5 orbitals",
-            "npar": N_PAR, "norb": N_ORB, "grid": GRID, "lanczos_iter": LANCZOS_M, "dt": DT,
-            "step": "SIL(6 H.C) + rho1 + rho2 (one CUDA graph)",
-            "parallelism": f"replicas{args.gpus}",
-            "l2": "inputs larger than L2 (165 MB coefficient vector, 1 GB of Krylov vectors)"}
+def workload_config(args, jobs):
+    return {"workload": f"batched: {len(jobs)} imaginary-time relaxations, N~U{{10..60}}, "
+                        "M in {3,4,5,6}, grid in {256,512,1024} on [-10,10], g~U(0.01,1), "
+                        "harmonic or double-well trap, RK5 orbitals, Lanczos 5, energy rule "
+                        "1e-10 every step, 5000-step limit, dt=min(0.01, 1.5/lambda_max)",
+            "mix": mix_summary(jobs), "seed": MIX_SEED, "lanczos_iter": LZ,
+            "step": "one full MCTDHB step of every running system: one CUDA graph launch",
+            "parallelism": f"replicas{args.gpus}: each GPU its own mix, no collective",
+            "l2": "inputs larger than L2 (the mix holds ~12 GB of coefficient and Krylov "
+                  "vectors)"}
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle's C restatement on a bounded row sample
+# CPU baseline: the oracle's C restatement on a sample of the jobs
 # ---------------------------------------------------------------------------
-def cpu_step_estimate(hob, hint, rows_per_sample=200000, samples=8, m=LANCZOS_M):
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    from oracle import Oracle
+def oracle_state(O, j):
+    orb = np.ascontiguousarray(j["orbitals"].copy())
+    G = j["grid_size"]
+    dx = (j["xf"] - j["xi"]) / (G - 1)
+    r1, r2, ri = O.sync_density_matrices(j["npar"], j["norb"], j["coef"])
+    return {"orb": orb, "coef": np.ascontiguousarray(j["coef"].copy()),
+            "hob": np.ascontiguousarray(O.orbital_hob(orb, dx, -0.5, 0.0, j["pot"])),
+            "hint": np.ascontiguousarray(O.orbital_hint(orb, dx, j["g"])),
+            "rho1": np.ascontiguousarray(r1), "rho2": np.ascontiguousarray(r2),
+            "rinv": np.ascontiguousarray(ri)}, dx
 
-    O = Oracle()
-    nc = O.dim(N_PAR, N_ORB)
-    c = coefficients(nc, 7)
-    offs = [int(nc * f) for f in np.linspace(0.0, 0.9, samples)]
-    t_hc = t_dn = 0.0
-    for r0 in offs:
+
+def step_bytes(j, m=LZ):
+    """algorithmic bytes of one full step of a job: m H.C launches
+    (32 nc + 16 G each) and the densities (16 nc + 16 G)"""
+    nc, G = dim(j["npar"], j["norb"]), distinct_couplings(j["npar"], j["norb"])
+    return m * (32.0 * nc + 16.0 * G) + 16.0 * nc + 16.0 * G
+
+
+class CpuEstimate:
+    """CPU time of one full step of the whole mix, estimated from full oracle
+    steps of a stratified sample of its jobs.
+
+    The cost of a job's step is heavy-tailed in its size (at N ~ U{10..60},
+    M in {3..6} the 25 largest of 256 jobs hold ~85% of the algorithmic
+    bytes), so the jobs are split into the TOP largest by step_bytes and the
+    rest; each stratum's CPU seconds per algorithmic byte is measured on the
+    jobs sampled from it (ratio estimator) and applied to the stratum's total
+    bytes.  Each sampled job runs one complete oracle step (orbitals, h, g,
+    SIL, rho1, rho2); its set-up (initial densities) is not timed."""
+    TOP = 25
+
+    def __init__(self, jobs, seed):
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        from oracle import Oracle
+
+        self.O = Oracle()
+        self.jobs = jobs
+        self.rng = np.random.default_rng(seed)
+        order = sorted(range(len(jobs)), key=lambda i: -step_bytes(jobs[i]))
+        self.strata = {"large": order[:self.TOP], "rest": order[self.TOP:]}
+        self.total = {h: sum(step_bytes(jobs[i]) for i in ix) for h, ix in self.strata.items()}
+        self.t = {h: 0.0 for h in self.strata}
+        self.b = {h: 0.0 for h in self.strata}
+        self.n = {h: 0 for h in self.strata}
+        self.queue = {h: [] for h in self.strata}
+
+    def _draw(self, h):
+        if not self.queue[h]:
+            self.queue[h] = self.rng.permutation(self.strata[h]).tolist()
+        return self.queue[h].pop()
+
+    def _run(self, h, i):
+        j = self.jobs[i]
+        st, dx = oracle_state(self.O, j)
         t0 = time.perf_counter()
-        O.apply_hamiltonian(N_PAR, N_ORB, c, hob, hint, rows=(r0, r0 + rows_per_sample))
-        t1 = time.perf_counter()
-        O.twobody_dm(N_PAR, N_ORB, c, rows=(r0, r0 + rows_per_sample))
-        t2 = time.perf_counter()
-        t_hc += t1 - t0
-        t_dn += t2 - t1
-    rows = rows_per_sample * samples
-    step_s = (m * t_hc / rows + t_dn / rows) * nc
-    return {"value": 1.0 / step_s, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{samples}x{rows_per_sample} rows of H.C and rho2 (oracle C restatement, "
-                      f"OpenMP, {os.cpu_count()} threads) scaled to {m} H.C + rho2 over "
-                      f"{nc} rows (the orbital part, <1% of a step, is not counted); the "
-                      f"reference itself cannot build its maps at this size",
-            "seconds_per_step": step_s, "sample_seconds": t_hc + t_dn}
+        self.O.propagate_step(st, j["npar"], dx, j["dt"], -0.5, 0.0, j["g"], True,
+                              bool(j["imagtime"]), j["rk_order"], LZ, j["pot"])
+        dt = time.perf_counter() - t0
+        self.t[h] += dt
+        self.b[h] += step_bytes(j)
+        self.n[h] += 1
+        return dt
+
+    def sample(self, n_large=1, rest_budget_s=3.0):
+        """one bounded round: n_large jobs of the large stratum, then jobs of
+        the rest until rest_budget_s seconds of their steps"""
+        for _ in range(n_large):
+            self._run("large", self._draw("large"))
+        spent = 0.0
+        while spent < rest_budget_s:
+            spent += self._run("rest", self._draw("rest"))
+
+    def seconds_per_mix_step(self):
+        return sum(self.t[h] / self.b[h] * self.total[h] for h in self.strata if self.b[h] > 0)
+
+    def value(self):
+        return len(self.jobs) / self.seconds_per_mix_step()
+
+    def describe(self):
+        return {h: {"jobs_in_stratum": len(self.strata[h]), "jobs_timed": self.n[h],
+                    "seconds": self.t[h], "s_per_gb": self.t[h] / self.b[h] * 1e9}
+                for h in self.strata if self.n[h]}
+
+
+def cpu_sample(jobs, seed=5):
+    """the oracle's C restatement (OpenMP, all host threads) on a bounded
+    stratified sample of the mix, scaled to instance-steps/s"""
+    est = CpuEstimate(jobs, seed)
+    est.sample(n_large=1, rest_budget_s=4.0)
+    cores = os.cpu_count()
+    return {"value": est.value(), "unit": "instance-steps/s", "cores": cores, "kind": "port",
+            "seconds": sum(est.t.values()), "strata": est.describe(),
+            "sample": f"full oracle steps (RK5 orbitals, h, g, SIL({LZ}), rho1, rho2; C "
+                      f"restatement, OpenMP on {cores} host threads) of 1 job drawn from the "
+                      f"{CpuEstimate.TOP} largest and of jobs from the rest for ~4 s; each "
+                      f"stratum's seconds per algorithmic byte scaled to its total bytes"}
 
 
 def run_reference(args):
+    """the reference arm: the oracle port on the host cores, same metric"""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    hob, hint = orbital_matrices(hermite_orbitals())
+    jobs = mix_jobs()
+    warm = CpuEstimate(jobs, seed=100)
     for _ in range(args.warmup):
-        cpu_step_estimate(hob, hint, rows_per_sample=5000, samples=2)
-    vals = [cpu_step_estimate(hob, hint, rows_per_sample=50000, samples=8)
-            for _ in range(args.steps)]
-    v = statistics.median(x["value"] for x in vals)
-    base = dict(vals[0], value=v)
+        warm.sample(n_large=0, rest_budget_s=0.5)
+    est = CpuEstimate(jobs, seed=5)
+    for _ in range(args.steps):
+        est.sample(n_large=1, rest_budget_s=2.0)
+    v = est.value()
+    cores = os.cpu_count()
+    base = {"value": v, "unit": "instance-steps/s", "cores": cores, "kind": "port",
+            "seconds": sum(est.t.values()), "strata": est.describe(),
+            "sample": f"per timed step: a full oracle step (C restatement, OpenMP on {cores} "
+                      f"host threads) of 1 job drawn from the {CpuEstimate.TOP} largest of the "
+                      f"mix and of jobs from the rest for ~2 s; pooled over {args.steps} steps, "
+                      f"each stratum's seconds per algorithmic byte scaled to its total bytes"}
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-        "data": "synthetic", "config": workload_config(args), "cpu_baseline": base,
-        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "instance-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * MIX_N / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": workload_config(args, jobs), "cpu_baseline": base,
+        "e2e": {"value": v, "unit": "instance-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# batched engine and the plain path
+# ---------------------------------------------------------------------------
+def arena_bytes(mb, jobs, slack=1.02):
+    return int(sum(mb.Batch.job_bytes(j, LZ) for j in jobs) * slack) + (64 << 20)
+
+
+def batch_hc_roofline(mb, torch, b, jobs, reps=5):
+    """time each orbital count's batched H.C launch on the engine's stream;
+    algorithmic bytes = sum over its jobs of 32 nc + 16 G(N, M)"""
+    st = b.stream
+    out = {}
+    for M in sorted({j["norb"] for j in jobs}):
+        byts = sum(32.0 * dim(j["npar"], M) + 16.0 * distinct_couplings(j["npar"], M)
+                   for j in jobs if j["norb"] == M)
+        b.launch_hc(M)
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(reps):
+            b.launch_hc(M)
+        c.record(st)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(c) / reps
+        out[M] = {"ms_per_launch": ms, "algorithmic_bytes": byts,
+                  "achieved_gbs": byts / (ms / 1000.0) / 1e9}
+    return out
+
+
+def plain_timed(mb, torch, jobs, warmup, steps, compare=None):
+    """the same jobs one at a time through the plain solver: per job, set-up
+    and `warmup` untimed steps, then `steps` steps timed with CUDA events.
+    compare: {job index: total steps} -- those jobs are run on to that many
+    steps in all and their energies returned."""
+    compare = compare or {}
+    stream = torch.cuda.current_stream()
+    total, energies = 0.0, {}
+    for i, j in enumerate(jobs):
+        s = mb.Solver(j["npar"], j["norb"], j["grid_size"], j["xi"], j["xf"], j["dt"],
+                      bool(j["imagtime"]), j["rk_order"], LZ, periodic=bool(j["periodic"]))
+        s.set_potential(j["pot"])
+        s.set_interaction(j["g"])
+        s.set_state(j["orbitals"], j["coef"])
+        s.step(warmup, stream)
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.step(steps, stream)
+        c.record(stream)
+        torch.cuda.synchronize()
+        total += a.elapsed_time(c) / 1000.0
+        if i in compare:
+            extra = compare[i] - warmup - steps
+            if extra > 0:
+                s.step(extra, stream)
+            energies[i] = s.energy().real
+        s.close()
+    n = len(jobs) * steps
+    return {"value": n / total, "unit": "instance-steps/s", "seconds": total,
+            "instance_steps": n,
+            "what": f"the same jobs one at a time through mctdhb_solver (two CUDA graphs per "
+                    f"step), {steps} timed steps per job after set-up and {warmup} untimed"}, \
+        energies
+
+
+def e2e_batch(mb, torch, jobs, steps):
+    """end to end through the public API from host memory: admit every job
+    (state uploaded), `steps` steps, fetch every job's orbitals,
+    coefficients and densities; wall clock around all of it"""
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b = mb.Batch(len(jobs), arena_bytes(mb, jobs), LZ)
+    slots = [b.admit(j) for j in jobs]
+    b.step(steps)
+    outs = [b.fetch(s) for s in slots]
+    t1 = time.perf_counter()
+    b.close()
+    h2d = sum(16 * (dim(j["npar"], j["norb"]) + j["norb"] * j["grid_size"]) + 8 * j["grid_size"]
+              for j in jobs)
+    d2h = sum(o["coef"].nbytes + o["orb"].nbytes + o["rho1"].nbytes + o["rho2"].nbytes
+              for o in outs)
+    return {"value": len(jobs) * steps / (t1 - t0), "unit": "instance-steps/s",
+            "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+            "seconds": t1 - t0, "steps": steps,
+            "path": "mctdhb_batch_admit (host state) + mctdhb_batch_step + mctdhb_batch_fetch, "
+                    "wall clock"}
+
+
+# ---------------------------------------------------------------------------
+# serving: continuous batching against one-at-a-time
+# ---------------------------------------------------------------------------
+def serve_batched(mb, arrivals, arena, max_slots=512, steps_per_poll=2):
+    """continuous batching in real time: jobs are admitted (first come first
+    served) once arrived and once they fit in the arena, advanced together
+    by the batch step, retired when they stop.  Returns latencies, the
+    makespan and the jobs' final energies."""
+    b = mb.Batch(max_slots, arena, LZ)
+    pending = list(enumerate(arrivals))
+    waiting, running, lat, energy = [], {}, {}, {}
+    t_start = time.perf_counter()
+    while pending or waiting or running:
+        now = time.perf_counter() - t_start
+        while pending and pending[0][1][0] <= now:
+            waiting.append(pending.pop(0))
+        while waiting:
+            s = b.admit(waiting[0][1][1])
+            if s is None:
+                break
+            running[s] = waiting.pop(0)
+        if not running:
+            if pending:
+                time.sleep(max(0.0, min(0.002, pending[0][1][0] - now)))
+            continue
+        b.step(steps_per_poll)
+        _, state, _, en = b.poll()
+        now = time.perf_counter() - t_start
+        for s in [s for s in running if state[s] == 2]:
+            i, (ta, _) = running.pop(s)
+            lat[i] = now - ta
+            energy[i] = float(en[s])
+            b.release(s)
+    total = time.perf_counter() - t_start
+    b.close()
+    n = len(arrivals)
+    return [lat[i] for i in range(n)], total, [energy[i] for i in range(n)]
+
+
+def plain_service(mb, torch, jobs):
+    """each job alone through the plain solver, back to back, to its own stop
+    (step limit, or the imaginary-time energy rule of the reference's driver
+    checked on the host every check_every steps); service time = wall clock
+    from solver creation to the stop, set-up included"""
+    stream = torch.cuda.current_stream()
+    svc, energy = [], []
+    for j in jobs:
+        t0 = time.perf_counter()
+        s = mb.Solver(j["npar"], j["norb"], j["grid_size"], j["xi"], j["xf"], j["dt"],
+                      bool(j["imagtime"]), j["rk_order"], LZ, periodic=bool(j["periodic"]))
+        s.set_potential(j["pot"])
+        s.set_interaction(j["g"])
+        s.set_state(j["orbitals"], j["coef"])
+        prev = s.energy().real / j["npar"]
+        e = prev
+        k = 0
+        while k < j["max_steps"]:
+            n = j["check_every"] if (j["imagtime"] and j["check_every"]) else j["max_steps"]
+            n = min(n, j["max_steps"] - k)
+            s.step(n, stream)
+            k += n
+            if j["imagtime"] and j["check_every"]:
+                e = s.energy().real / j["npar"]
+                if abs(e - prev) < j["energy_tol"] * prev:
+                    break
+                prev = e
+        e = s.energy().real
+        torch.cuda.synchronize()
+        s.close()
+        svc.append(time.perf_counter() - t0)
+        energy.append(e)
+    return svc, energy
+
+
+def fcfs(arr, svc):
+    """latencies and makespan of one first-come-first-served server: job i
+    starts at max(its arrival, the previous job's finish)"""
+    fin, lat = 0.0, []
+    for a, s in zip(arr, svc):
+        fin = max(fin, a) + s
+        lat.append(fin - a)
+    return lat, fin
+
+
+def percentiles(lat):
+    a = np.asarray(lat)
+    return {"p50_s": float(np.percentile(a, 50)), "p99_s": float(np.percentile(a, 99)),
+            "mean_s": float(a.mean()), "max_s": float(a.max())}
+
+
+def run_serving(mb, torch, rates, njobs, imag_steps, real_steps, big_frac, nmax):
+    seq = served_jobs(njobs, imag_steps=imag_steps, real_steps=real_steps, big_frac=big_frac,
+                      nmax=nmax)
+    jobs = [j for _, j in seq]
+    unit = [t for t, _ in seq]
+    arena = min(arena_bytes(mb, jobs), 96 << 30)
+    svc, e_plain = plain_service(mb, torch, jobs)
+    out = {"jobs": len(jobs), "imag_steps": imag_steps, "real_steps": real_steps,
+           "big_frac": big_frac, "nmax": nmax, "arena_bytes": arena,
+           "plain_service_s": {"sum": float(sum(svc)), "mean": float(np.mean(svc)),
+                               "max": float(max(svc))},
+           "plain_method": "each job's service time measured alone through mctdhb_solver, "
+                           "back to back; latencies from the first-come-first-served "
+                           "recurrence over the arrivals (what one-at-a-time serving gives)",
+           "rates": []}
+    worst = 0.0
+    for r in rates:
+        arr = [u / r for u in unit]
+        lat_b, t_b, e_b = serve_batched(mb, list(zip(arr, jobs)), arena)
+        lat_p, t_p = fcfs(arr, svc)
+        worst = max(worst, max(abs(x - y) / abs(y) for x, y in zip(e_b, e_plain)))
+        out["rates"].append({
+            "rate_jobs_per_s": r,
+            "batched": dict(percentiles(lat_b), jobs_per_s=len(jobs) / t_b, makespan_s=t_b),
+            "plain": dict(percentiles(lat_p), jobs_per_s=len(jobs) / t_p, makespan_s=t_p),
+            "p99_speedup": float(np.percentile(lat_p, 99) / np.percentile(lat_b, 99)),
+            "throughput_speedup": t_p / t_b})
+    out["energy_max_rel_diff_batched_vs_plain"] = worst
+    return out
+
+
+# ---------------------------------------------------------------------------
+# the N=30 M=8 quench: configurational step and the H.C roofline
+# ---------------------------------------------------------------------------
+def quench_inputs(mb):
+    x = np.linspace(Q_XI, Q_XF, Q_GRID)
+    phi = hermite_orbitals(N_ORB, Q_GRID, Q_XI, Q_XF)
+    dx = x[1] - x[0]
+    w = simpson_weights(Q_GRID, dx)
+    d = (np.roll(phi, 2, 1) - np.roll(phi, -2, 1) +
+         8 * (np.roll(phi, -1, 1) - np.roll(phi, 1, 1))) / (12 * dx)
+    hob = 0.5 * np.einsum("x,ax,bx->ab", w, d.conj(), d) + \
+        np.einsum("x,ax,bx->ab", w * trap(True, Q_GRID, Q_XI, Q_XF), phi.conj(), phi)
+    t = Q_G * np.einsum("x,ax,bx,cx,dx->abcd", w, phi.conj(), phi.conj(), phi, phi)
+    hint = np.ascontiguousarray(t.transpose(3, 2, 1, 0)).reshape(-1)
+    c0 = coefficients(int(mb.load().space_dimension(N_PAR, N_ORB)), np.random.default_rng(1234))
+    return np.ascontiguousarray(hob), hint, c0
+
+
+def run_quench(mb, torch, steps, warmup):
+    stream = torch.cuda.current_stream()
+    hob, hint, c0 = quench_inputs(mb)
+    sp = mb.Space(N_PAR, N_ORB)
+    nc = sp.dim
+    d_c = torch.from_numpy(c0).cuda()
+    sp.set_matrices(torch.from_numpy(hob.reshape(-1)).cuda(), torch.from_numpy(hint).cuda())
+    r1 = torch.empty(N_ORB * N_ORB, dtype=torch.complex128, device="cuda")
+    r2 = torch.empty(N_ORB ** 4, dtype=torch.complex128, device="cuda")
+    step = mb.Step(sp, d_c, r1, r2, Q_LZ, Q_DT, False)
+    for _ in range(warmup):
+        step.launch(stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step.launch(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_step = e0.elapsed_time(e1) / steps
+    norm = float(torch.linalg.vector_norm(d_c).item())
+    assert abs(norm - 1.0) < 1e-10, f"real-time SIL must conserve the norm, got {norm}"
+    step.close()
+    hc_out = torch.empty_like(d_c)
+    for _ in range(2):
+        sp.apply_hamiltonian(d_c, hc_out, stream)
+        sp.density_matrices(d_c, r1, r2, stream)
+    reps = 5
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        sp.apply_hamiltonian(d_c, hc_out, stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    t_hc = a.elapsed_time(b) / reps / 1000.0
+    a.record(stream)
+    for _ in range(reps):
+        sp.density_matrices(d_c, r1, r2, stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    t_dn = a.elapsed_time(b) / reps / 1000.0
+    G = distinct_couplings(N_PAR, N_ORB)
+    b_hc = 32.0 * nc + 16.0 * G
+    b_dn = 16.0 * nc + 16.0 * G
+    peak, kind = peaks()
+    del sp, d_c, hc_out
+    return {"workload": "real-time quench N=30 M=8 (nc=10295472), grid 1024 on [-15,15], "
+                        "V=x^2/2+4exp(-x^2/0.5), g=0.1, Lanczos 6, dt=0.005",
+            "step": "SIL(6 H.C) + rho1 + rho2, one CUDA graph",
+            "steps_per_s": 1000.0 / t_step, "ms_per_step": t_step,
+            "hc": {"kernel": "hc_kernel<8>", "ms_per_launch": t_hc * 1e3,
+                   "algorithmic_bytes_per_launch": b_hc, "achieved_gbs": b_hc / t_hc / 1e9,
+                   "peak": peak, "frac": b_hc / t_hc / 1e9 / peak, "peak_source": kind,
+                   "traffic": ncu_traffic().get("hc_bytes_per_launch")},
+            "density": {"ms_per_launch": t_dn * 1e3, "algorithmic_bytes_per_launch": b_dn,
+                        "achieved_gbs": b_dn / t_dn / 1e9}}
 
 
 # ---------------------------------------------------------------------------
@@ -273,45 +721,18 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    phi = hermite_orbitals()
-    pot = double_well(grid())
-    hob, hint = orbital_matrices(phi)
-    c0 = coefficients(int(mb.load().space_dimension(N_PAR, N_ORB)), 1234 + rank)
-
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    stream = torch.cuda.current_stream()
-    # informational: the full mctdhb_propagate_step (orbital RK5 + h, g + SIL +
-    # densities) over its first steps.  At this grid and dt the explicit RK5
-    # orbital step is outside its stability region (dt * max eigenvalue of the
-    # finite-difference kinetic operator ~ 11) and diverges after ~5 steps in
-    # the reference's own method as well; its cost is timed, not its values.
-    s = mb.Solver(N_PAR, N_ORB, GRID, XI, XF, DT, False, 5, LANCZOS_M)
-    s.set_potential(pot)
-    s.set_interaction(G_INT)
-    s.set_state(phi, c0)
-    s.step(1, stream)
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    s.step(2, stream)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    full_step_ms = f0.elapsed_time(f1) / 2
-    full_step_kernels = s.kernels
-    s.close()
-
-    # the measured step: SIL(6) + rho1, rho2 of the coefficients, one CUDA graph
-    sp = mb.Space(N_PAR, N_ORB)
-    nc = sp.dim
-    d_c = torch.from_numpy(c0).cuda()
-    sp.set_matrices(torch.from_numpy(hob.reshape(-1)).cuda(), torch.from_numpy(hint).cuda())
-    r1 = torch.empty(N_ORB * N_ORB, dtype=torch.complex128, device="cuda")
-    r2 = torch.empty(N_ORB ** 4, dtype=torch.complex128, device="cuda")
-    step = mb.Step(sp, d_c, r1, r2, LANCZOS_M, DT, False)
-    for _ in range(args.warmup):
-        step.launch(stream)
+    jobs = mix_jobs(seed=MIX_SEED + rank)
+    b = mb.Batch(len(jobs), arena_bytes(mb, jobs), LZ)
+    slots = [b.admit(j) for j in jobs]
+    assert None not in slots, "the arena is sized for every job"
+    b.step(args.warmup)
+    b.sync()
+    _, _, s0, _ = b.poll()
+    st = b.stream
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -319,181 +740,100 @@ def run_gpu(args):
     clocks.start()
     torch.cuda.profiler.start()  # ncu --profile-from-start off sees the timed steps only
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step.launch(stream)
-    e1.record(stream)
+    e0.record(st)
+    b.step(args.steps)
+    e1.record(st)
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
     barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()
     t_ms = e0.elapsed_time(e1)
+    _, state, s1, energy = b.poll()
+    inst = int(np.sum(s1.astype(np.int64) - s0.astype(np.int64)))
     if dist is not None:
         t = torch.tensor([t_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_ms = float(t.item())
-    value = world * args.steps / (t_ms / 1000.0)
-    norm = float(torch.linalg.vector_norm(d_c).item())
-    assert abs(norm - 1.0) < 1e-10, f"real-time SIL must conserve the norm, got {norm}"
-    kernels_per_step = step.kernels
-    step.close()
-
-    # H.C and density kernels alone on the same data (CUDA events on the
-    # launching stream) for the roofline
-    hc_out = torch.empty_like(d_c)
-    for _ in range(2):
-        sp.apply_hamiltonian(d_c, hc_out, stream)
-        sp.density_matrices(d_c, r1, r2, stream)
-    reps = 5
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(reps):
-        sp.apply_hamiltonian(d_c, hc_out, stream)
-    b.record(stream)
-    torch.cuda.synchronize()
-    t_hc = a.elapsed_time(b) / reps / 1000.0
-    a.record(stream)
-    for _ in range(reps):
-        sp.density_matrices(d_c, r1, r2, stream)
-    b.record(stream)
-    torch.cuda.synchronize()
-    t_dn = a.elapsed_time(b) / reps / 1000.0
-    G = distinct_couplings(N_PAR, N_ORB)
-    b_hc = 32.0 * nc + 16.0 * G
-    b_dn = 16.0 * nc + 16.0 * G
-    peak, peak_kind = peaks()
-    traffic = ncu_traffic()
-    del sp, d_c, hc_out
-
-    e2e = run_e2e(args, mb, hob, hint, c0, stream)
-    if dist is not None:
-        t = torch.tensor([args.steps / e2e["value"]], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e["value"] = world * args.steps / float(t.item())
-
+        n = torch.tensor([inst], device="cuda", dtype=torch.float64)
+        dist.all_reduce(n)
+        inst_all = int(n.item())
+    else:
+        inst_all = inst
+    value = inst_all / (t_ms / 1000.0)
+    kernels = b.kernels
     line = {
-        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+        "metric": METRIC, "value": value, "unit": "instance-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-        "data": "synthetic", "config": workload_config(args),
-        "roofline": {
-            "bound": "hbm", "kernel": "hc_kernel<8>",
-            "achieved": b_hc / t_hc / 1e9, "peak": peak, "unit": "GB/s",
-            "frac": b_hc / t_hc / 1e9 / peak, "peak_source": peak_kind,
-            "traffic": (traffic or {}).get("hc_bytes_per_launch"),
-            "algorithmic_bytes_per_launch": b_hc, "ms_per_launch": t_hc * 1e3,
-            "density_ms_per_launch": t_dn * 1e3, "density_achieved_gbs": b_dn / t_dn / 1e9,
-        },
-        "clocks": clk,
-        "gpu_launches": kernels_per_step * args.steps,
-        "e2e": e2e,
-        "full_step": {"ms_per_step": full_step_ms, "kernels_per_step": full_step_kernels,
-                      "what": "mctdhb_propagate_step incl. RK5 orbitals, first steps only"},
+        "data": "synthetic", "config": workload_config(args, jobs),
+        "instance_steps": inst_all, "clocks": clk, "gpu_launches": kernels * args.steps,
+        "kernels_per_step": kernels,
     }
-    if world == 1 and rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_step_estimate(hob, hint)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+    if rank != 0:
+        b.close()
+        return
 
+    # roofline: the dominant kernel of the step, the batched H.C per M
+    peak, kind = peaks()
+    groups = batch_hc_roofline(mb, torch, b, jobs)
+    Mtop = max(groups, key=lambda m: groups[m]["ms_per_launch"])
+    gt = groups[Mtop]
+    line["roofline"] = {
+        "bound": "hbm", "kernel": f"hc_batch_kernel<{Mtop}>", "achieved": gt["achieved_gbs"],
+        "peak": peak, "unit": "GB/s", "frac": gt["achieved_gbs"] / peak, "peak_source": kind,
+        "traffic": ncu_traffic().get(f"hc_batch_m{Mtop}_bytes_per_launch"),
+        "algorithmic_bytes_per_launch": gt["algorithmic_bytes"],
+        "ms_per_launch": gt["ms_per_launch"],
+        "groups": {str(m): g for m, g in groups.items()},
+        "note": "achieved = algorithmic bytes (32 nc + 16 G per job) / launch time; the "
+                "gathers are served from L2 and L1, so this can exceed the DRAM copy peak"}
+    # energies of a few jobs after warmup + steps, for the agreement check
+    cmp_idx = {i: int(s1[slots[i]]) for i in range(0, len(jobs), 37)}
+    e_batch = {i: float(energy[slots[i]]) for i in cmp_idx}
+    b.close()
 
-def run_e2e(args, mb, hob, hint, c0, stream):
-    """K steps through the reference's own calls, propagate_coef_sil
-    (coefficients_integration.c:59) then sync_density_matrices
-    (synchronize.c:42), on a reference-layout MCTDHBDataStruct whose buffers
-    are pinned host memory: every step uploads its inputs and copies its
-    results back (host<->device copies inside the timed region)."""
-    import torch
+    plain, e_plain = plain_timed(mb, torch, jobs, 1, args.plain_steps, compare=cmp_idx)
+    line["plain"] = plain
+    line["vs_plain"] = (value / world) / plain["value"]
+    line["energy_agreement"] = {
+        "max_rel_diff": max(abs(e_batch[i] - e_plain[i]) / abs(e_plain[i]) for i in cmp_idx),
+        "jobs": len(cmp_idx), "what": "energy after the same number of steps, batched vs plain"}
 
-    import mctdhb_types as T
-
-    L = mb.load()
-    M = N_ORB
-    nc = len(c0)
-    pin = lambda n: torch.empty(n, dtype=torch.complex128, pin_memory=True).numpy()
-    keep = []
-
-    def rows(a2):
-        a = pin(a2.size).reshape(a2.shape)
-        a[:] = a2
-        ptrs = (T.Carray * a.shape[0])(*[T.carray(a[i]) for i in range(a.shape[0])])
-        keep.append((a, ptrs))
-        return C.cast(ptrs, T.Cmatrix)
-
-    coef, cnext, hintv, rho2 = pin(nc), pin(nc), pin(M ** 4), pin(M ** 4)
-    coef[:] = c0
-    hintv[:] = hint
-    mc = T.MultiConfigurationS()
-    mc.npar, mc.norb, mc.dim = N_PAR, M, nc  # the GPU path ranks on the fly: no tables
-    stt = T.ManyBodyStateS()
-    stt.npar, stt.norb, stt.space_dim = N_PAR, M, nc
-    stt.coef, stt.hint, stt.tb_denmat = T.carray(coef), T.carray(hintv), T.carray(rho2)
-    stt.hob = rows(hob)
-    stt.ob_denmat = rows(np.zeros((M, M), np.complex128))
-    stt.inv_ob_denmat = rows(np.zeros((M, M), np.complex128))
-    eq = T.OrbitalEquationS()
-    eq.tstep, eq.prop_dt, eq.time_fac = DT, T.dcomplex.of(DT), T.dcomplex.of(1.0)
-    lw = T.WorkspaceLanczosS()
-    lw.iter, lw.space_dim = LANCZOS_M, nc
-    dd, od = np.zeros(LANCZOS_M, np.complex128), np.zeros(LANCZOS_M, np.complex128)
-    lw.decomp_diag, lw.decomp_offd = T.carray(dd), T.carray(od)
-    cw = T.CoefWorkspaceS()
-    cw.lan_work = C.pointer(lw)
-    ms = T.MCTDHBDataStructS()
-    ms.integ_type, ms.coef_integ_method = T.REALTIME, T.LANCZOS
-    ms.multiconfig_space, ms.orb_eq = C.pointer(mc), C.pointer(eq)
-    ms.coef_workspace, ms.state = C.pointer(cw), C.pointer(stt)
-    pms, pmc, pst = C.pointer(ms), C.pointer(mc), C.pointer(stt)
-
-    def one():
-        L.propagate_coef_sil(pms, T.carray(cnext))
-        L.sync_density_matrices(pmc, pst)
-
-    L.mctdhb_gpu_clear_error()
-    for _ in range(max(1, args.warmup)):
-        one()
-    if mb.last_error():
-        raise mb.MctdhbError(mb.last_error())
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(args.steps):
-        one()
-    b.record(stream)
-    torch.cuda.synchronize()
-    t = a.elapsed_time(b) / 1000.0
-    return {"value": args.steps / t, "unit": "steps/s",
-            "h2d_bytes_per_step": 2 * nc * 16 + (M * M + M ** 4) * 16,
-            "d2h_bytes_per_step": nc * 16 + (2 * M * M + M ** 4) * 16,
-            "path": "propagate_coef_sil + sync_density_matrices on pinned host buffers"}
+    line["quench_n30_m8"] = run_quench(mb, torch, max(3, args.steps // 2), args.warmup)
+    line["e2e"] = e2e_batch(mb, torch, jobs, args.steps)
+    if not args.no_serving:
+        line["serving"] = run_serving(mb, torch, [float(r) for r in args.serve_rates.split(",")],
+                                      args.serve_jobs, args.serve_imag_steps,
+                                      args.serve_real_steps, args.serve_big_frac,
+                                      args.serve_nmax)
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(jobs)
+    print(json.dumps(line), flush=True)
 
 
 def run_profile():
-    """H.C three times then the density kernel once at N=30, M=8: a small,
-    single-GPU case for `ncu -k regex:<kernel> -s <n> -c 1`."""
+    """a small single-GPU case for ncu: 24 jobs of the mix admitted, two
+    batch steps outside the profiled range, then one step inside it
+    (cudaProfilerStart/Stop; use --profile-from-start off)"""
     import torch
 
     import mctdhb_b200 as mb
 
-    hob, hint = orbital_matrices(hermite_orbitals())
-    sp = mb.Space(N_PAR, N_ORB)
-    d_c = torch.from_numpy(coefficients(sp.dim, 1234)).cuda()
-    out = torch.empty_like(d_c)
-    r1 = torch.empty(N_ORB * N_ORB, dtype=torch.complex128, device="cuda")
-    r2 = torch.empty(N_ORB ** 4, dtype=torch.complex128, device="cuda")
-    sp.set_matrices(torch.from_numpy(hob.reshape(-1)).cuda(), torch.from_numpy(hint).cuda())
-    for _ in range(2):  # autotuning happens here, outside the profiled range
-        sp.apply_hamiltonian(d_c, out)
-        sp.density_matrices(d_c, r1, r2)
-    torch.cuda.synchronize()
-    torch.cuda.profiler.start()  # ncu --profile-from-start off: one launch of each
-    sp.apply_hamiltonian(d_c, out)
-    sp.density_matrices(d_c, r1, r2)
-    torch.cuda.synchronize()
+    jobs = mix_jobs(n=24)
+    b = mb.Batch(len(jobs), arena_bytes(mb, jobs), LZ)
+    for j in jobs:
+        b.admit(j)
+    b.step(2)
+    b.sync()
+    torch.cuda.profiler.start()
+    b.step(1)
+    b.sync()
     torch.cuda.profiler.stop()
-    print("profile run done", float(torch.linalg.vector_norm(out).item()))
+    b.close()
+    print("profile run done")
 
 
 def main():
@@ -503,8 +843,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=2,
+                    help="timed steps per job on the plain one-at-a-time path")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-rates", default="10,50,500", help="arrival rates swept, jobs/s")
+    ap.add_argument("--serve-jobs", type=int, default=96, help="jobs served per rate")
+    ap.add_argument("--serve-imag-steps", type=int, default=300)
+    ap.add_argument("--serve-real-steps", type=int, default=100)
+    ap.add_argument("--serve-big-frac", type=float, default=0.0)
+    ap.add_argument("--serve-nmax", type=int, default=30)
     ap.add_argument("--profile", action="store_true",
-                    help="only launch the H.C and density kernels (for ncu captures)")
+                    help="one profiled batch step of a small mix (for ncu captures)")
     args = ap.parse_args()
     if args.profile:
         run_profile()

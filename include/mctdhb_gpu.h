@@ -23,6 +23,9 @@
  * Part 2 is a device-resident API: Fock-space handles and operations on
  * device pointers with an explicit CUDA stream (passed as void*), used for
  * throughput work where coefficients, orbitals and matrices stay in HBM.
+ *
+ * Part 3 is the batched engine: many independent systems of uneven size
+ * resident in one HBM arena, admitted by footprint and advanced together.
  */
 #ifndef MCTDHB_B200_GPU_H
 #define MCTDHB_B200_GPU_H
@@ -199,7 +202,7 @@ int mctdhb_dev_double_jump_map(mctdhb_space sp, int diff, void* d_strides, void*
                                void* stream);
 
 /* ---------------------------------------------------------------------- */
-/* Part 5: batched engine -- many independent systems on one GPU          */
+/* Part 3: batched engine -- many independent systems on one GPU          */
 /* ---------------------------------------------------------------------- */
 /* The reference integrates one system per process (driver.c:205-330; its
  * globals driver.c:15-19 make it single-instance).  These calls have no
@@ -258,6 +261,10 @@ int    mctdhb_batch_fetch(mctdhb_batch b, int slot, void* orbitals, void* coef, 
 /* frees the slot and its arena range */
 int    mctdhb_batch_release(mctdhb_batch b, int slot);
 int    mctdhb_batch_kernel_count(mctdhb_batch b); /* kernels per step graph */
+/* one launch of the batched H.C kernel of the running jobs with norb
+ * orbitals (out = H C of each job, on the engine's stream): a measurement
+ * hook for timing the dominant kernel of a step */
+int    mctdhb_batch_launch_hc(mctdhb_batch b, int norb);
 void*  mctdhb_batch_stream(mctdhb_batch b);       /* the engine's cudaStream_t */
 
 /* rho1 and rho2 of C, as mctdhb_dev_density_matrices computes them, with no

@@ -104,6 +104,32 @@ def test_solver_vs_oracle(gpu, oracle, N, M, G, imag, rk, m, dt, g, steps):
     s.close()
 
 
+@pytest.mark.parametrize("side_stream", [False, True])
+def test_solver_energy_follows_steps_on_any_stream(gpu, oracle, side_stream):
+    """energy() read right after step() -- no other synchronisation -- is the
+    energy of the stepped state, whichever stream the steps ran on"""
+    import torch
+
+    N, M, G, dt, g, steps = 10, 4, 128, 0.01, 0.5, 6
+    xi, xf = -8.0, 8.0
+    orb, dx = hermite_orbitals(M, G, xi, xf)
+    coef = rand_coef(np.random.default_rng(17), oracle.dim(N, M))
+    pot = harmonic(G, xi, xf)
+    s = gpu.Solver(N, M, G, xi, xf, dt, True, 5, 5)
+    s.set_potential(pot)
+    s.set_interaction(g)
+    s.set_state(orb, coef)
+    st = oracle_init(oracle, N, orb, coef, dx, pot, g)
+    for _ in range(steps):
+        oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, True, 5, 5, pot)
+    stream = torch.cuda.Stream() if side_stream else torch.cuda.current_stream()
+    s.step(steps, stream)
+    e = s.energy()
+    e_ref = oracle.total_energy(M, st["rho1"], st["rho2"], st["hob"], st["hint"])
+    assert abs(e - e_ref) < 1e-10 * abs(e_ref)
+    s.close()
+
+
 @pytest.mark.parametrize("imag,rk", [(True, 5), (False, 5), (False, 4)])
 def test_dropin_step_vs_reference(gpu, reference, imag, rk):
     """the same reference-built struct stepped by the reference and by the
