@@ -466,10 +466,16 @@ __global__ void bt_small_kernel(const BatchSlot* __restrict__ slots, const int* 
     double* z = (double*)(S.scal + BS_Z);
     S.flags[BF_QL] = tridiag_ql(n, d, e, z);
     const double2 pdt = S.pdt;
+    // imaginary time: exponents shifted by their maximum (a constant factor
+    // the renormalisation at the end of the step removes), so exp cannot
+    // overflow at |E| dt > 709; real time: no shift, unchanged bits
+    double shift = 0.0;
+    if (pdt.y != 0.0)
+        for (int k = 0; k < n; k++) shift = k == 0 ? d[k] * pdt.y : fmax(shift, d[k] * pdt.y);
     double2 aux[kBatchMaxLz];
     for (int k = 0; k < n; k++) {
         const double re = d[k] * pdt.y, im = -d[k] * pdt.x;
-        const double mag = exp(re);
+        const double mag = exp(re - shift);
         double sn, cs;
         sincos(im, &sn, &cs);
         const double u = z[0 * n + k];

@@ -86,7 +86,7 @@ int mctdhb_dev_set_matrices(mctdhb_space h, const void* d_hob, const void* d_hin
         set_error("mctdhb_dev_set_matrices: null argument");
         return -1;
     }
-    return hc_prep(h->sp.M, (const double2*)d_hob, (const double2*)d_hint, h->sp.d_tab,
+    return hc_prep(h->sp.view, (const double2*)d_hob, (const double2*)d_hint, h->sp.d_tab,
                    (cudaStream_t)stream);
 }
 

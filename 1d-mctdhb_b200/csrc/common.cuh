@@ -42,12 +42,17 @@ void clear_error();
     } while (0)
 
 // Device view of one Fock space.  T is the (M-1) x (N+1) rank-weight table,
-// sq the sqrt table sqrt(x), x = 0..N+2.
+// sq the sqrt table sqrt(x), x = 0..N+2.  The pair-space H.C
+// (pairhc_tmpl.cuh) uses dim2 = D(N-2, M), the pair matrix pair_w (P x P)
+// and its scratch pair_y (P x dim2); pair_y is null where that path is off.
 struct SpaceView {
     int N, M;
     uint32_t dim;
     const uint32_t* T;
     const double* sq;
+    uint32_t dim2 = 0;
+    double2* pair_w = nullptr;
+    double2* pair_y = nullptr;
 };
 
 __host__ __device__ constexpr int dl_index(int d) { return d < 0 ? d + 2 : d + 1; }

@@ -16,6 +16,8 @@
 #include <vector>
 
 #include "common.cuh"
+#include "engine.h"
+#include "gram.h"
 #include "kernels.h"
 #include "moves.cuh"
 
@@ -171,8 +173,36 @@ static int dens_slices(const SpaceView& sp) {
     return dens_templated(sp.M) ? dens_grid(sp) : dens_grid(sp) * 4;
 }
 
+// rows of the one- and two-boson-annihilated spaces (0 when empty)
+static uint32_t annihilated_dim(const SpaceView& sp, int R) {
+    return sp.N >= R ? (uint32_t)fock_dimension(sp.N - R, sp.M) : 0u;
+}
+
+static size_t gram_partial(const SpaceView& sp) {
+    return (size_t)gram_blocks(annihilated_dim(sp, 2)) * gram_entries(sp.M, 2) +
+           (size_t)gram_blocks(annihilated_dim(sp, 1)) * gram_entries(sp.M, 1);
+}
+
 size_t dens_partial_elems(const SpaceView& sp) {
-    return (size_t)dens_slices(sp) * dens_ep(sp.M);
+    const size_t per_row = (size_t)dens_slices(sp) * dens_ep(sp.M);
+    return dens_templated(sp.M) ? std::max(per_row, gram_partial(sp)) : per_row;
+}
+
+// M <= 8: the Gram-matrix kernels (gram_tmpl.cuh)
+static int gram_apply(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
+                      double2* rho2, cudaStream_t st) {
+    const uint32_t D2 = annihilated_dim(sp, 2), D1 = annihilated_dim(sp, 1);
+    switch (sp.M) {
+        case 2: return gram_apply_tmpl<2>(sp, D2, D1, C, partial, rho1, rho2, st);
+        case 3: return gram_apply_tmpl<3>(sp, D2, D1, C, partial, rho1, rho2, st);
+        case 4: return gram_apply_tmpl<4>(sp, D2, D1, C, partial, rho1, rho2, st);
+        case 5: return gram_apply_tmpl<5>(sp, D2, D1, C, partial, rho1, rho2, st);
+        case 6: return gram_apply_tmpl<6>(sp, D2, D1, C, partial, rho1, rho2, st);
+        case 7: return gram_apply_tmpl<7>(sp, D2, D1, C, partial, rho1, rho2, st);
+        case 8: return gram_apply_tmpl<8>(sp, D2, D1, C, partial, rho1, rho2, st);
+    }
+    set_error("gram_apply: %d orbitals outside 2..8", sp.M);
+    return -1;
 }
 
 static int dens_launch_v(const SpaceView& sp, const double2* C, double2* partial, int grid,
@@ -213,6 +243,15 @@ int dens_variant(const SpaceView& sp, const double2* C, double2* partial, cudaSt
 }  // namespace
 
 int dens_prepare(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st) {
+    (void)C;
+    (void)partial;
+    (void)st;
+    return 0;  // the Gram kernels (M <= 8) and the generic kernel need no set-up
+}
+
+// Set-up of the per-row kernels (dens_tmpl.cuh): launch attributes and the
+// tuned variant, before any capture.
+int dens_prepare_rows(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st) {
     if (!dens_templated(sp.M)) return 0;
     for (int v = 0; v < kDensVariants; v++)
         if (dens_launch_v(sp, nullptr, nullptr, 0, v, st)) return -1;  // attributes only
@@ -223,6 +262,15 @@ int dens_prepare(const SpaceView& sp, const double2* C, double2* partial, cudaSt
 
 int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
                double2* rho2, const int* d_desc, cudaStream_t st) {
+    if (dens_templated(sp.M)) return gram_apply(sp, C, partial, rho1, rho2, st);
+    return dens_apply_rows(sp, C, partial, rho1, rho2, d_desc, st);
+}
+
+// The per-row pass: every row's contributions to every unique element,
+// reduced across the warp (dens_tmpl.cuh for M <= 8, the generic kernel
+// beyond).
+int dens_apply_rows(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
+                    double2* rho2, const int* d_desc, cudaStream_t st) {
     const int grid = dens_grid(sp);
     const int M = sp.M;
     const int EP = dens_ep(M);

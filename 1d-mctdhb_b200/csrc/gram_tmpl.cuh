@@ -1,0 +1,286 @@
+// gram_tmpl.cuh -- density matrices as Gram matrices of annihilated states,
+// register-tiled for M <= 8 orbitals (explicit instantiations in dens_m*.cu).
+//
+// rho2[k,s,q,l] = <a+_k a+_s a_q a_l> and rho1[k][l] = <a+_k a_l>
+// (density_matrices.c:9-443) are inner products of states with one or two
+// bosons removed.  Inserting the identity of the (N-R)-boson space,
+//     rho2[k,s,q,l] = sum_m conj(A_m(k,s)) A_m(q,l),  A_m(q,l) = <m|a_q a_l|C>,
+//     rho1[k][l]    = sum_m conj(B_m(k))   B_m(l),    B_m(l)   = <m|a_l|C>,
+// with m over the D(N-2, M) (resp. D(N-1, M)) configurations.  Each A value
+// is one scaled coefficient, A_m(q,l) = sqrt((m_q+1)(m_l+1+[q=l])) C[m+e_q+e_l]:
+// at N=30, M=8 that is 6.7 M rows x 36 pairs = 242 M gathers (against the
+// ~3 G coupling gathers of a per-row pass) and a 36 x 36 Hermitian Gram
+// matrix, FP64-FMA bound instead of gather and shuffle bound.
+//
+// Ranking.  With the cumulative occupations L_x of m and the rank-weight
+// table T_x(L) = C(L+x, x+1) (common.cuh), the rank of m + e_q + e_l in the
+// N-boson space is
+//     j = (D_N - D_{N-R}) + rank(m) - (U1[q] - U1[l]) - U2[l],
+//     U_d[x] = sum_{y=x}^{M-2} (T_y(L_y + d) - T_y(L_y)),
+// two subtractions per pair once U1, U2 are formed per row.
+//
+// Work split.  A block takes tiles of ROWS rows: every thread unranks its
+// row and gathers its share of the row's A values into shared memory; then
+// thread groups accumulate the upper triangle of the P x P Gram matrix in
+// RT x RT complex register tiles, each group over an interleaved subset of
+// the tile's rows.  At the end the groups are added in a fixed order and the
+// block writes one partial; gram_finalize_kernel adds the partials in block
+// order.  The grid is a function of (N, M) only, so the result is
+// deterministic and the same in any launch context.
+#pragma once
+#include "common.cuh"
+#include "kernels.h"
+#include "gram.h"
+#include "movelist.cuh"
+
+namespace mctdhb {
+
+// pair p <-> (q, l), q <= l, in row-major order of the upper triangle
+template <int M>
+struct PairList {
+    int q[M * (M + 1) / 2], l[M * (M + 1) / 2];
+    constexpr PairList() : q{}, l{} {
+        int p = 0;
+        for (int a = 0; a < M; a++)
+            for (int b = a; b < M; b++) {
+                q[p] = a;
+                l[p] = b;
+                p++;
+            }
+    }
+};
+template <int M>
+inline constexpr PairList<M> kPairs{};
+
+// Unrank `row` of the space of Np bosons (dimension Dp) with the rank table
+// of a space of N >= Np bosons (row stride N + 1): occupations n[] and the
+// suffix sums U1, U2 of the rank offsets of adding one / two bosons.
+template <int M, int R>
+__device__ __forceinline__ void gram_unrank(const uint32_t* __restrict__ T, int N, int Np,
+                                            uint32_t Dp, uint32_t row, int (&n)[M],
+                                            uint32_t (&U1)[M], uint32_t (&U2)[M]) {
+    uint32_t S = Dp - 1u - row;
+    int Lnext = Np;
+    int L[M > 1 ? M - 1 : 1];
+#pragma unroll
+    for (int x = M - 2; x >= 0; x--) {
+        const uint32_t* Tx = T + x * (N + 1);
+        int lo = 0, hi = Lnext;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(Tx + mid) <= S)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        S -= __ldg(Tx + lo);
+        n[x + 1] = Lnext - lo;
+        L[x] = lo;
+        Lnext = lo;
+    }
+    n[0] = Lnext;
+    U1[M - 1] = 0u;
+    U2[M - 1] = 0u;
+#pragma unroll
+    for (int x = M - 2; x >= 0; x--) {
+        const uint32_t* Tx = T + x * (N + 1);
+        const uint32_t t0 = __ldg(Tx + L[x]);
+        U1[x] = U1[x + 1] + (__ldg(Tx + L[x] + 1) - t0);
+        if constexpr (R == 2) U2[x] = U2[x + 1] + (__ldg(Tx + L[x] + 2) - t0);
+    }
+}
+
+// One block's share of the Gram matrix of the R-annihilated states of C.
+// Dp = D(N-R, M) rows; jbase = D(N, M) - Dp.  partial: gridDim.x x
+// gram_entries(M, R) complex.
+template <int M, int R>
+__global__ void __launch_bounds__(kGramThreads, 2)
+    gram_kernel(SpaceView sp, uint32_t Dp, const double2* __restrict__ C,
+                double2* __restrict__ partial) {
+    constexpr int P = gram_p(M, R);
+    constexpr int RT = gram_rt(P);
+    constexpr int NT = P / RT;
+    constexpr int NTILES = NT * (NT + 1) / 2;
+    constexpr int ENT = NTILES * RT * RT;
+    constexpr int ROWS = kGramRows;
+    constexpr int PARTS = kGramThreads / ROWS;  // threads per row in the gather phase
+    constexpr int GROUPS = (kGramThreads / NTILES) < ROWS ? (kGramThreads / NTILES) : ROWS;
+    static_assert(ENT <= ROWS * P, "the group reduction reuses the A tile");
+
+    __shared__ double2 As[ROWS * P];  // As[r * P + p]
+    const int t = threadIdx.x;
+    const int N = sp.N, Np = N - R;
+    const uint32_t jbase = sp.dim - Dp;
+    const int grp = t / NTILES, tile = t % NTILES;
+    const bool accum = grp < GROUPS;
+    int ti = 0, tj = 0;
+    for (int a = 0, c = 0; a < NT; a++)
+        for (int b = a; b < NT; b++, c++)
+            if (c == tile) ti = a, tj = b;
+
+    double2 acc[RT][RT];
+#pragma unroll
+    for (int a = 0; a < RT; a++)
+#pragma unroll
+        for (int b = 0; b < RT; b++) acc[a][b] = make_double2(0.0, 0.0);
+
+    const uint32_t ntile_rows = (Dp + ROWS - 1) / ROWS;
+    for (uint32_t tr = blockIdx.x; tr < ntile_rows; tr += gridDim.x) {
+        // gather: thread (r, part) fills pairs p = part, part + PARTS, ... of row r
+        {
+            const int r = t % ROWS, part = t / ROWS;
+            const uint32_t row = tr * ROWS + r;
+            const bool live = row < Dp;
+            int n[M];
+            uint32_t U1[M], U2[M];
+            if (live) {
+                gram_unrank<M, R>(sp.T, N, Np, Dp, row, n, U1, U2);
+            } else {
+#pragma unroll
+                for (int x = 0; x < M; x++) n[x] = 0, U1[x] = 0u, U2[x] = 0u;
+            }
+            const uint32_t j0 = jbase + row;
+            static_for<P>([&](auto pi) {
+                constexpr int p = decltype(pi)::value;
+                if (p % PARTS == part) {
+                    double2 v = make_double2(0.0, 0.0);
+                    if (live) {
+                        if constexpr (R == 1) {
+                            const uint32_t j = j0 - U1[p];
+                            v = cscale(__ldg(C + j), __ldg(sp.sq + n[p] + 1));
+                        } else {
+                            constexpr int q = kPairs<M>.q[p], l = kPairs<M>.l[p];
+                            const uint32_t j = j0 - (U1[q] - U1[l]) - U2[l];
+                            double f;
+                            if constexpr (q == l)
+                                f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[q] + 2);
+                            else
+                                f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
+                            v = cscale(__ldg(C + j), f);
+                        }
+                    }
+                    As[r * P + p] = v;
+                }
+            });
+        }
+        __syncthreads();
+        // Gram update: rows grp, grp + GROUPS, ... of the tile
+        if (accum) {
+            for (int r = grp; r < ROWS; r += GROUPS) {
+                double2 a[RT], b[RT];
+#pragma unroll
+                for (int x = 0; x < RT; x++) {
+                    a[x] = As[r * P + ti * RT + x];
+                    b[x] = As[r * P + tj * RT + x];
+                }
+#pragma unroll
+                for (int x = 0; x < RT; x++)
+#pragma unroll
+                    for (int y = 0; y < RT; y++) acc[x][y] = cfma_conj(a[x], b[y], acc[x][y]);
+            }
+        }
+        __syncthreads();
+    }
+    // groups added in order 0, 1, ... into the (now free) A tile
+    double2* red = As;
+    for (int g = 0; g < GROUPS; g++) {
+        if (accum && grp == g) {
+#pragma unroll
+            for (int x = 0; x < RT; x++)
+#pragma unroll
+                for (int y = 0; y < RT; y++) {
+                    const int e = (tile * RT + x) * RT + y;
+                    if (g == 0)
+                        red[e] = acc[x][y];
+                    else
+                        red[e] = cadd(red[e], acc[x][y]);
+                }
+        }
+        __syncthreads();
+    }
+    for (int e = t; e < ENT; e += kGramThreads) partial[(size_t)blockIdx.x * ENT + e] = red[e];
+}
+
+// Sum of the block partials (block order) and the fill of rho2 (M^4,
+// element (k,s,q,l) at k + sM + qM^2 + lM^3) and rho1 (M x M row-major):
+// every ordering of a pair reads the same Gram entry, the lower triangle is
+// the conjugate of the upper, diagonal entries are real.  One thread per
+// entry of the packed upper-triangle tiles: first rho2's, then rho1's.
+template <int M>
+__global__ void gram_finalize_kernel(int blocks2, int blocks1, const double2* __restrict__ part2,
+                                     const double2* __restrict__ part1, double2* __restrict__ rho1,
+                                     double2* __restrict__ rho2) {
+    constexpr int ENT2 = gram_entries(M, 2), ENT1 = gram_entries(M, 1);
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ENT2 + ENT1) return;
+    const bool two = e < ENT2;
+    const int ee = two ? e : e - ENT2;
+    const int P = two ? gram_p(M, 2) : gram_p(M, 1);
+    const int RT = gram_rt(P), NT = P / RT;
+    const int nb = two ? blocks2 : blocks1;
+    const int ent = two ? ENT2 : ENT1;
+    const double2* part = two ? part2 : part1;
+    // packed index -> (tile, x, y) -> (p, p')
+    const int tile = ee / (RT * RT), x = (ee / RT) % RT, y = ee % RT;
+    int ti = 0, tj = 0, c = 0;
+    for (int a = 0; a < NT; a++)
+        for (int b = a; b < NT; b++) {
+            if (c == tile) ti = a, tj = b;
+            c++;
+        }
+    const int pa = ti * RT + x, pb = tj * RT + y;
+    if (pa > pb) return;  // lower part of a diagonal tile: the conjugate is written by (pb, pa)
+    double2 v = make_double2(0.0, 0.0);
+    for (int b = 0; b < nb; b++) v = cadd(v, part[(size_t)b * ent + ee]);
+    if (pa == pb) v.y = 0.0;
+    const double2 vc = make_double2(v.x, -v.y);
+    if (!two) {
+        rho1[pa * M + pb] = v;
+        rho1[pb * M + pa] = vc;
+        return;
+    }
+    auto pair = [](int p, int& q, int& l) {
+        int c2 = 0;
+        for (int a = 0; a < M; a++)
+            for (int b = a; b < M; b++) {
+                if (c2 == p) q = a, l = b;
+                c2++;
+            }
+    };
+    int k = 0, s = 0, q = 0, l = 0;
+    pair(pa, k, s);
+    pair(pb, q, l);
+    constexpr int M2 = M * M, M3 = M2 * M;
+    auto put = [&](int a, int b2, int cc, int d, double2 w) { rho2[a + b2 * M + cc * M2 + d * M3] = w; };
+    const int ks[2][2] = {{k, s}, {s, k}}, ql[2][2] = {{q, l}, {l, q}};
+    for (int u = 0; u < (k == s ? 1 : 2); u++)
+        for (int w = 0; w < (q == l ? 1 : 2); w++) {
+            put(ks[u][0], ks[u][1], ql[w][0], ql[w][1], v);
+            put(ql[w][0], ql[w][1], ks[u][0], ks[u][1], vc);
+        }
+}
+
+template <int M, int R>
+int gram_launch(const SpaceView& sp, uint32_t Dp, const double2* C, double2* partial, int blocks,
+                cudaStream_t st) {
+    if (blocks <= 0) return 0;
+    gram_kernel<M, R><<<blocks, kGramThreads, 0, st>>>(sp, Dp, C, partial);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <int M>
+int gram_apply_tmpl(const SpaceView& sp, uint32_t D2, uint32_t D1, const double2* C,
+                    double2* partial, double2* rho1, double2* rho2, cudaStream_t st) {
+    const int b2 = gram_blocks(D2), b1 = gram_blocks(D1);
+    double2* part2 = partial;
+    double2* part1 = partial + (size_t)b2 * gram_entries(M, 2);
+    if (gram_launch<M, 2>(sp, D2, C, part2, b2, st)) return -1;
+    if (gram_launch<M, 1>(sp, D1, C, part1, b1, st)) return -1;
+    constexpr int ENT = gram_entries(M, 2) + gram_entries(M, 1);
+    gram_finalize_kernel<M><<<(ENT + 127) / 128, 128, 0, st>>>(b2, b1, part2, part1, rho1, rho2);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace mctdhb

@@ -24,6 +24,7 @@
 #include <tuple>
 
 #include "common.cuh"
+#include "engine.h"
 #include "kernels.h"
 #include "moves.cuh"
 
@@ -136,14 +137,115 @@ __global__ void __launch_bounds__(128)
 // ---------------------------------------------------------------------------
 // launchers and autotuner
 // ---------------------------------------------------------------------------
-int hc_prep(int M, const double2* d_hob, const double2* d_hint, double2* d_tab,
+// ---------------------------------------------------------------------------
+// pair matrix W of H = sum_{P,Q} W[P][Q] a+_P a_Q (pairhc_tmpl.cuh)
+// ---------------------------------------------------------------------------
+// W[P][Q], P = {k <= s} created, Q = {q <= l} annihilated, with the g
+// elements and factors of the reference's rules (the move coefficients of
+// moves.cuh) and the one-body part spread over the spectator orbital x
+// with weight 1/(N-1):
+//   P = Q = {k,k}:    1/2 g_kkkk + h_kk/(N-1)
+//   P = Q = {k,s}:    2 g_ksks + (h_kk + h_ss)/(N-1)
+//   P = {a,x}, Q = {b,x}, a != b (one boson b -> a, spectator x):
+//                     c + h_ab/(N-1),  c = g_aaab (x = a), g_abbb (x = b),
+//                                          2 g_axxb otherwise
+//   P, Q disjoint:    f g_ksql, f = 1/2 (k=s, q=l), 1 (one of them), 2
+__global__ void hcp_w_kernel(int N, int M, const double2* __restrict__ hob,
+                             const double2* __restrict__ hint, double2* __restrict__ W) {
+    const int P = M * (M + 1) / 2, M2 = M * M, M3 = M2 * M;
+    const double inv = 1.0 / (double)(N - 1);
+    auto g = [&](int a, int b, int c, int d) { return hint[a + b * M + c * M2 + d * M3]; };
+    auto h = [&](int a, int b) { return hob[a * M + b]; };
+    auto pair = [&](int p, int& a, int& b) {
+        for (int u = 0, c = 0; u < M; u++)
+            for (int v = u; v < M; v++, c++)
+                if (c == p) a = u, b = v;
+    };
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P * P; e += gridDim.x * blockDim.x) {
+        const int pa = e / P, pb = e % P;
+        int k = 0, s = 0, q = 0, l = 0;
+        pair(pa, k, s);
+        pair(pb, q, l);
+        double2 w;
+        if (pa == pb) {
+            if (k == s) {
+                w = cadd(cscale(g(k, k, k, k), 0.5), cscale(h(k, k), inv));
+            } else {
+                w = cadd(cscale(g(k, s, k, s), 2.0), cscale(cadd(h(k, k), h(s, s)), inv));
+            }
+        } else {
+            int x = -1;
+            if (k == q || k == l)
+                x = k;
+            else if (s == q || s == l)
+                x = s;
+            if (x >= 0) {
+                const int a = (k == x) ? s : k, b = (q == x) ? l : q;
+                double2 c;
+                if (x == a)
+                    c = g(a, a, a, b);
+                else if (x == b)
+                    c = g(a, b, b, b);
+                else
+                    c = cscale(g(a, x, x, b), 2.0);
+                w = cadd(c, cscale(h(a, b), inv));
+            } else {
+                const double f = (k == s && q == l) ? 0.5 : ((k == s || q == l) ? 1.0 : 2.0);
+                w = cscale(g(k, s, q, l), f);
+            }
+        }
+        W[e] = w;
+    }
+}
+
+bool hcp_eligible(int N, int M) { return N >= 2 && M >= 2 && M <= kMaxTemplOrb; }
+
+size_t hcp_scratch_bytes(int N, int M) {
+    if (!hcp_eligible(N, M)) return 0;
+    return (size_t)fock_dimension(N - 2, M) * (size_t)(M * (M + 1) / 2) * sizeof(double2);
+}
+
+int hcp_prepare(int M) {
+    switch (M) {
+        case 2: return hcp_prepare_tmpl<2>();
+        case 3: return hcp_prepare_tmpl<3>();
+        case 4: return hcp_prepare_tmpl<4>();
+        case 5: return hcp_prepare_tmpl<5>();
+        case 6: return hcp_prepare_tmpl<6>();
+        case 7: return hcp_prepare_tmpl<7>();
+        case 8: return hcp_prepare_tmpl<8>();
+    }
+    return 0;
+}
+
+int hc_prep(const SpaceView& sp, const double2* d_hob, const double2* d_hint, double2* d_tab,
             cudaStream_t st) {
-    hc_prep_kernel<<<1, 32, 0, st>>>(M, d_hob, d_hint, d_tab);
+    hc_prep_kernel<<<1, 32, 0, st>>>(sp.M, d_hob, d_hint, d_tab);
     MCTDHB_CUDA_TRY(cudaGetLastError());
+    if (sp.pair_y != nullptr) {
+        const int P = sp.M * (sp.M + 1) / 2;
+        hcp_w_kernel<<<(P * P + 127) / 128, 128, 0, st>>>(sp.N, sp.M, d_hob, d_hint, sp.pair_w);
+        MCTDHB_CUDA_TRY(cudaGetLastError());
+    }
     return 0;
 }
 
 static bool hc_templated(int M) { return M >= 2 && M <= kMaxTemplOrb; }
+
+static int hcp_apply(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
+                     cudaStream_t st) {
+    switch (sp.M) {
+        case 2: return hcp_apply_tmpl<2>(sp, C, HC, ep, st);
+        case 3: return hcp_apply_tmpl<3>(sp, C, HC, ep, st);
+        case 4: return hcp_apply_tmpl<4>(sp, C, HC, ep, st);
+        case 5: return hcp_apply_tmpl<5>(sp, C, HC, ep, st);
+        case 6: return hcp_apply_tmpl<6>(sp, C, HC, ep, st);
+        case 7: return hcp_apply_tmpl<7>(sp, C, HC, ep, st);
+        case 8: return hcp_apply_tmpl<8>(sp, C, HC, ep, st);
+    }
+    set_error("hcp_apply: %d orbitals outside 2..8", sp.M);
+    return -1;
+}
 
 static int hc_launch_v(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
                        const HcEpilogue& ep, int v, cudaStream_t st) {
@@ -184,13 +286,14 @@ int hc_tune_launch(void* p, int v, cudaStream_t st) {
 
 int hc_variant(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
                const HcEpilogue& ep, cudaStream_t st) {
-    if (!hc_templated(sp.M) || sp.dim < 4096) return 0;
+    if (!hc_templated(sp.M) || sp.dim < 4096 || sp.pair_y != nullptr) return 0;
     HcTuneCtx ctx{&sp, C, HC, tab, &ep};
     return tune_pick("hc", sp.N, sp.M, kHcVariants, st, hc_tune_launch, &ctx);
 }
 
 int hc_apply(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
              const HcEpilogue& ep, cudaStream_t st) {
+    if (sp.pair_y != nullptr) return hcp_apply(sp, C, HC, ep, st);
     const int v = hc_variant(sp, C, HC, tab, ep, st);
     return hc_launch_v(sp, C, HC, tab, ep, v, st);
 }

@@ -53,6 +53,20 @@ int hc_launch_tmpl(const SpaceView& sp, const double2* C, double2* HC, const dou
 template <int M>
 int dens_launch_tmpl(const SpaceView& sp, const double2* C, double2* partial, int grid,
                      int variant, cudaStream_t st);
+// rho1/rho2 as Gram matrices of the one- and two-boson-annihilated states
+// (gram_tmpl.cuh): D2 = D(N-2, M), D1 = D(N-1, M) rows; partial holds
+// gram_partial_elems(M, D2, D1) complex
+template <int M>
+int gram_apply_tmpl(const SpaceView& sp, uint32_t D2, uint32_t D1, const double2* C,
+                    double2* partial, double2* rho1, double2* rho2, cudaStream_t st);
+
+// H.C through the two-boson-annihilated space (pairhc_tmpl.cuh), M <= 8,
+// N >= 2: launch attributes (before any capture) and the two launches
+template <int M>
+int hcp_prepare_tmpl();
+template <int M>
+int hcp_apply_tmpl(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
+                   cudaStream_t st);
 
 // tune.cu: autotuner.  The launch variant of `kernel` for (current device,
 // N, M): the cached choice, else -- outside a stream capture -- each variant
@@ -64,8 +78,13 @@ int tune_pick(const char* kernel, int N, int M, int nvariants, cudaStream_t st,
 int tune_lookup(const char* kernel, int N, int M);  // -1 when not tuned
 
 // hamiltonian.cu
-int hc_prep(int M, const double2* d_hob, const double2* d_hint, double2* d_tab,
+// the packed coefficient table of h, g (and the pair matrix when sp has one)
+int hc_prep(const SpaceView& sp, const double2* d_hob, const double2* d_hint, double2* d_tab,
             cudaStream_t st);
+// whether the pair-space H.C applies to (N, M), and its scratch size in bytes
+bool hcp_eligible(int N, int M);
+size_t hcp_scratch_bytes(int N, int M);
+int hcp_prepare(int M);
 int hc_variant(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
                const HcEpilogue& ep, cudaStream_t st);
 int hc_apply(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
@@ -77,7 +96,12 @@ size_t dens_partial_elems(const SpaceView& sp);  // doubles2 in the partial buff
 int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
                double2* rho2, const int* d_desc, cudaStream_t st);
 int dens_descriptors(int M, int* host_desc);  // returns count; desc = 5 ints/elem
-// one-time launch attributes and the tuned variant, before any capture
+// rho1/rho2 by the per-row pass (dens_tmpl.cuh, generic kernel) and its
+// one-time launch attributes and tuned variant, before any capture
+int dens_apply_rows(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
+                    double2* rho2, const int* d_desc, cudaStream_t st);
+int dens_prepare_rows(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st);
+// set-up of dens_apply before any capture (nothing for the current kernels)
 int dens_prepare(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st);
 // kernels of density.cu also launched by noalloc.cu on its own scratch
 __global__ void dens_generic_kernel(SpaceView sp, const double2* __restrict__ C,

@@ -179,6 +179,8 @@ __global__ void lz_init_kernel(double2* scal, int* iflag, int m) {
 }
 
 // mode 0: SIL propagator y = U exp(-i D prop_dt) U^T e1
+// mode 2: the same up to a positive constant factor, for a step that
+//         renormalises y (imaginary time)
 // mode 1: lowest Ritz vector y = U[:, argmin D], energy -> scal[S_MISC+2]
 __global__ void lz_small_kernel(int mode, double2 prop_dt, double2* __restrict__ scal,
                                 int* __restrict__ iflag, double* __restrict__ z,
@@ -191,12 +193,19 @@ __global__ void lz_small_kernel(int mode, double2 prop_dt, double2* __restrict__
         e[k] = scal[S_OFFD + k].x;
     }
     iflag[2] = tridiag_ql(n, d, e, z);
-    if (mode == 0) {
+    if (mode != 1) {
+        // mode 2: exponents shifted by their maximum (a constant factor the
+        // renormalisation at the end of the step removes), so exp cannot
+        // overflow at |E| dt > 709; a real prop_dt has no shift either way
+        double shift = 0.0;
+        if (mode == 2 && prop_dt.y != 0.0)
+            for (int k = 0; k < n; k++)
+                shift = k == 0 ? d[k] * prop_dt.y : fmax(shift, d[k] * prop_dt.y);
         double2 aux[kSlots];
         for (int k = 0; k < n; k++) {
             // exp(-i d_k prop_dt), prop_dt complex
             const double re = d[k] * prop_dt.y, im = -d[k] * prop_dt.x;
-            const double mag = exp(re);
+            const double mag = exp(re - shift);
             double sn, cs;
             sincos(im, &sn, &cs);
             const double u = z[0 * n + k];
@@ -344,7 +353,8 @@ int sil_step(const SpaceCtx& s, LanczosWork& w, double2* d_C, int m, double2 pro
     MCTDHB_CUDA_TRY(cudaMemcpyAsync(w.V, d_C, (size_t)n * sizeof(double2),
                                     cudaMemcpyDeviceToDevice, st));
     if (lanczos_run(s, w, m, st)) return -1;
-    lz_small_kernel<<<1, 32, 0, st>>>(0, prop_dt, w.scal, w.iflag, zbuf(w), nullptr);
+    lz_small_kernel<<<1, 32, 0, st>>>(imagtime ? 2 : 0, prop_dt, w.scal, w.iflag, zbuf(w),
+                                      nullptr);
     lz_combine_kernel<<<w.vec_grid, 256, 0, st>>>(w.V, n, w.scal, w.iflag, d_C);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     if (imagtime) {

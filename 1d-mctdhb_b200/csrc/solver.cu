@@ -66,7 +66,7 @@ int phase_coefficients(mctdhb_solver_s* s, cudaStream_t st) {
     if (orb_matrices(o, s->d_orb, s->d_hob, s->d_hint, st)) return -1;
     if (s->M == 1) return 0;  // Gross-Pitaevskii: the coefficient is trivial
     SpaceCtx& sc = s->sp->sp;
-    if (hc_prep(s->M, s->d_hob, s->d_hint, sc.d_tab, st)) return -1;
+    if (hc_prep(sc.view, s->d_hob, s->d_hint, sc.d_tab, st)) return -1;
     const double2 pdt = s->imagtime ? make_double2(0.0, -s->dt) : make_double2(s->dt, 0.0);
     if (sil_step(sc, s->sp->lw, s->d_coef, s->lanczos_m, pdt, s->imagtime, st)) return -1;
     if (dens_apply(sc.view, s->d_coef, sc.d_dens_part, s->d_rho1, s->d_rho2, sc.d_dens_desc, st))
@@ -261,7 +261,7 @@ int mctdhb_solver_set_state(mctdhb_solver s, const void* orb, const void* coef) 
     if (orb_sync_rho1(s->orb, s->d_rho1, s->d_rinv, s->reg_fac, s->d_info, st)) return -1;
     if (orb_matrices(s->orb, s->d_orb, s->d_hob, s->d_hint, st)) return -1;
     if (s->M > 1) {
-        if (hc_prep(s->M, s->d_hob, s->d_hint, sc.d_tab, st)) return -1;
+        if (hc_prep(sc.view, s->d_hob, s->d_hint, sc.d_tab, st)) return -1;
         HcEpilogue ep;  // tune H.C on this state before the graph is captured
         hc_variant(sc.view, s->d_coef, s->sp->lw.out, sc.d_tab, ep, st);
     }

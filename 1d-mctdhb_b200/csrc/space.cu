@@ -75,6 +75,22 @@ int space_init(SpaceCtx& s, int N, int M) {
     MCTDHB_CUDA_TRY(cudaMemcpy(s.d_dens_desc, desc.data(), desc.size() * sizeof(int),
                                cudaMemcpyHostToDevice));
     MCTDHB_CUDA_TRY(cudaMalloc(&s.d_dens_part, dens_partial_elems(s.view) * sizeof(double2)));
+    // pair-space H.C: the pair matrix and its D(N-2, M) x P scratch; when the
+    // scratch cannot be had the space keeps the per-row kernel
+    if (hcp_eligible(N, M)) {
+        const size_t P = (size_t)M * (M + 1) / 2;
+        double2 *w = nullptr, *y = nullptr;
+        if (cudaMalloc(&w, P * P * sizeof(double2)) == cudaSuccess &&
+            cudaMalloc(&y, hcp_scratch_bytes(N, M)) == cudaSuccess && hcp_prepare(M) == 0) {
+            s.view.dim2 = (uint32_t)fock_dimension(N - 2, M);
+            s.view.pair_w = w;
+            s.view.pair_y = y;
+        } else {
+            cudaGetLastError();  // clear the allocation failure
+            cudaFree(w);
+            cudaFree(y);
+        }
+    }
     return 0;
 }
 
@@ -84,6 +100,8 @@ void space_release(SpaceCtx& s) {
     cudaFree(s.d_tab);
     cudaFree(s.d_dens_desc);
     cudaFree(s.d_dens_part);
+    cudaFree(s.view.pair_w);
+    cudaFree(s.view.pair_y);
     s = SpaceCtx();
 }
 

@@ -628,31 +628,55 @@ def run_serving(mb, torch, rates, njobs, imag_steps, real_steps, big_frac, nmax)
 # ---------------------------------------------------------------------------
 # the N=30 M=8 quench: configurational step and the H.C roofline
 # ---------------------------------------------------------------------------
-def quench_inputs(mb):
-    x = np.linspace(Q_XI, Q_XF, Q_GRID)
-    phi = hermite_orbitals(N_ORB, Q_GRID, Q_XI, Q_XF)
+SINGLE = {
+    "quench_n30_m8": dict(
+        N=N_PAR, M=N_ORB, G=Q_GRID, xi=Q_XI, xf=Q_XF, double_well=True, g=Q_G, m=Q_LZ,
+        dt=Q_DT, seed=1234,
+        workload="real-time quench N=30 M=8 (nc=10295472), grid 1024 on [-15,15], "
+                 "V=x^2/2+4exp(-x^2/0.5), g=0.1, Lanczos 6, dt=0.005"),
+    "memory_edge_n100_m6": dict(
+        N=100, M=6, G=2048, xi=-20.0, xf=20.0, double_well=False, g=0.02, m=LZ, dt=0.001,
+        seed=4321,
+        workload="single system at the memory edge N=100 M=6 (nc=96560646, 1.5 GB per "
+                 "vector), grid 2048 on [-20,20], V=x^2/2, g=0.02, Lanczos 5, dt=0.001, "
+                 "real time"),
+}
+
+
+def single_inputs(mb, c):
+    """h and g of the Hermite-Gaussian orbitals of a configuration (4th-order
+    periodic finite differences, Simpson weights) and seeded normalised
+    random coefficients"""
+    N, M, G, xi, xf = c["N"], c["M"], c["G"], c["xi"], c["xf"]
+    x = np.linspace(xi, xf, G)
+    phi = hermite_orbitals(M, G, xi, xf)
     dx = x[1] - x[0]
-    w = simpson_weights(Q_GRID, dx)
+    w = simpson_weights(G, dx)
     d = (np.roll(phi, 2, 1) - np.roll(phi, -2, 1) +
          8 * (np.roll(phi, -1, 1) - np.roll(phi, 1, 1))) / (12 * dx)
     hob = 0.5 * np.einsum("x,ax,bx->ab", w, d.conj(), d) + \
-        np.einsum("x,ax,bx->ab", w * trap(True, Q_GRID, Q_XI, Q_XF), phi.conj(), phi)
-    t = Q_G * np.einsum("x,ax,bx,cx,dx->abcd", w, phi.conj(), phi.conj(), phi, phi)
+        np.einsum("x,ax,bx->ab", w * trap(c["double_well"], G, xi, xf), phi.conj(), phi)
+    t = c["g"] * np.einsum("x,ax,bx,cx,dx->abcd", w, phi.conj(), phi.conj(), phi, phi)
     hint = np.ascontiguousarray(t.transpose(3, 2, 1, 0)).reshape(-1)
-    c0 = coefficients(int(mb.load().space_dimension(N_PAR, N_ORB)), np.random.default_rng(1234))
+    c0 = coefficients(int(mb.load().space_dimension(N, M)), np.random.default_rng(c["seed"]))
     return np.ascontiguousarray(hob), hint, c0
 
 
-def run_quench(mb, torch, steps, warmup):
+def run_single(mb, torch, name, steps, warmup):
+    """one system of a full-size configuration: the configurational step
+    (SIL + rho1 + rho2, one CUDA graph) and its H.C and density kernels"""
+    c = SINGLE[name]
+    N, M = c["N"], c["M"]
     stream = torch.cuda.current_stream()
-    hob, hint, c0 = quench_inputs(mb)
-    sp = mb.Space(N_PAR, N_ORB)
+    hob, hint, c0 = single_inputs(mb, c)
+    sp = mb.Space(N, M)
     nc = sp.dim
     d_c = torch.from_numpy(c0).cuda()
+    del c0
     sp.set_matrices(torch.from_numpy(hob.reshape(-1)).cuda(), torch.from_numpy(hint).cuda())
-    r1 = torch.empty(N_ORB * N_ORB, dtype=torch.complex128, device="cuda")
-    r2 = torch.empty(N_ORB ** 4, dtype=torch.complex128, device="cuda")
-    step = mb.Step(sp, d_c, r1, r2, Q_LZ, Q_DT, False)
+    r1 = torch.empty(M * M, dtype=torch.complex128, device="cuda")
+    r2 = torch.empty(M ** 4, dtype=torch.complex128, device="cuda")
+    step = mb.Step(sp, d_c, r1, r2, c["m"], c["dt"], False)
     for _ in range(warmup):
         step.launch(stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -683,19 +707,20 @@ def run_quench(mb, torch, steps, warmup):
     b.record(stream)
     torch.cuda.synchronize()
     t_dn = a.elapsed_time(b) / reps / 1000.0
-    G = distinct_couplings(N_PAR, N_ORB)
+    G = distinct_couplings(N, M)
     b_hc = 32.0 * nc + 16.0 * G
     b_dn = 16.0 * nc + 16.0 * G
     peak, kind = peaks()
+    sp.close()
     del sp, d_c, hc_out
-    return {"workload": "real-time quench N=30 M=8 (nc=10295472), grid 1024 on [-15,15], "
-                        "V=x^2/2+4exp(-x^2/0.5), g=0.1, Lanczos 6, dt=0.005",
-            "step": "SIL(6 H.C) + rho1 + rho2, one CUDA graph",
-            "steps_per_s": 1000.0 / t_step, "ms_per_step": t_step,
-            "hc": {"kernel": "hc_kernel<8>", "ms_per_launch": t_hc * 1e3,
+    torch.cuda.empty_cache()
+    return {"workload": c["workload"],
+            "step": f"SIL({c['m']} H.C) + rho1 + rho2, one CUDA graph",
+            "steps_per_s": 1000.0 / t_step, "ms_per_step": t_step, "norm_after": norm,
+            "hc": {"kernel": f"hc_kernel<{M}>", "ms_per_launch": t_hc * 1e3,
                    "algorithmic_bytes_per_launch": b_hc, "achieved_gbs": b_hc / t_hc / 1e9,
                    "peak": peak, "frac": b_hc / t_hc / 1e9 / peak, "peak_source": kind,
-                   "traffic": ncu_traffic().get("hc_bytes_per_launch")},
+                   "traffic": ncu_traffic().get(f"hc_n{N}_m{M}_bytes_per_launch")},
             "density": {"ms_per_launch": t_dn * 1e3, "algorithmic_bytes_per_launch": b_dn,
                         "achieved_gbs": b_dn / t_dn / 1e9}}
 
@@ -802,7 +827,8 @@ def run_gpu(args):
         "max_rel_diff": max(abs(e_batch[i] - e_plain[i]) / abs(e_plain[i]) for i in cmp_idx),
         "jobs": len(cmp_idx), "what": "energy after the same number of steps, batched vs plain"}
 
-    line["quench_n30_m8"] = run_quench(mb, torch, max(3, args.steps // 2), args.warmup)
+    for name in SINGLE:
+        line[name] = run_single(mb, torch, name, max(3, args.steps // 2), args.warmup)
     line["e2e"] = e2e_batch(mb, torch, jobs, args.steps)
     if not args.no_serving:
         line["serving"] = run_serving(mb, torch, [float(r) for r in args.serve_rates.split(",")],
@@ -836,6 +862,35 @@ def run_profile():
     print("profile run done")
 
 
+def run_profile_kernels():
+    """the single-system kernels of the N=30 M=8 quench for ncu: set-up and
+    one untimed H.C + density outside the profiled range, then one H.C and
+    one density launch inside it (cudaProfilerStart/Stop; use
+    --profile-from-start off)"""
+    import torch
+
+    import mctdhb_b200 as mb
+
+    c = SINGLE["quench_n30_m8"]
+    hob, hint, c0 = single_inputs(mb, c)
+    sp = mb.Space(c["N"], c["M"])
+    d_c = torch.from_numpy(c0).cuda()
+    sp.set_matrices(torch.from_numpy(hob.reshape(-1)).cuda(), torch.from_numpy(hint).cuda())
+    r1 = torch.empty(c["M"] ** 2, dtype=torch.complex128, device="cuda")
+    r2 = torch.empty(c["M"] ** 4, dtype=torch.complex128, device="cuda")
+    out = torch.empty_like(d_c)
+    sp.apply_hamiltonian(d_c, out)
+    sp.density_matrices(d_c, r1, r2)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    sp.apply_hamiltonian(d_c, out)
+    sp.density_matrices(d_c, r1, r2)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    sp.close()
+    print("profile run done")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -854,9 +909,13 @@ def main():
     ap.add_argument("--serve-nmax", type=int, default=30)
     ap.add_argument("--profile", action="store_true",
                     help="one profiled batch step of a small mix (for ncu captures)")
+    ap.add_argument("--profile-kernels", action="store_true",
+                    help="one profiled H.C and density launch at N=30 M=8 (for ncu captures)")
     args = ap.parse_args()
     if args.profile:
         run_profile()
+    elif args.profile_kernels:
+        run_profile_kernels()
     elif args.impl == "reference":
         run_reference(args)
     else:

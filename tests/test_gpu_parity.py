@@ -318,16 +318,18 @@ def test_sync_density_matrices_dropin(gpu, oracle):
 
 
 # ---------------------------------------------------------------------------
-# full size (N=30, M=8): size-independent properties + sampled rows
+# full sizes (N=30 M=8, nc = 10,295,472; N=100 M=6, nc = 96,560,646 -- 1.5 GB
+# per vector, beyond the reference's 32-bit map guards): size-independent
+# properties + sampled rows
 # ---------------------------------------------------------------------------
-def test_hc_large_properties(gpu, oracle):
+@pytest.mark.parametrize("N,M,nc_expected", [(30, 8, 10295472), (100, 6, 96560646)])
+def test_hc_large_properties(gpu, oracle, N, M, nc_expected):
     import torch
 
-    N, M = 30, 8
     rng = np.random.default_rng(99)
     sp = gpu.Space(N, M)
     nc = sp.dim
-    assert nc == 10295472
+    assert nc == nc_expected
     h, g = rand_hob(rng, M), phys_hint(rng, M)
     sp.set_matrices(dev(h), dev(g))
     u = torch.randn(nc, dtype=torch.complex128, device="cuda", generator=None)
@@ -355,3 +357,41 @@ def test_hc_large_properties(gpu, oracle):
     for r0 in (0, nc // 3, nc // 2 + 12345, nc - 2000):
         ref = oracle.apply_hamiltonian(N, M, un, h, g, rows=(r0, r0 + 2000))
         assert rel_err(hun[r0:r0 + 2000], ref[r0:r0 + 2000]) < TOL
+    del u, v, hu, hv
+    sp.close()
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("N,M,m", [(30, 8, 6), (100, 6, 5)])
+def test_sil_large_norm_and_energy(gpu, N, M, m):
+    """real-time SIL steps conserve the norm to 1e-12 and the energy
+    <C|H|C> to 1e-10 (H is time independent within the step); an
+    imaginary-time step lowers the energy and renormalises"""
+    import torch
+
+    rng = np.random.default_rng(7 * N + M)
+    sp = gpu.Space(N, M)
+    nc = sp.dim
+    h, g = rand_hob(rng, M), phys_hint(rng, M)
+    sp.set_matrices(dev(h), dev(g))
+    c = torch.randn(nc, dtype=torch.complex128, device="cuda")
+    c /= torch.linalg.vector_norm(c)
+    hc = torch.empty_like(c)
+
+    def energy():
+        sp.apply_hamiltonian(c, hc)
+        return torch.vdot(c, hc).item()
+
+    e0 = energy()
+    for _ in range(3):
+        sp.sil_step(c, m, 0.005, False)
+    torch.cuda.synchronize()
+    assert abs(torch.linalg.vector_norm(c).item() - 1.0) < 1e-12
+    e1 = energy()
+    assert abs(e1 - e0) < 1e-10 * abs(e0)
+    sp.sil_step(c, m, 0.005, True)
+    assert abs(torch.linalg.vector_norm(c).item() - 1.0) < 1e-12
+    assert energy().real < e1.real
+    del c, hc
+    sp.close()
+    torch.cuda.empty_cache()
