@@ -33,6 +33,7 @@
 #include "batch_kernels.h"
 #include "common.cuh"
 #include "engine.h"
+#include "gram.h"
 #include "kernels.h"
 #include "moves.cuh"
 #include "orbital.h"
@@ -45,10 +46,10 @@ size_t al256(size_t b) { return (b + 255) / 256 * 256; }
 
 // sizes of one job's parts, in the arena order
 struct JobLayout {
-    uint32_t nc = 0;
-    int vtiles = 0, dslices = 0, dchunks = 0, E = 0, EP = 0;
-    size_t o_orb, o_stage, o_H, o_pot, o_w, o_Q, o_hob, o_hint, o_tab, o_rho1, o_rho2, o_rinv,
-        o_work, o_T, o_sq, o_g, o_V, o_out, o_part, o_dpart, total;
+    uint32_t nc = 0, D1 = 0, D2 = 0;
+    int vtiles = 0, ytiles = 0, gs[3] = {0, 0, 0}, gk[3] = {0, 0, 0};
+    size_t o_orb, o_stage, o_H, o_pot, o_w, o_Q, o_hob, o_hint, o_pw, o_rho1, o_rho2, o_rinv,
+        o_work, o_T, o_sq, o_g, o_V, o_out, o_part, o_py, o_gpart, total;
 };
 
 int job_layout(int N, int M, int G, int lz, JobLayout& L) {
@@ -56,8 +57,9 @@ int job_layout(int N, int M, int G, int lz, JobLayout& L) {
         set_error("batch: %d orbitals outside %d..%d", M, kBatchMinOrb, kBatchMaxOrb);
         return -1;
     }
-    if (N < 1 || N > 10000) {
-        set_error("batch: %d particles outside 1..10000", N);
+    if (N < 2 || N > 10000) {
+        set_error("batch: %d particles outside 2..10000 (one boson: the single-system solver)",
+                  N);
         return -1;
     }
     if (G < 5 || G > kBatchMaxGrid) {
@@ -70,13 +72,19 @@ int job_layout(int N, int M, int G, int lz, JobLayout& L) {
         return -1;
     }
     L.nc = (uint32_t)dim;
+    L.D1 = (uint32_t)fock_dimension(N - 1, M);
+    L.D2 = (uint32_t)fock_dimension(N - 2, M);
     L.vtiles = (int)((dim + kBatchVecRows - 1) / kBatchVecRows);
-    const uint64_t chunks = (dim + kBatchDensThreads - 1) / kBatchDensThreads;
-    L.dchunks = (int)std::max<uint64_t>(8, (chunks + kBatchMaxSlices - 1) / kBatchMaxSlices);
-    L.dslices = (int)((chunks + L.dchunks - 1) / L.dchunks);
-    L.E = dens_nelem(M);
-    L.EP = (L.E + 7) / 8 * 8;
+    L.ytiles = (int)((L.D2 + batch_pair_rows(M) - 1) / batch_pair_rows(M));
+    // Gram slices: consecutive row tiles, at most kBatchMaxSlices per order
+    for (int R = 1; R <= 2; R++) {
+        const uint64_t Dp = R == 2 ? L.D2 : L.D1;
+        const uint64_t ntr = (Dp + gram_rows(M, R) - 1) / gram_rows(M, R);
+        L.gk[R] = (int)std::max<uint64_t>(1, (ntr + kBatchMaxSlices - 1) / kBatchMaxSlices);
+        L.gs[R] = (int)((ntr + L.gk[R] - 1) / L.gk[R]);
+    }
     const size_t n = (size_t)M * G, M2 = (size_t)M * M, M4 = M2 * M2, z = sizeof(double2);
+    const size_t P = (size_t)M * (M + 1) / 2;
     size_t o = 0;
     auto take = [&](size_t bytes) {
         const size_t at = o;
@@ -91,7 +99,7 @@ int job_layout(int N, int M, int G, int lz, JobLayout& L) {
     L.o_Q = take(M4 * z);
     L.o_hob = take(M2 * z);
     L.o_hint = take(M4 * z);
-    L.o_tab = take((size_t)hc_table_size(M) * z);
+    L.o_pw = take(P * P * z);
     L.o_rho1 = take(M2 * z);
     L.o_rho2 = take(M4 * z);
     L.o_rinv = take(M2 * z);
@@ -102,7 +110,9 @@ int job_layout(int N, int M, int G, int lz, JobLayout& L) {
     L.o_V = take((size_t)lz * dim * z);
     L.o_out = take((size_t)dim * z);
     L.o_part = take((size_t)kBatchMaxLz * L.vtiles * z);
-    L.o_dpart = take((size_t)L.dslices * L.EP * z);
+    L.o_py = take((size_t)L.D2 * P * z);
+    L.o_gpart = take(((size_t)L.gs[2] * gram_entries(M, 2) + (size_t)L.gs[1] * gram_entries(M, 1)) *
+                     z);
     L.total = o;
     return 0;
 }
@@ -128,20 +138,23 @@ struct mctdhb_batch_s {
     BatchSlot* d_slots = nullptr;
     double2* d_scal = nullptr;  // max_slots x BS_TOTAL
     int* d_flags = nullptr;     // max_slots x BF_TOTAL
-    int* d_desc[kNumM] = {};
-    // work lists (device) and their pinned host images
-    size_t cap_vec = 0, cap_hc = 0, cap_dn = 0;
+    // work lists (device) and their pinned host images: vector tiles, and the
+    // per-M lists LIST_HG, LIST_HY, LIST_G2, LIST_G1 (batch.h)
+    size_t cap_vec = 0, cap[kBatchLists] = {};
     int* d_list = nullptr;  // [0] count, [1..] slots
-    BatchTile *d_vec = nullptr, *d_hc = nullptr, *d_dn = nullptr;
-    int* d_cnt = nullptr;  // [0] vec count, [1..9] hc off, [10..18] hc cnt, [19..27] dn off, [28..36] dn cnt
+    BatchTile* d_vec = nullptr;
+    BatchTile* d_tl[kBatchLists] = {};
+    int* d_cnt = nullptr;  // count block (batch.h)
     int* h_list = nullptr;
-    BatchTile *h_vec = nullptr, *h_hc = nullptr, *h_dn = nullptr;
+    BatchTile* h_vec = nullptr;
+    BatchTile* h_tl[kBatchLists] = {};
     int* h_cnt = nullptr;
-    // single-slot lists of the admission set-up
-    int* d_pro = nullptr;  // [0] 1, [1] slot, then 1 + 2 kNumM ints of offsets / counts
-    BatchTile* d_pro_dn = nullptr;
+    // single-slot lists of the admission set-up: [0] 1, [1] slot, then a
+    // count block; Gram slices of R = 2 at d_pro_g, of R = 1 after them
+    int* d_pro = nullptr;
+    BatchTile* d_pro_g = nullptr;
     int* h_pro = nullptr;
-    BatchTile* h_pro_dn = nullptr;
+    BatchTile* h_pro_g = nullptr;
     int* h_flags = nullptr;
     double2* h_scal = nullptr;
     unsigned present_mask = 0;  // orbital counts present in the lists
@@ -159,11 +172,7 @@ struct mctdhb_batch_s {
 namespace {
 
 int* cnt_vec(int* c) { return c; }
-int* hc_off(int* c) { return c + 1; }
-int* hc_cnt(int* c) { return c + 1 + kNumM; }
-int* dn_off(int* c) { return c + 1 + 2 * kNumM; }
-int* dn_cnt(int* c) { return c + 1 + 3 * kNumM; }
-constexpr int kCntInts = 1 + 4 * kNumM;
+constexpr int kCntInts = kBatchCntInts;
 
 void drop_graph(mctdhb_batch_s* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -219,21 +228,29 @@ int rebuild_lists(mctdhb_batch_s* b) {
     }
     b->h_list[0] = ns;
     cnt_vec(b->h_cnt)[0] = (int)nv;
-    size_t nh = 0, nd = 0;
+    size_t n[kBatchLists] = {};
     for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++) {
-        hc_off(b->h_cnt)[M] = (int)nh;
-        dn_off(b->h_cnt)[M] = (int)nd;
+        for (int li = 0; li < kBatchLists; li++) batch_offs(b->h_cnt, li)[M] = (int)n[li];
         for (int q = 0; q < ns; q++) {
             const int s = b->h_list[1 + q];
             const HostSlot& h = b->hs[s];
             if (h.d.M != M) continue;
-            for (uint32_t r = 0; r < h.L.nc; r += kBatchHcRows) b->h_hc[nh++] = BatchTile{s, r};
-            for (int sl = 0; sl < h.L.dslices; sl++) b->h_dn[nd++] = BatchTile{s, (uint32_t)sl};
+            BatchTile* const* tl = b->h_tl;
+            auto push = [&](int li, uint32_t idx) {
+                if (n[li] < b->cap[li]) tl[li][n[li]] = BatchTile{s, idx};
+                n[li]++;
+            };
+            for (uint32_t r = 0; r < h.L.nc; r += kBatchHcRows) push(LIST_HG, r);
+            for (int t = 0; t < h.L.ytiles; t++) push(LIST_HY, (uint32_t)t);
+            for (int g = 0; g < h.L.gs[2]; g++) push(LIST_G2, (uint32_t)g);
+            for (int g = 0; g < h.L.gs[1]; g++) push(LIST_G1, (uint32_t)g);
         }
-        hc_cnt(b->h_cnt)[M] = (int)nh - hc_off(b->h_cnt)[M];
-        dn_cnt(b->h_cnt)[M] = (int)nd - dn_off(b->h_cnt)[M];
+        for (int li = 0; li < kBatchLists; li++)
+            batch_cnts(b->h_cnt, li)[M] = (int)n[li] - batch_offs(b->h_cnt, li)[M];
     }
-    if (nv > b->cap_vec || nh > b->cap_hc || nd > b->cap_dn) {
+    bool over = nv > b->cap_vec;
+    for (int li = 0; li < kBatchLists; li++) over = over || n[li] > b->cap[li];
+    if (over) {
         set_error("batch: work lists exceed their capacity");
         return -1;
     }
@@ -245,41 +262,56 @@ int rebuild_lists(mctdhb_batch_s* b) {
     if (nv)
         MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_vec, b->h_vec, nv * sizeof(BatchTile),
                                         cudaMemcpyHostToDevice, st));
-    if (nh)
-        MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_hc, b->h_hc, nh * sizeof(BatchTile),
-                                        cudaMemcpyHostToDevice, st));
-    if (nd)
-        MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_dn, b->h_dn, nd * sizeof(BatchTile),
-                                        cudaMemcpyHostToDevice, st));
+    for (int li = 0; li < kBatchLists; li++)
+        if (n[li])
+            MCTDHB_CUDA_TRY(cudaMemcpyAsync(b->d_tl[li], b->h_tl[li], n[li] * sizeof(BatchTile),
+                                            cudaMemcpyHostToDevice, st));
     b->present_mask = mask;
     b->lists_dirty = false;
     return 0;
 }
 
-int hc_group(int M, const BatchSlot* slots, const BatchTile* tiles, const int* off,
+// H.C of Lanczos iteration `iter` of the slots of orbital count M
+int hc_group(int M, const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
              const int* cnt, int iter, cudaStream_t st) {
     switch (M) {
-        case 2: return hc_batch_launch<2>(slots, tiles, off, cnt, iter, st);
-        case 3: return hc_batch_launch<3>(slots, tiles, off, cnt, iter, st);
-        case 4: return hc_batch_launch<4>(slots, tiles, off, cnt, iter, st);
-        case 5: return hc_batch_launch<5>(slots, tiles, off, cnt, iter, st);
-        case 6: return hc_batch_launch<6>(slots, tiles, off, cnt, iter, st);
-        case 7: return hc_batch_launch<7>(slots, tiles, off, cnt, iter, st);
-        case 8: return hc_batch_launch<8>(slots, tiles, off, cnt, iter, st);
+        case 2: return hcp_batch_launch<2>(slots, hy, hg, cnt, iter, st);
+        case 3: return hcp_batch_launch<3>(slots, hy, hg, cnt, iter, st);
+        case 4: return hcp_batch_launch<4>(slots, hy, hg, cnt, iter, st);
+        case 5: return hcp_batch_launch<5>(slots, hy, hg, cnt, iter, st);
+        case 6: return hcp_batch_launch<6>(slots, hy, hg, cnt, iter, st);
+        case 7: return hcp_batch_launch<7>(slots, hy, hg, cnt, iter, st);
+        case 8: return hcp_batch_launch<8>(slots, hy, hg, cnt, iter, st);
     }
     return 0;
 }
 
-int dens_group(int M, const BatchSlot* slots, const BatchTile* tiles, const int* off,
-               const int* cnt, cudaStream_t st) {
+// rho1 / rho2 of the slots of orbital count M (the slot list gives the
+// finalize blocks)
+int dens_group(int M, const BatchSlot* slots, const BatchTile* g2, const BatchTile* g1,
+               const int* cnt, const int* list, const int* nlist, int nblocks, cudaStream_t st) {
     switch (M) {
-        case 2: return dens_batch_launch<2>(slots, tiles, off, cnt, st);
-        case 3: return dens_batch_launch<3>(slots, tiles, off, cnt, st);
-        case 4: return dens_batch_launch<4>(slots, tiles, off, cnt, st);
-        case 5: return dens_batch_launch<5>(slots, tiles, off, cnt, st);
-        case 6: return dens_batch_launch<6>(slots, tiles, off, cnt, st);
-        case 7: return dens_batch_launch<7>(slots, tiles, off, cnt, st);
-        case 8: return dens_batch_launch<8>(slots, tiles, off, cnt, st);
+        case 2: return gram_batch_launch<2>(slots, g2, g1, cnt, list, nlist, nblocks, st);
+        case 3: return gram_batch_launch<3>(slots, g2, g1, cnt, list, nlist, nblocks, st);
+        case 4: return gram_batch_launch<4>(slots, g2, g1, cnt, list, nlist, nblocks, st);
+        case 5: return gram_batch_launch<5>(slots, g2, g1, cnt, list, nlist, nblocks, st);
+        case 6: return gram_batch_launch<6>(slots, g2, g1, cnt, list, nlist, nblocks, st);
+        case 7: return gram_batch_launch<7>(slots, g2, g1, cnt, list, nlist, nblocks, st);
+        case 8: return gram_batch_launch<8>(slots, g2, g1, cnt, list, nlist, nblocks, st);
+    }
+    return 0;
+}
+
+// launch attributes of the per-M kernels (before any capture)
+int prepare_group(int M) {
+    switch (M) {
+        case 2: return batch_prepare<2>();
+        case 3: return batch_prepare<3>();
+        case 4: return batch_prepare<4>();
+        case 5: return batch_prepare<5>();
+        case 6: return batch_prepare<6>();
+        case 7: return batch_prepare<7>();
+        case 8: return batch_prepare<8>();
     }
     return 0;
 }
@@ -322,7 +354,7 @@ int enqueue_step(mctdhb_batch_s* b, unsigned mask) {
     MCTDHB_CUDA_TRY(cudaGetLastError());
     auto hc = [&](int iter) {
         return per_group(b, mask, [&](int M, cudaStream_t s) {
-            return hc_group(M, S, b->d_hc, hc_off(b->d_cnt), hc_cnt(b->d_cnt), iter, s);
+            return hc_group(M, S, b->d_tl[LIST_HY], b->d_tl[LIST_HG], b->d_cnt, iter, s);
         });
     };
     // Lanczos (multiconfig_lanczos.c:12-90)
@@ -349,10 +381,10 @@ int enqueue_step(mctdhb_batch_s* b, unsigned mask) {
     MCTDHB_CUDA_TRY(cudaGetLastError());
     // densities, rho1 synchronisation, energy, stop rules
     if (per_group(b, mask, [&](int M, cudaStream_t s) {
-            return dens_group(M, S, b->d_dn, dn_off(b->d_cnt), dn_cnt(b->d_cnt), s);
+            return dens_group(M, S, b->d_tl[LIST_G2], b->d_tl[LIST_G1], b->d_cnt, sl, nL, sgrid,
+                              s);
         }))
         return -1;
-    bt_dens_finalize_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL);
     bt_tail_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 0);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
@@ -377,7 +409,7 @@ int ensure_graph(mctdhb_batch_s* b) {
     drop_graph(b);
     for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++)
         if (b->present_mask >> M & 1)
-            if (dens_group(M, nullptr, nullptr, nullptr, nullptr, b->st)) return -1;
+            if (prepare_group(M)) return -1;
     cudaError_t e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) {
         set_error("batch: capture: %s", cudaGetErrorString(e));
@@ -445,27 +477,30 @@ int mctdhb_batch_create(int max_slots, size_t arena_bytes, int lanczos_iter, mct
     };
     // every job holds at least (lz + 1) nc complex numbers: bounds the tiles
     const size_t max_rows = b->arena_bytes / ((size_t)(lanczos_iter + 1) * sizeof(double2));
+    // (the Y tiles and Gram row tiles have at least 64 rows each)
     b->cap_vec = max_rows / kBatchVecRows + max_slots;
-    b->cap_hc = max_rows / kBatchHcRows + max_slots;
-    b->cap_dn = max_rows / (kBatchDensThreads * 8) + max_slots;
-    if (cudaMalloc(&b->arena, std::max<size_t>(b->arena_bytes, 256)) ||
-        cudaMalloc(&b->d_slots, max_slots * sizeof(BatchSlot)) ||
-        cudaMalloc(&b->d_scal, (size_t)max_slots * BS_TOTAL * sizeof(double2)) ||
-        cudaMalloc(&b->d_flags, (size_t)max_slots * BF_TOTAL * sizeof(int)) ||
-        cudaMalloc(&b->d_list, (max_slots + 1) * sizeof(int)) ||
-        cudaMalloc(&b->d_vec, b->cap_vec * sizeof(BatchTile)) ||
-        cudaMalloc(&b->d_hc, b->cap_hc * sizeof(BatchTile)) ||
-        cudaMalloc(&b->d_dn, b->cap_dn * sizeof(BatchTile)) ||
-        cudaMalloc(&b->d_cnt, kCntInts * sizeof(int)) ||
-        cudaMalloc(&b->d_pro, (2 + kCntInts) * sizeof(int)) ||
-        cudaMalloc(&b->d_pro_dn, kBatchMaxSlices * sizeof(BatchTile)) ||
-        cudaMallocHost(&b->h_list, (max_slots + 1) * sizeof(int)) ||
-        cudaMallocHost(&b->h_vec, b->cap_vec * sizeof(BatchTile)) ||
-        cudaMallocHost(&b->h_hc, b->cap_hc * sizeof(BatchTile)) ||
-        cudaMallocHost(&b->h_dn, b->cap_dn * sizeof(BatchTile)) ||
-        cudaMallocHost(&b->h_cnt, kCntInts * sizeof(int)) ||
-        cudaMallocHost(&b->h_pro, (2 + kCntInts) * sizeof(int)) ||
-        cudaMallocHost(&b->h_pro_dn, kBatchMaxSlices * sizeof(BatchTile)) ||
+    b->cap[LIST_HG] = max_rows / kBatchHcRows + max_slots;
+    b->cap[LIST_HY] = max_rows / 64 + max_slots;
+    b->cap[LIST_G2] = max_rows / 64 + max_slots;
+    b->cap[LIST_G1] = max_rows / 64 + max_slots;
+    bool bad = cudaMalloc(&b->arena, std::max<size_t>(b->arena_bytes, 256)) ||
+               cudaMalloc(&b->d_slots, max_slots * sizeof(BatchSlot)) ||
+               cudaMalloc(&b->d_scal, (size_t)max_slots * BS_TOTAL * sizeof(double2)) ||
+               cudaMalloc(&b->d_flags, (size_t)max_slots * BF_TOTAL * sizeof(int)) ||
+               cudaMalloc(&b->d_list, (max_slots + 1) * sizeof(int)) ||
+               cudaMalloc(&b->d_vec, b->cap_vec * sizeof(BatchTile)) ||
+               cudaMalloc(&b->d_cnt, kCntInts * sizeof(int)) ||
+               cudaMalloc(&b->d_pro, (2 + kCntInts) * sizeof(int)) ||
+               cudaMalloc(&b->d_pro_g, 2 * kBatchMaxSlices * sizeof(BatchTile)) ||
+               cudaMallocHost(&b->h_list, (max_slots + 1) * sizeof(int)) ||
+               cudaMallocHost(&b->h_vec, b->cap_vec * sizeof(BatchTile)) ||
+               cudaMallocHost(&b->h_cnt, kCntInts * sizeof(int)) ||
+               cudaMallocHost(&b->h_pro, (2 + kCntInts) * sizeof(int)) ||
+               cudaMallocHost(&b->h_pro_g, 2 * kBatchMaxSlices * sizeof(BatchTile));
+    for (int li = 0; li < kBatchLists && !bad; li++)
+        bad = cudaMalloc(&b->d_tl[li], b->cap[li] * sizeof(BatchTile)) ||
+              cudaMallocHost(&b->h_tl[li], b->cap[li] * sizeof(BatchTile));
+    if (bad ||
         cudaMallocHost(&b->h_flags, (size_t)max_slots * BF_TOTAL * sizeof(int)) ||
         cudaMallocHost(&b->h_scal, (size_t)max_slots * BS_TOTAL * sizeof(double2)) ||
         cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) ||
@@ -485,17 +520,6 @@ int mctdhb_batch_create(int max_slots, size_t arena_bytes, int lanczos_iter, mct
         set_error("mctdhb_batch_create: initialisation failed");
         return fail();
     }
-    for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++) {
-        const int E = dens_descriptors(M, nullptr);
-        std::vector<int> desc((size_t)5 * E);
-        dens_descriptors(M, desc.data());
-        if (cudaMalloc(&b->d_desc[M], desc.size() * sizeof(int)) ||
-            cudaMemcpy(b->d_desc[M], desc.data(), desc.size() * sizeof(int),
-                       cudaMemcpyHostToDevice)) {
-            set_error("mctdhb_batch_create: descriptor upload failed");
-            return fail();
-        }
-    }
     if (b->arena_bytes) b->free_ranges[0] = b->arena_bytes;
     if (rebuild_lists(b)) return fail();
     *out = b;
@@ -512,23 +536,22 @@ void mctdhb_batch_destroy(mctdhb_batch b) {
     cudaFree(b->d_flags);
     cudaFree(b->d_list);
     cudaFree(b->d_vec);
-    cudaFree(b->d_hc);
-    cudaFree(b->d_dn);
     cudaFree(b->d_cnt);
     cudaFree(b->d_pro);
-    cudaFree(b->d_pro_dn);
+    cudaFree(b->d_pro_g);
+    for (int li = 0; li < kBatchLists; li++) {
+        cudaFree(b->d_tl[li]);
+        cudaFreeHost(b->h_tl[li]);
+    }
     for (int M = 0; M < kNumM; M++) {
-        cudaFree(b->d_desc[M]);
         if (b->side[M]) cudaStreamDestroy(b->side[M]);
         if (b->ev_join[M]) cudaEventDestroy(b->ev_join[M]);
     }
     cudaFreeHost(b->h_list);
     cudaFreeHost(b->h_vec);
-    cudaFreeHost(b->h_hc);
-    cudaFreeHost(b->h_dn);
     cudaFreeHost(b->h_cnt);
     cudaFreeHost(b->h_pro);
-    cudaFreeHost(b->h_pro_dn);
+    cudaFreeHost(b->h_pro_g);
     cudaFreeHost(b->h_flags);
     cudaFreeHost(b->h_scal);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
@@ -584,8 +607,12 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     d.nc = L.nc;
     d.max_steps = job->max_steps;
     d.vtiles = L.vtiles;
-    d.dslices = L.dslices;
-    d.dchunks = L.dchunks;
+    d.ytiles = L.ytiles;
+    for (int R = 0; R < 3; R++) {
+        d.gs[R] = L.gs[R];
+        d.gk[R] = L.gk[R];
+    }
+    d.D1 = L.D1;
     d.dt = job->dt;
     d.etol = job->energy_tol;
     d.reg_fac = reg;
@@ -604,15 +631,16 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     d.sp.dim = L.nc;
     d.sp.T = (const uint32_t*)P(L.o_T);
     d.sp.sq = (const double*)P(L.o_sq);
+    d.sp.dim2 = L.D2;
+    d.sp.pair_w = (double2*)P(L.o_pw);
+    d.sp.pair_y = (double2*)P(L.o_py);
     d.g = (const double*)P(L.o_g);
-    d.desc = b->d_desc[M];
     d.orb = (double2*)P(L.o_orb);
     d.stage = (double2*)P(L.o_stage);
     d.H = (double2*)P(L.o_H);
     d.Q = (double2*)P(L.o_Q);
     d.hob = (double2*)P(L.o_hob);
     d.hint = (double2*)P(L.o_hint);
-    d.tab = (double2*)P(L.o_tab);
     d.rho1 = (double2*)P(L.o_rho1);
     d.rho2 = (double2*)P(L.o_rho2);
     d.rinv = (double2*)P(L.o_rinv);
@@ -620,7 +648,7 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     d.V = (double2*)P(L.o_V);
     d.out = (double2*)P(L.o_out);
     d.part = (double2*)P(L.o_part);
-    d.dpart = (double2*)P(L.o_dpart);
+    d.gpart = (double2*)P(L.o_gpart);
     d.scal = b->d_scal + (size_t)s * BS_TOTAL;
     d.flags = b->d_flags + (size_t)s * BF_TOTAL;
     // host-side tables (the rank table of space_init, Simpson weights)
@@ -663,23 +691,26 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     hp[0] = 1;
     hp[1] = s;
     int* pc = hp + 2;
-    dn_off(pc)[M] = 0;
-    dn_cnt(pc)[M] = L.dslices;
-    for (int q = 0; q < L.dslices; q++) b->h_pro_dn[q] = BatchTile{s, (uint32_t)q};
+    batch_offs(pc, LIST_G2)[M] = 0;
+    batch_cnts(pc, LIST_G2)[M] = L.gs[2];
+    batch_offs(pc, LIST_G1)[M] = 0;
+    batch_cnts(pc, LIST_G1)[M] = L.gs[1];
+    for (int q = 0; q < L.gs[2]; q++) b->h_pro_g[q] = BatchTile{s, (uint32_t)q};
+    for (int q = 0; q < L.gs[1]; q++) b->h_pro_g[kBatchMaxSlices + q] = BatchTile{s, (uint32_t)q};
     const int* pl = b->d_pro;
-    int* dpc = b->d_pro + 2;
+    const int* dpc = b->d_pro + 2;
     if (cudaMemcpyAsync(b->d_pro, hp, (2 + kCntInts) * sizeof(int), cudaMemcpyHostToDevice, st) ||
-        cudaMemcpyAsync(b->d_pro_dn, b->h_pro_dn, L.dslices * sizeof(BatchTile),
+        cudaMemcpyAsync(b->d_pro_g, b->h_pro_g, 2 * kBatchMaxSlices * sizeof(BatchTile),
                         cudaMemcpyHostToDevice, st)) {
         set_error("mctdhb_batch_admit: upload failed");
         return undo();
     }
     bt_orbital_kernel<<<1, kBatchOrbThreads, kBatchMaxGrid * sizeof(double), st>>>(
         b->d_slots, pl + 1, pl, 1);
-    if (dens_group(M, nullptr, nullptr, nullptr, nullptr, st) ||
-        dens_group(M, b->d_slots, b->d_pro_dn, dn_off(dpc), dn_cnt(dpc), st))
+    if (prepare_group(M) ||
+        dens_group(M, b->d_slots, b->d_pro_g, b->d_pro_g + kBatchMaxSlices, dpc, pl + 1, pl, 1,
+                   st))
         return undo();
-    bt_dens_finalize_kernel<<<1, kBatchVecThreads, 0, st>>>(b->d_slots, pl + 1, pl);
     bt_tail_kernel<<<1, kBatchVecThreads, 0, st>>>(b->d_slots, pl + 1, pl, 1);
     const cudaError_t e = cudaGetLastError();
     const cudaError_t e2 = cudaStreamSynchronize(st);
@@ -812,7 +843,8 @@ int mctdhb_batch_launch_hc(mctdhb_batch b, int norb) {
     }
     std::lock_guard<std::mutex> lk(b->mu);
     if (b->lists_dirty && rebuild_lists(b)) return -1;
-    return hc_group(norb, b->d_slots, b->d_hc, hc_off(b->d_cnt), hc_cnt(b->d_cnt), 0, b->st);
+    if (prepare_group(norb)) return -1;
+    return hc_group(norb, b->d_slots, b->d_tl[LIST_HY], b->d_tl[LIST_HG], b->d_cnt, 0, b->st);
 }
 
 void* mctdhb_batch_stream(mctdhb_batch b) { return b ? (void*)b->st : nullptr; }

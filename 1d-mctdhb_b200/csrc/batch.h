@@ -20,9 +20,8 @@ namespace mctdhb {
 
 constexpr int kBatchVecRows = 1024;  // rows of one vector tile (256 threads x 4)
 constexpr int kBatchVecThreads = 256;
-constexpr int kBatchHcRows = 256;    // rows of one H.C tile (one 256-thread block)
-constexpr int kBatchDensThreads = 128;
-constexpr int kBatchMaxSlices = 1024;  // density slices per slot
+constexpr int kBatchHcRows = 256;    // rows of one H.C gather-back tile (one 256-thread block)
+constexpr int kBatchMaxSlices = 1024;  // Gram slices per slot and annihilation order
 constexpr int kBatchMaxLz = 16;        // Lanczos vectors per step
 constexpr int kBatchMinOrb = 2, kBatchMaxOrb = 8;
 constexpr int kBatchMaxGrid = 4096;
@@ -54,18 +53,20 @@ struct BatchSlot {
     int N, M, G, imag, rk, check_every, lz, pad0;
     uint32_t nc, max_steps;
     int vtiles;   // ceil(nc / kBatchVecRows)
-    int dslices;  // density slices; each covers dchunks x 128 rows
-    int dchunks;
+    int ytiles;   // tiles of the (N-2)-boson space of the pair-space H.C
+    int gs[3];    // Gram slices of the (N-R)-boson space, index R = 1, 2
+    int gk[3];    // row tiles per Gram slice, index R
+    uint32_t D1;  // D(N-1, M); D(N-2, M) is sp.dim2
     int pad1;
     double dt, etol, reg_fac;
     double2 pdt;  // SIL time step: dt (real time) or -i dt (imaginary time)
     OrbView ov;   // grid, equation coefficients, Simpson weights, trap
-    SpaceView sp;
+    SpaceView sp; // with the pair matrix sp.pair_w and its scratch sp.pair_y
     const double* g;     // contact interaction (device scalar)
-    const int* desc;     // density element descriptors for M
-    double2 *orb, *stage, *H, *Q, *hob, *hint, *tab, *rho1, *rho2, *rinv, *work;
+    double2 *orb, *stage, *H, *Q, *hob, *hint, *rho1, *rho2, *rinv, *work;
     double2 *V;          // lz x nc Krylov vectors; V[0] holds the coefficients
-    double2 *out, *part, *dpart;
+    double2 *out, *part;
+    double2* gpart;      // Gram partials: gs[2] slices of rho2's, then gs[1] of rho1's
     double2* scal;       // BS_TOTAL
     int* flags;          // BF_TOTAL
 };
@@ -77,15 +78,47 @@ struct BatchTile {
     uint32_t idx;
 };
 
-// batch_m*.cu: per-M H.C and density kernels over a tile list.  `off` and
-// `cnt` are device arrays indexed by M (the list of orbital count M starts
-// at tiles + off[M]).  dens_batch_launch with slots == nullptr only sets the
-// kernel's launch attributes (call it before any stream capture).
+// Tile lists of the per-M kernels.  The count block c (device) holds, after
+// c[0] (the vector-tile count), the offset and the count of every list for
+// every orbital count: the list `list` of orbital count M is
+// tiles_list[batch_off(c, list, M) ...] with batch_cnt(c, list, M) tiles.
+constexpr int kBatchNumM = kBatchMaxOrb + 1;
+constexpr int LIST_HG = 0;  // H.C gather-back: idx = first row (kBatchHcRows rows)
+constexpr int LIST_HY = 1;  // H.C pair contraction: idx = tile of the (N-2)-space
+constexpr int LIST_G2 = 2;  // rho2 Gram: idx = slice
+constexpr int LIST_G1 = 3;  // rho1 Gram: idx = slice
+constexpr int kBatchLists = 4;
+constexpr int kBatchCntInts = 1 + 2 * kBatchLists * kBatchNumM;
+__host__ __device__ inline int* batch_offs(int* c, int list) { return c + 1 + 2 * list * kBatchNumM; }
+__host__ __device__ inline int* batch_cnts(int* c, int list) {
+    return c + 1 + (2 * list + 1) * kBatchNumM;
+}
+__host__ __device__ inline int batch_off(const int* c, int list, int M) {
+    return c[1 + 2 * list * kBatchNumM + M];
+}
+__host__ __device__ inline int batch_cnt(const int* c, int list, int M) {
+    return c[1 + (2 * list + 1) * kBatchNumM + M];
+}
+
+// rows per tile of the pair contraction (pairhc_tmpl.cuh, PairHcShape)
+__host__ __device__ constexpr int batch_pair_rows(int M) {
+    return M * (M + 1) / 2 <= 21 ? 256 : 128;
+}
+
+// batch_m*.cu: per-M kernels over the tile lists.
+//   hcp_batch_launch   out = H V[iter] (- beta V[iter-1]) of every running
+//                      slot of orbital count M: pair contraction, gather-back
+//   gram_batch_launch  rho1 / rho2 of V[0] of the slots of orbital count M
+//                      (`list` / `nlist`: the slots, one finalize block each)
+//   batch_prepare      launch attributes (call before any stream capture)
 template <int M>
-int hc_batch_launch(const BatchSlot* slots, const BatchTile* tiles, const int* off,
-                    const int* cnt, int iter, cudaStream_t st);
+int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
+                     const int* cnt, int iter, cudaStream_t st);
 template <int M>
-int dens_batch_launch(const BatchSlot* slots, const BatchTile* tiles, const int* off,
-                      const int* cnt, cudaStream_t st);
+int gram_batch_launch(const BatchSlot* slots, const BatchTile* g2, const BatchTile* g1,
+                      const int* cnt, const int* list, const int* nlist, int nblocks,
+                      cudaStream_t st);
+template <int M>
+int batch_prepare();
 
 }  // namespace mctdhb

@@ -4,13 +4,14 @@
 //   bt_orbital_kernel   one block per slot: Runge-Kutta step of the orbital
 //                       equation with the slot's rho1^{-1} and rho2,
 //                       Gram-Schmidt in imaginary time, h_kl and g_ksql of the
-//                       new orbitals, the packed H.C table, Lanczos set-up
-//   Lanczos             hc_batch_kernel (per M) and the vector kernels below,
-//                       multiconfig_lanczos.c:12-90 operation for operation
+//                       new orbitals, the pair matrix of H.C, Lanczos set-up
+//   Lanczos             the pair-space H.C (per M, batch_tmpl.cuh) and the
+//                       vector kernels below, multiconfig_lanczos.c:12-90
+//                       operation for operation
 //   SIL                 tridiagonal eigenproblem, C = V U exp(-i D dt) U^T e1,
 //                       renormalisation in imaginary time
 //                       (coefficients_integration.c:59-160)
-//   densities           dens_batch_kernel (per M) + bt_dens_finalize_kernel
+//   densities           Gram-matrix rho1 / rho2 (per M, batch_tmpl.cuh)
 //   bt_tail_kernel      rho1 regularisation and inverse (synchronize.c:42-57),
 //                       energy (integrator_monitor.c:56-88), step count and
 //                       the imaginary-time stop rule (driver.c:47-67)
@@ -238,8 +239,11 @@ __global__ void __launch_bounds__(kBatchOrbThreads)
         bt_periodic(S);
     }
     bt_matrices(S);
+    __syncthreads();
+    // the pair matrix of H.C for the new h and g (pairhc_tmpl.cuh)
+    for (int e = threadIdx.x; e < M * (M + 1) / 2 * (M * (M + 1) / 2); e += blockDim.x)
+        S.sp.pair_w[e] = pair_w_entry(S.N, M, S.hob, S.hint, e);
     if (threadIdx.x == 0) {
-        hc_pack_table(M, S.hob, S.hint, S.tab);
         // Lanczos set-up of this step (multiconfig_lanczos.c:30-41)
         S.flags[BF_BREAK] = 0;
         S.flags[BF_ITERS] = S.lz;
@@ -488,25 +492,6 @@ __global__ void bt_small_kernel(const BatchSlot* __restrict__ slots, const int* 
             s.y += z[k * n + j] * aux[j].y;
         }
         S.scal[BS_Y + k] = s;
-    }
-}
-
-// rho1 / rho2: fixed-order sum of the slices, the reference's symmetric fill
-__global__ void __launch_bounds__(kBatchVecThreads)
-    bt_dens_finalize_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
-                            const int* __restrict__ nlist) {
-    BT_SLOT
-    const int M = S.M;
-    const int E = dens_nelem(M), EP = (E + 7) / 8 * 8;
-    for (int e = threadIdx.x; e < E; e += blockDim.x) {
-        double2 v = S.dpart[e];
-        for (int b = 1; b < S.dslices; b++) {
-            const double2 p = S.dpart[(size_t)b * EP + e];
-            v.x += p.x;
-            v.y += p.y;
-        }
-        const int* d = S.desc + 5 * e;
-        dens_fill(d[0], d[1], d[2], d[3], d[4], v, M, S.rho1, S.rho2);
     }
 }
 

@@ -35,9 +35,6 @@ __global__ void bt_norm_kernel(const BatchSlot* __restrict__ slots, const int* _
                                const int* __restrict__ nlist, int i);
 __global__ void bt_small_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
                                 const int* __restrict__ nlist);
-__global__ void bt_dens_finalize_kernel(const BatchSlot* __restrict__ slots,
-                                        const int* __restrict__ list,
-                                        const int* __restrict__ nlist);
 __global__ void bt_tail_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
                                const int* __restrict__ nlist, int prologue);
 

@@ -1,8 +1,9 @@
 // batch_m8.cu -- batched H.C and density kernels for 8 orbitals
 #include "batch_tmpl.cuh"
 namespace mctdhb {
-template int hc_batch_launch<8>(const BatchSlot*, const BatchTile*, const int*, const int*, int,
-                                cudaStream_t);
-template int dens_batch_launch<8>(const BatchSlot*, const BatchTile*, const int*, const int*,
-                                  cudaStream_t);
+template int hcp_batch_launch<8>(const BatchSlot*, const BatchTile*, const BatchTile*, const int*,
+                                 int, cudaStream_t);
+template int gram_batch_launch<8>(const BatchSlot*, const BatchTile*, const BatchTile*,
+                                  const int*, const int*, const int*, int, cudaStream_t);
+template int batch_prepare<8>();
 }  // namespace mctdhb

@@ -1,122 +1,203 @@
 // batch_tmpl.cuh -- per-M H.C and density kernels of the batched engine:
-// persistent blocks walk the tile list of one orbital count M, each tile a
-// run of rows of one slot, with the row bodies of the single-system kernels
-// (hc_row, dens_row).  One explicit instantiation per M (batch_m*.cu).
+// persistent blocks walk the tile lists of one orbital count M (batch.h),
+// each tile a run of rows of one slot, with the building blocks of the
+// single-system kernels (pairhc_tmpl.cuh, gram_tmpl.cuh).  One explicit
+// instantiation per M (batch_m*.cu).
+//
+// Every value of a slot is computed by one thread, or summed over the
+// slot's own slices in a fixed order, so a slot's result does not depend on
+// the other slots of the batch.
 #pragma once
+#include <algorithm>
+
 #include "batch.h"
-#include "dens_tmpl.cuh"
-#include "hc_tmpl.cuh"
+#include "gram_tmpl.cuh"
+#include "pairhc_tmpl.cuh"
 
 namespace mctdhb {
 
-// Lanczos H.C of step iteration `iter` for every slot of the list:
+// H.C of this step's Lanczos iteration runs for the slot
+__device__ __forceinline__ bool bt_hc_active(const BatchSlot& S) {
+    return S.flags[BF_STATE] == SLOT_RUNNING && !S.flags[BF_BREAK];
+}
+
+// Pair contraction Y = A W^T of V[iter] for every tile of list LIST_HY:
+// warp-specialised and double-buffered as hcp_y_kernel; the producer warps
+// stage each tile's W with its A, since consecutive tiles may belong to
+// different slots.
+template <int M>
+__global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
+    bhcp_y_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                  const int* __restrict__ cnt, int iter) {
+    using PS_ = PairHcShape<M>;
+    constexpr int P = PS_::P, PS = PS_::PS, ROWS = PS_::ROWS;
+    static_assert(ROWS == batch_pair_rows(M), "tile rows of the host lists");
+    extern __shared__ double2 smem[];
+    double2* Wb = smem;              // two buffers of P x P
+    double2* Ab = smem + 2 * P * P;  // two buffers of ROWS x PS
+    const int nt = batch_cnt(cnt, LIST_HY, M);
+    const BatchTile* list = tiles + batch_off(cnt, LIST_HY, M);
+    const int t = threadIdx.x;
+    const bool producer = t >= PS_::CONSUMERS;
+    const int pt = t - PS_::CONSUMERS;
+    auto fill = [&](int k, int buf) {
+        const BatchTile tl = list[k];
+        const BatchSlot& S = slots[tl.slot];
+        if (!bt_hc_active(S)) return;
+        for (int i = pt; i < P * P; i += PS_::PRODUCERS) Wb[buf * P * P + i] = S.sp.pair_w[i];
+        pair_gather<M>(S.sp, S.V + (size_t)iter * S.nc, tl.idx, Ab + (size_t)buf * ROWS * PS, pt,
+                       PS_::PRODUCERS);
+    };
+    if (producer && (int)blockIdx.x < nt) fill(blockIdx.x, 0);
+    __syncthreads();
+    int buf = 0;
+    for (int k = blockIdx.x; k < nt; k += gridDim.x, buf ^= 1) {
+        if (producer) {
+            if (k + (int)gridDim.x < nt) fill(k + gridDim.x, buf ^ 1);
+        } else {
+            const BatchTile tl = list[k];
+            const BatchSlot& S = slots[tl.slot];
+            if (bt_hc_active(S)) {
+                const int r = t % ROWS, part = t / ROWS;  // part is warp-uniform
+                pair_contract<M>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * P, r, part,
+                                 tl.idx * ROWS + r, S.sp.dim2, S.sp.pair_y);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Lanczos H.C of step iteration `iter`, gathered back from Y:
 //   out = H V[iter] - beta_{iter-1} V[iter-1]   (iter > 0)
 //   out = H V[0]                                (iter == 0)
 // Slots that stopped, or whose Lanczos recurrence broke down in this step,
 // are skipped (multiconfig_lanczos.c:70-71).
-template <int M, int SYNC>
-__global__ void __launch_bounds__(kBatchHcRows, 2)
-    hc_batch_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
-                    const int* __restrict__ off, const int* __restrict__ cnt, int iter) {
-    constexpr int TAB = hc_table_size(M);
-    __shared__ double2 tab[TAB];
-    const int nt = cnt[M];
-    const BatchTile* list = tiles + off[M];
-    int cur = -1;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const BatchTile tl = list[t];
+template <int M>
+__global__ void __launch_bounds__(kBatchHcRows)
+    bhcp_g_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                  const int* __restrict__ cnt, int iter) {
+    const int nt = batch_cnt(cnt, LIST_HG, M);
+    const BatchTile* list = tiles + batch_off(cnt, LIST_HG, M);
+    for (int k = blockIdx.x; k < nt; k += gridDim.x) {
+        const BatchTile tl = list[k];
         const BatchSlot& S = slots[tl.slot];
-        if (S.flags[BF_STATE] != SLOT_RUNNING || S.flags[BF_BREAK]) continue;
-        if (tl.slot != cur) {
-            __syncthreads();
-            for (int i = threadIdx.x; i < TAB; i += kBatchHcRows) tab[i] = S.tab[i];
-            __syncthreads();
-            cur = tl.slot;
-        }
+        if (!bt_hc_active(S)) continue;
         const uint32_t nc = S.nc;
         const uint32_t row = tl.idx + threadIdx.x;
-        const bool live = row < nc;
-        double2 acc = hc_row<M, SYNC>(S.sp, row, live, S.V + (size_t)iter * nc, tab);
-        if (iter > 0 && live) {
+        if (row >= nc) continue;
+        double2 acc = pair_gather_back<M>(S.sp, S.sp.pair_y, row);
+        if (iter > 0) {
             const double2 pv = S.V[(size_t)(iter - 1) * nc + row];
             const double b = S.scal[BS_OFFD + iter - 1].x;
             acc.x -= b * pv.x;
             acc.y -= b * pv.y;
         }
-        if (live) S.out[row] = acc;
+        S.out[row] = acc;
     }
 }
 
-// rho1/rho2 partial sums of V[0]: slice `idx` of a slot covers dchunks runs
-// of 128 rows; its block writes the slice's sums to dpart[idx * EP ...].
-template <int M, int SYNC>
-__global__ void __launch_bounds__(kBatchDensThreads)
-    dens_batch_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
-                      const int* __restrict__ off, const int* __restrict__ cnt) {
-    constexpr int E = dens_nelem(M);
-    constexpr int EP = (E + 7) / 8 * 8;
-    constexpr int NW = kBatchDensThreads / 32;
-    extern __shared__ double2 sacc[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double2* wacc = sacc + warp * EP;
-    const int nt = cnt[M];
-    const BatchTile* list = tiles + off[M];
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const BatchTile tl = list[t];
+// Gram partial of slice `idx` of a slot: its gk[R] consecutive row tiles of
+// the (N-R)-boson space, summed into gpart (gram_tmpl.cuh building blocks)
+template <int M, int R>
+__global__ void __launch_bounds__(kGramThreads, 2)
+    bgram_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                 const int* __restrict__ cnt) {
+    using GS = GramShape<M, R>;
+    constexpr int LIST = R == 2 ? LIST_G2 : LIST_G1;
+    extern __shared__ double2 As[];
+    const int nt = batch_cnt(cnt, LIST, M);
+    const BatchTile* list = tiles + batch_off(cnt, LIST, M);
+    const GramRole<M, R> role(threadIdx.x);
+    for (int k = blockIdx.x; k < nt; k += gridDim.x) {
+        const BatchTile tl = list[k];
         const BatchSlot& S = slots[tl.slot];
-        if (S.flags[BF_STATE] != SLOT_RUNNING) continue;
-        for (int i = lane; i < EP; i += 32) wacc[i] = make_double2(0.0, 0.0);
-        __syncwarp();
-        const uint32_t nc = S.nc;
-        const uint32_t r0 = tl.idx * (uint32_t)S.dchunks * kBatchDensThreads;
-        for (int c = 0; c < S.dchunks; c++) {
-            const uint32_t base = r0 + (uint32_t)c * kBatchDensThreads;
-            if (base >= nc) break;  // block-uniform
-            const uint32_t row = base + threadIdx.x;
-            dens_row<M, SYNC>(S.sp, row, row < nc, S.V, wacc, lane);
+        if (S.flags[BF_STATE] != SLOT_RUNNING) continue;  // block-uniform
+        const uint32_t Dp = R == 2 ? S.sp.dim2 : S.D1;
+        const uint32_t ntr = (Dp + GS::ROWS - 1) / GS::ROWS;
+        const uint32_t t0 = tl.idx * (uint32_t)S.gk[R];
+        const uint32_t t1 = min(t0 + (uint32_t)S.gk[R], ntr);
+        double2 acc[GS::RT][GS::RT];
+#pragma unroll
+        for (int a = 0; a < GS::RT; a++)
+#pragma unroll
+            for (int b = 0; b < GS::RT; b++) acc[a][b] = make_double2(0.0, 0.0);
+        for (uint32_t tr = t0; tr < t1; tr++) {
+            gram_gather<M, R>(S.sp, Dp, S.V, tr, As, threadIdx.x);
+            __syncthreads();
+            gram_accumulate<M, R>(As, role, acc);
+            __syncthreads();
         }
-        __syncthreads();
-        for (int e = threadIdx.x; e < EP; e += kBatchDensThreads) {
-            double2 s = sacc[e];
-            for (int w = 1; w < NW; w++) {
-                s.x += sacc[w * EP + e].x;
-                s.y += sacc[w * EP + e].y;
-            }
-            S.dpart[(size_t)tl.idx * EP + e] = s;
-        }
-        __syncthreads();
+        double2* out = S.gpart + (R == 2 ? (size_t)tl.idx * gram_entries(M, 2)
+                                         : (size_t)S.gs[2] * gram_entries(M, 2) +
+                                               (size_t)tl.idx * gram_entries(M, 1));
+        gram_store<M, R>(role, acc, As, out);
     }
 }
 
-// barrier interval of the unrolled row bodies: the larger move lists need
-// the warps of a block to walk the code together (hc_tmpl.cuh)
+// rho1 / rho2 of every running slot of orbital count M: fixed-order sum of
+// the slot's slices and the reference's symmetric fill (gram_fill)
 template <int M>
-constexpr int batch_sync() {
-    return M >= 6 ? 64 : 0;
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bgram_finalize_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                          const int* __restrict__ nlist) {
+    if ((int)blockIdx.x >= *nlist) return;
+    const BatchSlot& S = slots[list[blockIdx.x]];
+    if (S.M != M || S.flags[BF_STATE] != SLOT_RUNNING) return;
+    constexpr int ENT2 = gram_entries(M, 2), ENT1 = gram_entries(M, 1);
+    for (int e = threadIdx.x; e < ENT2 + ENT1; e += blockDim.x) {
+        const bool two = e < ENT2;
+        const int ee = two ? e : e - ENT2;
+        const int ns = two ? S.gs[2] : S.gs[1], ent = two ? ENT2 : ENT1;
+        const double2* part = two ? S.gpart : S.gpart + (size_t)S.gs[2] * ENT2;
+        double2 v = make_double2(0.0, 0.0);
+        for (int q = 0; q < ns; q++) v = cadd(v, part[(size_t)q * ent + ee]);
+        gram_fill<M>(two ? 2 : 1, ee, v, S.rho1, S.rho2);
+    }
 }
 
 template <int M>
-int hc_batch_launch(const BatchSlot* slots, const BatchTile* tiles, const int* off,
-                    const int* cnt, int iter, cudaStream_t st) {
-    hc_batch_kernel<M, batch_sync<M>()><<<num_sms() * 2, kBatchHcRows, 0, st>>>(slots, tiles, off,
-                                                                              cnt, iter);
+constexpr size_t batch_y_smem() {
+    using PS_ = PairHcShape<M>;
+    return (2 * (size_t)PS_::P * PS_::P + 2 * (size_t)PS_::ROWS * PS_::PS) * sizeof(double2);
+}
+
+template <int M>
+int batch_prepare() {
+    static bool done = false;
+    if (done) return 0;
+    MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bhcp_y_kernel<M>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)batch_y_smem<M>()));
+    MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         gram_smem(M, 2)));
+    MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         gram_smem(M, 1)));
+    done = true;
+    return 0;
+}
+
+template <int M>
+int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
+                     const int* cnt, int iter, cudaStream_t st) {
+    bhcp_y_kernel<M><<<num_sms(), PairHcShape<M>::THREADS, batch_y_smem<M>(), st>>>(slots, hy,
+                                                                                 cnt, iter);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    bhcp_g_kernel<M><<<num_sms() * 8, kBatchHcRows, 0, st>>>(slots, hg, cnt, iter);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
 template <int M>
-int dens_batch_launch(const BatchSlot* slots, const BatchTile* tiles, const int* off,
-                      const int* cnt, cudaStream_t st) {
-    constexpr int EP = (dens_nelem(M) + 7) / 8 * 8;
-    const size_t smem = (size_t)(kBatchDensThreads / 32) * EP * sizeof(double2);
-    if (slots == nullptr) {  // launch attributes only (before graph capture)
-        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(dens_batch_kernel<M, batch_sync<M>()>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem));
-        return 0;
-    }
-    dens_batch_kernel<M, batch_sync<M>()><<<num_sms() * 3, kBatchDensThreads, smem, st>>>(
-        slots, tiles, off, cnt);
+int gram_batch_launch(const BatchSlot* slots, const BatchTile* g2, const BatchTile* g1,
+                      const int* cnt, const int* list, const int* nlist, int nblocks,
+                      cudaStream_t st) {
+    bgram_kernel<M, 2><<<num_sms() * 2, kGramThreads, gram_smem(M, 2), st>>>(slots, g2, cnt);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    bgram_kernel<M, 1><<<num_sms() * 2, kGramThreads, gram_smem(M, 1), st>>>(slots, g1, cnt);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    bgram_finalize_kernel<M><<<std::max(nblocks, 1), kBatchVecThreads, 0, st>>>(slots, list, nlist);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -6,4 +6,5 @@ template int dens_launch_tmpl<3>(const SpaceView&, const double2*, double2*, int
                                   cudaStream_t);
 template int gram_apply_tmpl<3>(const SpaceView&, uint32_t, uint32_t, const double2*, double2*,
                                   double2*, double2*, cudaStream_t);
+template int gram_prepare_tmpl<3>();
 }

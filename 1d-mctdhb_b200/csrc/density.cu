@@ -179,8 +179,8 @@ static uint32_t annihilated_dim(const SpaceView& sp, int R) {
 }
 
 static size_t gram_partial(const SpaceView& sp) {
-    return (size_t)gram_blocks(annihilated_dim(sp, 2)) * gram_entries(sp.M, 2) +
-           (size_t)gram_blocks(annihilated_dim(sp, 1)) * gram_entries(sp.M, 1);
+    return (size_t)gram_blocks(sp.M, 2, annihilated_dim(sp, 2)) * gram_entries(sp.M, 2) +
+           (size_t)gram_blocks(sp.M, 1, annihilated_dim(sp, 1)) * gram_entries(sp.M, 1);
 }
 
 size_t dens_partial_elems(const SpaceView& sp) {
@@ -246,7 +246,16 @@ int dens_prepare(const SpaceView& sp, const double2* C, double2* partial, cudaSt
     (void)C;
     (void)partial;
     (void)st;
-    return 0;  // the Gram kernels (M <= 8) and the generic kernel need no set-up
+    switch (sp.M) {  // launch attributes of the Gram kernels (M <= 8)
+        case 2: return gram_prepare_tmpl<2>();
+        case 3: return gram_prepare_tmpl<3>();
+        case 4: return gram_prepare_tmpl<4>();
+        case 5: return gram_prepare_tmpl<5>();
+        case 6: return gram_prepare_tmpl<6>();
+        case 7: return gram_prepare_tmpl<7>();
+        case 8: return gram_prepare_tmpl<8>();
+    }
+    return 0;
 }
 
 // Set-up of the per-row kernels (dens_tmpl.cuh): launch attributes and the

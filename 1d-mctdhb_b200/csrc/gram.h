@@ -19,13 +19,30 @@ __host__ __device__ constexpr int gram_entries(int M, int R) {
     return gram_ntiles(M, R) * gram_rt(gram_p(M, R)) * gram_rt(gram_p(M, R));
 }
 constexpr int kGramThreads = 256;
-constexpr int kGramRows = 64;        // rows of A per tile
 constexpr int kGramMaxBlocks = 296;  // 2 x 148: fixed, so the sums depend on (N, M) only
+constexpr int kGramSmemBudget = 96 * 1024;  // A tile bytes: two blocks per SM
 
-// blocks (= partial slices) for Dp rows: a function of the space size only
-inline int gram_blocks(uint32_t Dp) {
-    const uint32_t need = (Dp + kGramRows - 1) / kGramRows;
+// A tile layout: the RT-wide column chunks of a row sit RT + 1 words apart
+// and rows an odd number of 16-byte words apart, so the chunk reads of a
+// warp (different chunks of one row, or one column of consecutive rows)
+// fall in different shared-memory banks
+__host__ __device__ constexpr int gram_row_stride(int M, int R) {
+    return (gram_nt(M, R) * (gram_rt(gram_p(M, R)) + 1)) | 1;
+}
+// rows per tile: the largest of 256 / 128 / 64 whose tile fits the budget
+__host__ __device__ constexpr int gram_rows(int M, int R) {
+    return (256 * gram_row_stride(M, R) * 16 <= kGramSmemBudget) ? 256
+           : (128 * gram_row_stride(M, R) * 16 <= kGramSmemBudget) ? 128 : 64;
+}
+__host__ __device__ constexpr int gram_smem(int M, int R) {
+    return gram_rows(M, R) * gram_row_stride(M, R) * 16;
+}
+
+// blocks (= partial slices) for Dp rows: a function of (N, M) only
+inline int gram_blocks_rows(uint32_t Dp, int rows) {
+    const uint32_t need = (Dp + rows - 1) / rows;
     return (int)(need < (uint32_t)kGramMaxBlocks ? need : (uint32_t)kGramMaxBlocks);
 }
+inline int gram_blocks(int M, int R, uint32_t Dp) { return gram_blocks_rows(Dp, gram_rows(M, R)); }
 
 }  // namespace mctdhb

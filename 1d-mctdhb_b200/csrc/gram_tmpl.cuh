@@ -19,8 +19,9 @@
 //     U_d[x] = sum_{y=x}^{M-2} (T_y(L_y + d) - T_y(L_y)),
 // two subtractions per pair once U1, U2 are formed per row.
 //
-// Work split.  A block takes tiles of ROWS rows: every thread unranks its
-// row and gathers its share of the row's A values into shared memory; then
+// Work split.  A block takes tiles of ROWS rows (as many as a 96 KB tile
+// holds): every thread unranks its row and gathers its share of the row's
+// A values into shared memory (gram.h gives the bank-spread layout); then
 // thread groups accumulate the upper triangle of the P x P Gram matrix in
 // RT x RT complex register tiles, each group over an interleaved subset of
 // the tile's rows.  At the end the groups are added in a fixed order and the
@@ -90,122 +91,202 @@ __device__ __forceinline__ void gram_unrank(const uint32_t* __restrict__ T, int 
     }
 }
 
-// One block's share of the Gram matrix of the R-annihilated states of C.
-// Dp = D(N-R, M) rows; jbase = D(N, M) - Dp.  partial: gridDim.x x
-// gram_entries(M, R) complex.
+// ---------------------------------------------------------------------------
+// building blocks (shared with the batched engine, batch_tmpl.cuh)
+// ---------------------------------------------------------------------------
 template <int M, int R>
-__global__ void __launch_bounds__(kGramThreads, 2)
-    gram_kernel(SpaceView sp, uint32_t Dp, const double2* __restrict__ C,
-                double2* __restrict__ partial) {
-    constexpr int P = gram_p(M, R);
-    constexpr int RT = gram_rt(P);
-    constexpr int NT = P / RT;
-    constexpr int NTILES = NT * (NT + 1) / 2;
-    constexpr int ENT = NTILES * RT * RT;
-    constexpr int ROWS = kGramRows;
-    constexpr int PARTS = kGramThreads / ROWS;  // threads per row in the gather phase
-    constexpr int GROUPS = (kGramThreads / NTILES) < ROWS ? (kGramThreads / NTILES) : ROWS;
-    static_assert(ENT <= ROWS * P, "the group reduction reuses the A tile");
+struct GramShape {
+    static constexpr int P = gram_p(M, R);
+    static constexpr int RT = gram_rt(P);
+    static constexpr int NT = P / RT;
+    static constexpr int NTILES = NT * (NT + 1) / 2;
+    static constexpr int ENT = NTILES * RT * RT;
+    static constexpr int ROWS = gram_rows(M, R);
+    static constexpr int PS = gram_row_stride(M, R);
+    static constexpr int PARTS = kGramThreads / ROWS;  // threads per row in the gather
+    static constexpr int GROUPS = (kGramThreads / NTILES) < ROWS ? (kGramThreads / NTILES) : ROWS;
+    static_assert(ENT <= ROWS * PS, "the group reduction reuses the A tile");
+    // word of column p in a row of the A tile
+    __host__ __device__ static constexpr int col(int p) { return (p / RT) * (RT + 1) + p % RT; }
+};
 
-    __shared__ double2 As[ROWS * P];  // As[r * P + p]
-    const int t = threadIdx.x;
-    const int N = sp.N, Np = N - R;
-    const uint32_t jbase = sp.dim - Dp;
-    const int grp = t / NTILES, tile = t % NTILES;
-    const bool accum = grp < GROUPS;
-    int ti = 0, tj = 0;
-    for (int a = 0, c = 0; a < NT; a++)
-        for (int b = a; b < NT; b++, c++)
-            if (c == tile) ti = a, tj = b;
-
-    double2 acc[RT][RT];
-#pragma unroll
-    for (int a = 0; a < RT; a++)
-#pragma unroll
-        for (int b = 0; b < RT; b++) acc[a][b] = make_double2(0.0, 0.0);
-
-    const uint32_t ntile_rows = (Dp + ROWS - 1) / ROWS;
-    for (uint32_t tr = blockIdx.x; tr < ntile_rows; tr += gridDim.x) {
-        // gather: thread (r, part) fills pairs p = part, part + PARTS, ... of row r
-        {
-            const int r = t % ROWS, part = t / ROWS;
-            const uint32_t row = tr * ROWS + r;
-            const bool live = row < Dp;
-            int n[M];
-            uint32_t U1[M], U2[M];
-            if (live) {
-                gram_unrank<M, R>(sp.T, N, Np, Dp, row, n, U1, U2);
-            } else {
-#pragma unroll
-                for (int x = 0; x < M; x++) n[x] = 0, U1[x] = 0u, U2[x] = 0u;
-            }
-            const uint32_t j0 = jbase + row;
-            static_for<P>([&](auto pi) {
-                constexpr int p = decltype(pi)::value;
-                if (p % PARTS == part) {
-                    double2 v = make_double2(0.0, 0.0);
-                    if (live) {
-                        if constexpr (R == 1) {
-                            const uint32_t j = j0 - U1[p];
-                            v = cscale(__ldg(C + j), __ldg(sp.sq + n[p] + 1));
-                        } else {
-                            constexpr int q = kPairs<M>.q[p], l = kPairs<M>.l[p];
-                            const uint32_t j = j0 - (U1[q] - U1[l]) - U2[l];
-                            double f;
-                            if constexpr (q == l)
-                                f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[q] + 2);
-                            else
-                                f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
-                            v = cscale(__ldg(C + j), f);
-                        }
-                    }
-                    As[r * P + p] = v;
-                }
-            });
-        }
-        __syncthreads();
-        // Gram update: rows grp, grp + GROUPS, ... of the tile
-        if (accum) {
-            for (int r = grp; r < ROWS; r += GROUPS) {
-                double2 a[RT], b[RT];
-#pragma unroll
-                for (int x = 0; x < RT; x++) {
-                    a[x] = As[r * P + ti * RT + x];
-                    b[x] = As[r * P + tj * RT + x];
-                }
-#pragma unroll
-                for (int x = 0; x < RT; x++)
-#pragma unroll
-                    for (int y = 0; y < RT; y++) acc[x][y] = cfma_conj(a[x], b[y], acc[x][y]);
-            }
-        }
-        __syncthreads();
+// Per-thread role in the Gram accumulation: group and upper-triangle tile.
+template <int M, int R>
+struct GramRole {
+    int grp, tile, ti, tj;
+    bool accum;
+    __device__ explicit GramRole(int t) {
+        using S = GramShape<M, R>;
+        grp = t / S::NTILES;
+        tile = t % S::NTILES;
+        accum = grp < S::GROUPS;
+        ti = 0;
+        tj = 0;
+        for (int a = 0, c = 0; a < S::NT; a++)
+            for (int b = a; b < S::NT; b++, c++)
+                if (c == tile) ti = a, tj = b;
     }
-    // groups added in order 0, 1, ... into the (now free) A tile
-    double2* red = As;
-    for (int g = 0; g < GROUPS; g++) {
-        if (accum && grp == g) {
+};
+
+// Gather tile `tr` (ROWS rows of the (N-R)-boson space, Dp rows in all):
+// thread t fills the values p = part, part + PARTS, ... of row t % ROWS.
+template <int M, int R>
+__device__ __forceinline__ void gram_gather(const SpaceView& sp, uint32_t Dp,
+                                            const double2* __restrict__ C, uint32_t tr,
+                                            double2* As, int t) {
+    using S = GramShape<M, R>;
+    constexpr int P = S::P, PS = S::PS, ROWS = S::ROWS, PARTS = S::PARTS;
+    const int N = sp.N;
+    const int r = t % ROWS, part = t / ROWS;  // part is warp-uniform (ROWS >= 64)
+    const uint32_t row = tr * ROWS + r;
+    const bool live = row < Dp;
+    int n[M];
+    uint32_t U1[M], U2[M];
+    if (live) {
+        gram_unrank<M, R>(sp.T, N, N - R, Dp, row, n, U1, U2);
+    } else {
+#pragma unroll
+        for (int x = 0; x < M; x++) n[x] = 0, U1[x] = 0u, U2[x] = 0u;
+    }
+    const uint32_t j0 = sp.dim - Dp + row;
+    static_for<P>([&](auto pi) {
+        constexpr int p = decltype(pi)::value;
+        if (p % PARTS == part) {
+            double2 v = make_double2(0.0, 0.0);
+            if (live) {
+                if constexpr (R == 1) {
+                    const uint32_t j = j0 - U1[p];
+                    v = cscale(__ldg(C + j), __ldg(sp.sq + n[p] + 1));
+                } else {
+                    constexpr int q = kPairs<M>.q[p], l = kPairs<M>.l[p];
+                    const uint32_t j = j0 - (U1[q] - U1[l]) - U2[l];
+                    double f;
+                    if constexpr (q == l)
+                        f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[q] + 2);
+                    else
+                        f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
+                    v = cscale(__ldg(C + j), f);
+                }
+            }
+            As[r * PS + S::col(p)] = v;
+        }
+    });
+}
+
+// acc += conj(A[:, ti-chunk])^T A[:, tj-chunk] over rows grp, grp + GROUPS, ...
+template <int M, int R>
+__device__ __forceinline__ void gram_accumulate(const double2* As, const GramRole<M, R>& role,
+                                                double2 (&acc)[gram_rt(gram_p(M, R))]
+                                                              [gram_rt(gram_p(M, R))]) {
+    using S = GramShape<M, R>;
+    constexpr int RT = S::RT, PS = S::PS;
+    if (!role.accum) return;
+    for (int r = role.grp; r < S::ROWS; r += S::GROUPS) {
+        double2 a[RT], b[RT];
+#pragma unroll
+        for (int x = 0; x < RT; x++) {
+            a[x] = As[r * PS + role.ti * (RT + 1) + x];
+            b[x] = As[r * PS + role.tj * (RT + 1) + x];
+        }
+#pragma unroll
+        for (int x = 0; x < RT; x++)
+#pragma unroll
+            for (int y = 0; y < RT; y++) acc[x][y] = cfma_conj(a[x], b[y], acc[x][y]);
+    }
+}
+
+// groups added in order 0, 1, ... in shared memory `red` (ENT entries), then
+// stored to out[0..ENT); every thread of the block calls it
+template <int M, int R>
+__device__ __forceinline__ void gram_store(const GramRole<M, R>& role,
+                                           const double2 (&acc)[gram_rt(gram_p(M, R))]
+                                                               [gram_rt(gram_p(M, R))],
+                                           double2* red, double2* __restrict__ out) {
+    using S = GramShape<M, R>;
+    constexpr int RT = S::RT;
+    for (int g = 0; g < S::GROUPS; g++) {
+        if (role.accum && role.grp == g) {
 #pragma unroll
             for (int x = 0; x < RT; x++)
 #pragma unroll
                 for (int y = 0; y < RT; y++) {
-                    const int e = (tile * RT + x) * RT + y;
-                    if (g == 0)
-                        red[e] = acc[x][y];
-                    else
-                        red[e] = cadd(red[e], acc[x][y]);
+                    const int e = (role.tile * RT + x) * RT + y;
+                    red[e] = g == 0 ? acc[x][y] : cadd(red[e], acc[x][y]);
                 }
         }
         __syncthreads();
     }
-    for (int e = t; e < ENT; e += kGramThreads) partial[(size_t)blockIdx.x * ENT + e] = red[e];
+    for (int e = threadIdx.x; e < S::ENT; e += blockDim.x) out[e] = red[e];
+    __syncthreads();
 }
 
-// Sum of the block partials (block order) and the fill of rho2 (M^4,
-// element (k,s,q,l) at k + sM + qM^2 + lM^3) and rho1 (M x M row-major):
-// every ordering of a pair reads the same Gram entry, the lower triangle is
-// the conjugate of the upper, diagonal entries are real.  One thread per
-// entry of the packed upper-triangle tiles: first rho2's, then rho1's.
+// Summed Gram entry `ee` (packed upper-triangle tiles) written to rho1
+// (R = 1, M x M row-major) or rho2 (R = 2, M^4, (k,s,q,l) at k + sM + qM^2
+// + lM^3): every ordering of a pair reads the same entry, the lower
+// triangle is the conjugate of the upper, diagonal entries are real.
+template <int M>
+__device__ inline void gram_fill(int R, int ee, double2 v, double2* __restrict__ rho1,
+                                 double2* __restrict__ rho2) {
+    const int P = R == 2 ? gram_p(M, 2) : gram_p(M, 1);
+    const int RT = gram_rt(P), NT = P / RT;
+    const int tile = ee / (RT * RT), x = (ee / RT) % RT, y = ee % RT;
+    int ti = 0, tj = 0;
+    for (int a = 0, c = 0; a < NT; a++)
+        for (int b = a; b < NT; b++, c++)
+            if (c == tile) ti = a, tj = b;
+    const int pa = ti * RT + x, pb = tj * RT + y;
+    if (pa > pb) return;  // lower part of a diagonal tile: written by (pb, pa)
+    if (pa == pb) v.y = 0.0;
+    const double2 vc = make_double2(v.x, -v.y);
+    if (R == 1) {
+        rho1[pa * M + pb] = v;
+        rho1[pb * M + pa] = vc;
+        return;
+    }
+    int k = 0, s = 0, q = 0, l = 0;
+    for (int a = 0, c = 0; a < M; a++)
+        for (int b = a; b < M; b++, c++) {
+            if (c == pa) k = a, s = b;
+            if (c == pb) q = a, l = b;
+        }
+    constexpr int M2 = M * M, M3 = M2 * M;
+    const int ks[2][2] = {{k, s}, {s, k}}, ql[2][2] = {{q, l}, {l, q}};
+    for (int u = 0; u < (k == s ? 1 : 2); u++)
+        for (int w = 0; w < (q == l ? 1 : 2); w++) {
+            rho2[ks[u][0] + ks[u][1] * M + ql[w][0] * M2 + ql[w][1] * M3] = v;
+            rho2[ql[w][0] + ql[w][1] * M + ks[u][0] * M2 + ks[u][1] * M3] = vc;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// single-system kernels
+// ---------------------------------------------------------------------------
+// One block's share of the Gram matrix of the R-annihilated states of C:
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ...; partial: gridDim.x x ENT.
+template <int M, int R>
+__global__ void __launch_bounds__(kGramThreads, 2)
+    gram_kernel(SpaceView sp, uint32_t Dp, const double2* __restrict__ C,
+                double2* __restrict__ partial) {
+    using S = GramShape<M, R>;
+    extern __shared__ double2 As[];
+    const GramRole<M, R> role(threadIdx.x);
+    double2 acc[S::RT][S::RT];
+#pragma unroll
+    for (int a = 0; a < S::RT; a++)
+#pragma unroll
+        for (int b = 0; b < S::RT; b++) acc[a][b] = make_double2(0.0, 0.0);
+    const uint32_t ntile_rows = (Dp + S::ROWS - 1) / S::ROWS;
+    for (uint32_t tr = blockIdx.x; tr < ntile_rows; tr += gridDim.x) {
+        gram_gather<M, R>(sp, Dp, C, tr, As, threadIdx.x);
+        __syncthreads();
+        gram_accumulate<M, R>(As, role, acc);
+        __syncthreads();
+    }
+    gram_store<M, R>(role, acc, As, partial + (size_t)blockIdx.x * S::ENT);
+}
+
+// Sum of the block partials (block order) and the fill of rho1 / rho2; one
+// thread per packed entry, rho2's first.
 template <int M>
 __global__ void gram_finalize_kernel(int blocks2, int blocks1, const double2* __restrict__ part2,
                                      const double2* __restrict__ part1, double2* __restrict__ rho1,
@@ -215,64 +296,42 @@ __global__ void gram_finalize_kernel(int blocks2, int blocks1, const double2* __
     if (e >= ENT2 + ENT1) return;
     const bool two = e < ENT2;
     const int ee = two ? e : e - ENT2;
-    const int P = two ? gram_p(M, 2) : gram_p(M, 1);
-    const int RT = gram_rt(P), NT = P / RT;
-    const int nb = two ? blocks2 : blocks1;
-    const int ent = two ? ENT2 : ENT1;
+    const int nb = two ? blocks2 : blocks1, ent = two ? ENT2 : ENT1;
     const double2* part = two ? part2 : part1;
-    // packed index -> (tile, x, y) -> (p, p')
-    const int tile = ee / (RT * RT), x = (ee / RT) % RT, y = ee % RT;
-    int ti = 0, tj = 0, c = 0;
-    for (int a = 0; a < NT; a++)
-        for (int b = a; b < NT; b++) {
-            if (c == tile) ti = a, tj = b;
-            c++;
-        }
-    const int pa = ti * RT + x, pb = tj * RT + y;
-    if (pa > pb) return;  // lower part of a diagonal tile: the conjugate is written by (pb, pa)
     double2 v = make_double2(0.0, 0.0);
     for (int b = 0; b < nb; b++) v = cadd(v, part[(size_t)b * ent + ee]);
-    if (pa == pb) v.y = 0.0;
-    const double2 vc = make_double2(v.x, -v.y);
-    if (!two) {
-        rho1[pa * M + pb] = v;
-        rho1[pb * M + pa] = vc;
-        return;
-    }
-    auto pair = [](int p, int& q, int& l) {
-        int c2 = 0;
-        for (int a = 0; a < M; a++)
-            for (int b = a; b < M; b++) {
-                if (c2 == p) q = a, l = b;
-                c2++;
-            }
-    };
-    int k = 0, s = 0, q = 0, l = 0;
-    pair(pa, k, s);
-    pair(pb, q, l);
-    constexpr int M2 = M * M, M3 = M2 * M;
-    auto put = [&](int a, int b2, int cc, int d, double2 w) { rho2[a + b2 * M + cc * M2 + d * M3] = w; };
-    const int ks[2][2] = {{k, s}, {s, k}}, ql[2][2] = {{q, l}, {l, q}};
-    for (int u = 0; u < (k == s ? 1 : 2); u++)
-        for (int w = 0; w < (q == l ? 1 : 2); w++) {
-            put(ks[u][0], ks[u][1], ql[w][0], ql[w][1], v);
-            put(ql[w][0], ql[w][1], ks[u][0], ks[u][1], vc);
-        }
+    gram_fill<M>(two ? 2 : 1, ee, v, rho1, rho2);
 }
 
 template <int M, int R>
 int gram_launch(const SpaceView& sp, uint32_t Dp, const double2* C, double2* partial, int blocks,
                 cudaStream_t st) {
     if (blocks <= 0) return 0;
-    gram_kernel<M, R><<<blocks, kGramThreads, 0, st>>>(sp, Dp, C, partial);
+    gram_kernel<M, R><<<blocks, kGramThreads, gram_smem(M, R), st>>>(sp, Dp, C, partial);
     MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// launch attributes (dynamic shared memory beyond 48 KB), before any capture
+template <int M>
+int gram_prepare_tmpl() {
+    static bool done = false;
+    if (!done) {
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(gram_kernel<M, 2>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             gram_smem(M, 2)));
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(gram_kernel<M, 1>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             gram_smem(M, 1)));
+        done = true;
+    }
     return 0;
 }
 
 template <int M>
 int gram_apply_tmpl(const SpaceView& sp, uint32_t D2, uint32_t D1, const double2* C,
                     double2* partial, double2* rho1, double2* rho2, cudaStream_t st) {
-    const int b2 = gram_blocks(D2), b1 = gram_blocks(D1);
+    const int b2 = gram_blocks(M, 2, D2), b1 = gram_blocks(M, 1, D1);
     double2* part2 = partial;
     double2* part1 = partial + (size_t)b2 * gram_entries(M, 2);
     if (gram_launch<M, 2>(sp, D2, C, part2, b2, st)) return -1;

@@ -59,6 +59,8 @@ int dens_launch_tmpl(const SpaceView& sp, const double2* C, double2* partial, in
 template <int M>
 int gram_apply_tmpl(const SpaceView& sp, uint32_t D2, uint32_t D1, const double2* C,
                     double2* partial, double2* rho1, double2* rho2, cudaStream_t st);
+template <int M>
+int gram_prepare_tmpl();
 
 // H.C through the two-boson-annihilated space (pairhc_tmpl.cuh), M <= 8,
 // N >= 2: launch attributes (before any capture) and the two launches
@@ -101,7 +103,7 @@ int dens_descriptors(int M, int* host_desc);  // returns count; desc = 5 ints/el
 int dens_apply_rows(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
                     double2* rho2, const int* d_desc, cudaStream_t st);
 int dens_prepare_rows(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st);
-// set-up of dens_apply before any capture (nothing for the current kernels)
+// set-up of dens_apply before any capture (launch attributes)
 int dens_prepare(const SpaceView& sp, const double2* C, double2* partial, cudaStream_t st);
 // kernels of density.cu also launched by noalloc.cu on its own scratch
 __global__ void dens_generic_kernel(SpaceView sp, const double2* __restrict__ C,

@@ -130,6 +130,66 @@ __device__ inline void hc_pack_table(int M, const double2* __restrict__ hob,
                 }
 }
 
+// Entry e = P * npairs + Q of the pair matrix W of H = sum W[P][Q] a+_P a_Q
+// (pairhc_tmpl.cuh), P = {k <= s} created, Q = {q <= l} annihilated, with the g
+// elements and factors of the reference's rules (the move coefficients of
+// moves.cuh) and the one-body part spread over the spectator orbital x
+// with weight 1/(N-1):
+//   P = Q = {k,k}:    1/2 g_kkkk + h_kk/(N-1)
+//   P = Q = {k,s}:    2 g_ksks + (h_kk + h_ss)/(N-1)
+//   P = {a,x}, Q = {b,x}, a != b (one boson b -> a, spectator x):
+//                     c + h_ab/(N-1),  c = g_aaab (x = a), g_abbb (x = b),
+//                                          2 g_axxb otherwise
+//   P, Q disjoint:    f g_ksql, f = 1/2 (k=s, q=l), 1 (one of them), 2
+__device__ inline double2 pair_w_entry(int N, int M, const double2* __restrict__ hob,
+                                       const double2* __restrict__ hint, int e) {
+    const int P = M * (M + 1) / 2, M2 = M * M, M3 = M2 * M;
+    const double inv = 1.0 / (double)(N - 1);
+    auto g = [&](int a, int b, int c, int d) { return hint[a + b * M + c * M2 + d * M3]; };
+    auto h = [&](int a, int b) { return hob[a * M + b]; };
+    auto pair = [&](int p, int& a, int& b) {
+        for (int u = 0, c = 0; u < M; u++)
+            for (int v = u; v < M; v++, c++)
+                if (c == p) a = u, b = v;
+    };
+    {
+        const int pa = e / P, pb = e % P;
+        int k = 0, s = 0, q = 0, l = 0;
+        pair(pa, k, s);
+        pair(pb, q, l);
+        double2 w;
+        if (pa == pb) {
+            if (k == s) {
+                w = cadd(cscale(g(k, k, k, k), 0.5), cscale(h(k, k), inv));
+            } else {
+                w = cadd(cscale(g(k, s, k, s), 2.0), cscale(cadd(h(k, k), h(s, s)), inv));
+            }
+        } else {
+            int x = -1;
+            if (k == q || k == l)
+                x = k;
+            else if (s == q || s == l)
+                x = s;
+            if (x >= 0) {
+                const int a = (k == x) ? s : k, b = (q == x) ? l : q;
+                double2 c;
+                if (x == a)
+                    c = g(a, a, a, b);
+                else if (x == b)
+                    c = g(a, b, b, b);
+                else
+                    c = cscale(g(a, x, x, b), 2.0);
+                w = cadd(c, cscale(h(a, b), inv));
+            } else {
+                const double f = (k == s && q == l) ? 0.5 : ((k == s || q == l) ? 1.0 : 2.0);
+                w = cscale(g(k, s, q, l), f);
+            }
+        }
+        return w;
+    }
+}
+
+
 // Store the summed density element v (descriptor kind, k, s, q, l) into
 // rho1 (M x M row-major) / rho2 (M^4) with the reference's symmetric fill
 // (density_matrices.c:33-50, 86-442).

@@ -13,7 +13,8 @@
 //     Y_m(P) = sum_Q W[P][Q] A_m(Q)                 (hcp_y_kernel)
 //     (HC)_i = sum_{P in i} <i|a+_P|i-P> Y_{i-P}(P)  (hcp_g_kernel)
 // At N=30, M=8 this is 6.7 M x 36 gathers, a 36 x 36 complex matrix-vector
-// product per m (FP64 FMA, W staged in shared memory) and 10.3 M x 36
+// product per m (FP64 FMA, W staged in shared memory; gather and contraction
+// overlapped by warp specialisation) and 10.3 M x 36
 // coalesced reads of Y, instead of ~576 scattered coefficient gathers per
 // row.  Y (D(N-2, M) x P complex, pair-major so that both kernels access it
 // with consecutive lanes on consecutive m) is scratch owned by the Fock
@@ -32,151 +33,199 @@ namespace mctdhb {
 template <int M>
 struct PairHcShape {
     static constexpr int P = M * (M + 1) / 2;
-    static constexpr int PS = P | 1;                   // odd row stride: conflict-free columns
-    static constexpr int PG = P <= 21 ? P : P / 2;     // Y outputs per thread
-    static constexpr int NPG = P / PG;                 // threads per row (1 or 2)
-    static constexpr int THREADS = 256;
-    static constexpr int ROWS = THREADS / NPG;         // rows of A per tile
-    static constexpr size_t SMEM = ((size_t)ROWS * PS + (size_t)P * P) * sizeof(double2);
+    static constexpr int PS = P | 1;                 // odd row stride: conflict-free columns
+    static constexpr int PG = P <= 21 ? P : P / 2;   // Y outputs per consumer thread
+    static constexpr int NPG = P / PG;               // consumer threads per row (1 or 2)
+    static constexpr int CONSUMERS = 256;            // 8 warps: the contraction
+    static constexpr int PRODUCERS = 128;            // 4 warps: unrank and gather
+    static constexpr int THREADS = CONSUMERS + PRODUCERS;
+    static constexpr int ROWS = CONSUMERS / NPG;     // rows of A per tile
+    static constexpr size_t SMEM = (2 * (size_t)ROWS * PS + (size_t)P * P) * sizeof(double2);
 };
 
-// Y = A W^T for the rows m of the (N-2)-boson space; Y[p * D2 + m]
+// ---------------------------------------------------------------------------
+// building blocks (shared with the batched engine, batch_tmpl.cuh)
+// ---------------------------------------------------------------------------
+// Rows r = r0, r0 + rstep, ... < ROWS of tile `tr` of the (N-2)-boson space
+// into As[r * PS + p]: A_m(Q) = sqrt((m_q+1)(m_l+1+[q=l])) C[m + e_q + e_l].
 template <int M>
-__global__ void __launch_bounds__(PairHcShape<M>::THREADS, 2)
-    hcp_y_kernel(SpaceView sp, const double2* __restrict__ C, const double2* __restrict__ W,
-                 double2* __restrict__ Y, HcEpilogue ep) {
+__device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* __restrict__ C,
+                                            uint32_t tr, double2* As, int r0, int rstep) {
     using S = PairHcShape<M>;
-    constexpr int P = S::P, PS = S::PS, PG = S::PG, NPG = S::NPG, ROWS = S::ROWS;
-    extern __shared__ double2 smem[];
-    double2* As = smem;              // As[r * PS + p]
-    double2* Ws = smem + ROWS * PS;  // Ws[p * P + q]
-    if (ep.flag != nullptr && *ep.flag != 0) return;  // Lanczos breakdown: no-op
-    const int t = threadIdx.x;
-    for (int i = t; i < P * P; i += S::THREADS) Ws[i] = W[i];
+    constexpr int P = S::P, PS = S::PS, ROWS = S::ROWS;
     const int N = sp.N;
     const uint32_t D2 = sp.dim2;
     const uint32_t jbase = sp.dim - D2;
-    const int r = t % ROWS, part = t / ROWS;  // part is warp-uniform
-    const uint32_t ntiles = (D2 + ROWS - 1) / ROWS;
-    for (uint32_t tr = blockIdx.x; tr < ntiles; tr += gridDim.x) {
+    for (int r = r0; r < ROWS; r += rstep) {
         const uint32_t row = tr * ROWS + r;
         const bool live = row < D2;
-        // gather: A_m(Q) = sqrt((m_q+1)(m_l+1+[q=l])) C[m + e_q + e_l]
-        {
-            int n[M];
-            uint32_t U1[M], U2[M];
-            if (live) {
-                gram_unrank<M, 2>(sp.T, N, N - 2, D2, row, n, U1, U2);
-            } else {
-#pragma unroll
-                for (int x = 0; x < M; x++) n[x] = 0, U1[x] = 0u, U2[x] = 0u;
-            }
-            const uint32_t j0 = jbase + row;
-            static_for<P>([&](auto pi) {
-                constexpr int p = decltype(pi)::value;
-                if (p % NPG == part) {
-                    double2 v = make_double2(0.0, 0.0);
-                    if (live) {
-                        constexpr int q = kPairs<M>.q[p], l = kPairs<M>.l[p];
-                        const uint32_t j = j0 - (U1[q] - U1[l]) - U2[l];
-                        double f;
-                        if constexpr (q == l)
-                            f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[q] + 2);
-                        else
-                            f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
-                        v = cscale(__ldg(C + j), f);
-                    }
-                    As[r * PS + p] = v;
-                }
-            });
-        }
-        __syncthreads();
-        // Y_m(P) for this thread's PG outputs P = part * PG + g
-        double2 acc[PG];
-#pragma unroll
-        for (int g = 0; g < PG; g++) acc[g] = make_double2(0.0, 0.0);
-#pragma unroll 4
-        for (int q = 0; q < P; q++) {
-            const double2 a = As[r * PS + q];
-#pragma unroll
-            for (int g = 0; g < PG; g++) acc[g] = cfma(Ws[(part * PG + g) * P + q], a, acc[g]);
-        }
+        int n[M];
+        uint32_t U1[M], U2[M];
         if (live) {
+            gram_unrank<M, 2>(sp.T, N, N - 2, D2, row, n, U1, U2);
+        } else {
 #pragma unroll
-            for (int g = 0; g < PG; g++) Y[(size_t)(part * PG + g) * D2 + row] = acc[g];
+            for (int x = 0; x < M; x++) n[x] = 0, U1[x] = 0u, U2[x] = 0u;
+        }
+        const uint32_t j0 = jbase + row;
+        static_for<P>([&](auto pi) {
+            constexpr int p = decltype(pi)::value;
+            constexpr int q = kPairs<M>.q[p], l = kPairs<M>.l[p];
+            double2 v = make_double2(0.0, 0.0);
+            if (live) {
+                const uint32_t j = j0 - (U1[q] - U1[l]) - U2[l];
+                double f;
+                if constexpr (q == l)
+                    f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[q] + 2);
+                else
+                    f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
+                v = cscale(__ldg(C + j), f);
+            }
+            As[r * PS + p] = v;
+        });
+    }
+}
+
+// Y_m(P) = sum_Q W[P][Q] A_m(Q) for row r of the tile and the PG outputs
+// P = part * PG + g, stored to Y[P * D2 + row] when row < D2
+template <int M>
+__device__ __forceinline__ void pair_contract(const double2* As, const double2* Ws, int r,
+                                              int part, uint32_t row, uint32_t D2,
+                                              double2* __restrict__ Y) {
+    using S = PairHcShape<M>;
+    constexpr int P = S::P, PS = S::PS, PG = S::PG;
+    double2 acc[PG];
+#pragma unroll
+    for (int g = 0; g < PG; g++) acc[g] = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int q = 0; q < P; q++) {
+        const double2 a = As[r * PS + q];
+#pragma unroll
+        for (int g = 0; g < PG; g++) acc[g] = cfma(Ws[(part * PG + g) * P + q], a, acc[g]);
+    }
+    if (row < D2) {
+#pragma unroll
+        for (int g = 0; g < PG; g++) Y[(size_t)(part * PG + g) * D2 + row] = acc[g];
+    }
+}
+
+// (HC)_row = sum over pairs P = {k <= s} present in the row of
+// sqrt(n_k (n_s - [k=s])) Y_{row - e_k - e_s}(P)
+template <int M>
+__device__ __forceinline__ double2 pair_gather_back(const SpaceView& sp,
+                                                    const double2* __restrict__ Y,
+                                                    uint32_t row) {
+    constexpr int P = M * (M + 1) / 2;
+    const int N = sp.N;
+    const uint32_t D2 = sp.dim2;
+    // occupations and the suffix sums of the rank offsets of removing one /
+    // two bosons: V_d[x] = sum_{y >= x} T_y(L_y) - T_y(L_y - d)
+    int n[M];
+    uint32_t V1[M], V2[M];
+    {
+        uint32_t S = sp.dim - 1u - row;
+        int Lnext = N;
+        int L[M - 1];
+#pragma unroll
+        for (int x = M - 2; x >= 0; x--) {
+            const uint32_t* Tx = sp.T + x * (N + 1);
+            int lo = 0, hi = Lnext;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(Tx + mid) <= S)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            S -= __ldg(Tx + lo);
+            n[x + 1] = Lnext - lo;
+            L[x] = lo;
+            Lnext = lo;
+        }
+        n[0] = Lnext;
+        V1[M - 1] = 0u;
+        V2[M - 1] = 0u;
+        // an L_y below d only occurs for y below the orbitals of a pair that
+        // cannot be removed; those sums are never used
+#pragma unroll
+        for (int x = M - 2; x >= 0; x--) {
+            const uint32_t* Tx = sp.T + x * (N + 1);
+            const uint32_t t0 = __ldg(Tx + L[x]);
+            V1[x] = V1[x + 1] + (t0 - __ldg(Tx + (L[x] >= 1 ? L[x] - 1 : 0)));
+            V2[x] = V2[x + 1] + (t0 - __ldg(Tx + (L[x] >= 2 ? L[x] - 2 : 0)));
+        }
+    }
+    const uint32_t base = D2 - sp.dim + row;
+    double2 acc = make_double2(0.0, 0.0);
+    // every pair is loaded (row 0 of its plane where the pair is absent, with
+    // weight f = 0), so the loads do not wait on branches
+    static_for<P>([&](auto pi) {
+        constexpr int p = decltype(pi)::value;
+        constexpr int k = kPairs<M>.q[p], s = kPairs<M>.l[p];
+        bool valid;
+        double f;
+        if constexpr (k == s) {
+            valid = n[k] >= 2;
+            f = __ldg(sp.sq + n[k]) * __ldg(sp.sq + (n[k] >= 1 ? n[k] - 1 : 0));
+        } else {
+            valid = n[k] >= 1 && n[s] >= 1;
+            f = __ldg(sp.sq + n[k]) * __ldg(sp.sq + n[s]);
+        }
+        const uint32_t m = valid ? base + (V1[k] - V1[s]) + V2[s] : 0u;
+        const double2 y = __ldg(Y + (size_t)p * D2 + m);
+        acc.x = fma(f, y.x, acc.x);
+        acc.y = fma(f, y.y, acc.y);
+    });
+    return acc;
+}
+
+// ---------------------------------------------------------------------------
+// single-system kernels
+// ---------------------------------------------------------------------------
+// Y = A W^T for the rows m of the (N-2)-boson space; Y[p * D2 + m].
+// Warp-specialised and double-buffered: while the consumer warps contract
+// tile k from one A buffer, the producer warps unrank and gather tile k + 1
+// into the other; one block barrier per tile hands the buffers over.
+template <int M>
+__global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
+    hcp_y_kernel(SpaceView sp, const double2* __restrict__ C, const double2* __restrict__ W,
+                 double2* __restrict__ Y, HcEpilogue ep) {
+    using S = PairHcShape<M>;
+    constexpr int P = S::P, PS = S::PS, ROWS = S::ROWS;
+    extern __shared__ double2 smem[];
+    double2* Ws = smem;          // Ws[p * P + q]
+    double2* Ab = smem + P * P;  // two buffers of ROWS x PS
+    if (ep.flag != nullptr && *ep.flag != 0) return;  // Lanczos breakdown: no-op
+    const int t = threadIdx.x;
+    for (int i = t; i < P * P; i += S::THREADS) Ws[i] = W[i];
+    const uint32_t ntiles = (sp.dim2 + ROWS - 1) / ROWS;
+    const bool producer = t >= S::CONSUMERS;
+    const int pt = t - S::CONSUMERS;
+    if (producer && blockIdx.x < ntiles) pair_gather<M>(sp, C, blockIdx.x, Ab, pt, S::PRODUCERS);
+    __syncthreads();
+    int buf = 0;
+    for (uint32_t tr = blockIdx.x; tr < ntiles; tr += gridDim.x, buf ^= 1) {
+        if (producer) {
+            const uint32_t nx = tr + gridDim.x;
+            if (nx < ntiles)
+                pair_gather<M>(sp, C, nx, Ab + (size_t)(buf ^ 1) * ROWS * PS, pt, S::PRODUCERS);
+        } else {
+            const int r = t % ROWS, part = t / ROWS;  // part is warp-uniform
+            pair_contract<M>(Ab + (size_t)buf * ROWS * PS, Ws, r, part, tr * ROWS + r, sp.dim2, Y);
         }
         __syncthreads();
     }
 }
 
-// (HC)_i = sum over pairs P = {k <= s} present in row i of
-// sqrt(n_k (n_s - [k=s])) Y_{i - e_k - e_s}(P), then the Lanczos epilogue
+// (HC)_i gathered back from Y, then the Lanczos epilogue
 template <int M>
 __global__ void __launch_bounds__(256)
     hcp_g_kernel(SpaceView sp, const double2* __restrict__ Y, double2* __restrict__ HC,
                  HcEpilogue ep) {
-    constexpr int P = M * (M + 1) / 2;
     if (ep.flag != nullptr && *ep.flag != 0) return;
-    const int N = sp.N;
-    const uint32_t D2 = sp.dim2;
     for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < sp.dim;
          row += gridDim.x * blockDim.x) {
-        // occupations and the suffix sums of the rank offsets of removing
-        // one / two bosons: V_d[x] = sum_{y >= x} T_y(L_y) - T_y(L_y - d)
-        int n[M];
-        uint32_t V1[M], V2[M];
-        {
-            uint32_t S = sp.dim - 1u - row;
-            int Lnext = N;
-            int L[M - 1];
-#pragma unroll
-            for (int x = M - 2; x >= 0; x--) {
-                const uint32_t* Tx = sp.T + x * (N + 1);
-                int lo = 0, hi = Lnext;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (__ldg(Tx + mid) <= S)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
-                }
-                S -= __ldg(Tx + lo);
-                n[x + 1] = Lnext - lo;
-                L[x] = lo;
-                Lnext = lo;
-            }
-            n[0] = Lnext;
-            V1[M - 1] = 0u;
-            V2[M - 1] = 0u;
-            // an L_y below d only occurs for y below the orbitals of a pair
-            // that cannot be removed; those sums are never used
-#pragma unroll
-            for (int x = M - 2; x >= 0; x--) {
-                const uint32_t* Tx = sp.T + x * (N + 1);
-                const uint32_t t0 = __ldg(Tx + L[x]);
-                V1[x] = V1[x + 1] + (t0 - __ldg(Tx + (L[x] >= 1 ? L[x] - 1 : 0)));
-                V2[x] = V2[x + 1] + (t0 - __ldg(Tx + (L[x] >= 2 ? L[x] - 2 : 0)));
-            }
-        }
-        const uint32_t base = D2 - sp.dim + row;
-        double2 acc = make_double2(0.0, 0.0);
-        static_for<P>([&](auto pi) {
-            constexpr int p = decltype(pi)::value;
-            constexpr int k = kPairs<M>.q[p], s = kPairs<M>.l[p];
-            bool valid;
-            double f;
-            if constexpr (k == s) {
-                valid = n[k] >= 2;
-                f = valid ? __ldg(sp.sq + n[k]) * __ldg(sp.sq + n[k] - 1) : 0.0;
-            } else {
-                valid = n[k] >= 1 && n[s] >= 1;
-                f = __ldg(sp.sq + n[k]) * __ldg(sp.sq + n[s]);
-            }
-            if (valid) {
-                const uint32_t m = base + (V1[k] - V1[s]) + V2[s];
-                acc = cfma(make_double2(f, 0.0), __ldg(Y + (size_t)p * D2 + m), acc);
-            }
-        });
+        double2 acc = pair_gather_back<M>(sp, Y, row);
         if (ep.prev != nullptr) {
             const double2 pv = __ldg(ep.prev + row);
             const double b = *ep.beta;
@@ -204,7 +253,7 @@ int hcp_apply_tmpl(const SpaceView& sp, const double2* C, double2* HC, const HcE
                    cudaStream_t st) {
     using S = PairHcShape<M>;
     const uint32_t ntiles = (sp.dim2 + S::ROWS - 1) / S::ROWS;
-    const int gy = (int)std::min<uint32_t>(ntiles, (uint32_t)num_sms() * 2);
+    const int gy = (int)std::min<uint32_t>(ntiles, (uint32_t)num_sms());
     if (gy > 0) {
         hcp_y_kernel<M><<<gy, S::THREADS, S::SMEM, st>>>(sp, C, sp.pair_w, sp.pair_y, ep);
         MCTDHB_CUDA_TRY(cudaGetLastError());

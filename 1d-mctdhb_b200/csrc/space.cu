@@ -75,6 +75,7 @@ int space_init(SpaceCtx& s, int N, int M) {
     MCTDHB_CUDA_TRY(cudaMemcpy(s.d_dens_desc, desc.data(), desc.size() * sizeof(int),
                                cudaMemcpyHostToDevice));
     MCTDHB_CUDA_TRY(cudaMalloc(&s.d_dens_part, dens_partial_elems(s.view) * sizeof(double2)));
+    if (dens_prepare(s.view, nullptr, nullptr, nullptr)) return -1;
     // pair-space H.C: the pair matrix and its D(N-2, M) x P scratch; when the
     // scratch cannot be had the space keeps the per-row kernel
     if (hcp_eligible(N, M)) {

@@ -112,9 +112,14 @@ def test_batch_job_bytes_host():
 
     small = B.Batch.job_bytes(job(10, 3, 128), 5)
     big = B.Batch.job_bytes(job(40, 6, 128), 5)
-    nc = 1221759  # C(45, 5)
-    assert big > 6 * 16 * nc and big < 8 * 16 * nc  # 5 Krylov vectors + work vector dominate
+    nc, d2 = 1221759, 962598  # C(45, 5), C(43, 5): the N and N-2 boson spaces
+    # 5 Krylov vectors + work vector, and the pair-space H.C scratch
+    # (21 pairs x the N-2 space) dominate
+    core = 16 * (6 * nc + 21 * d2)
+    assert core < big < 1.05 * core
     assert small > 0 and small % 256 == 0 and big % 256 == 0
     assert B.Batch.job_bytes(job(40, 6, 1024), 5) > big  # orbital buffers grow with the grid
     with pytest.raises(B.MctdhbError):
         B.Batch.job_bytes(job(10, 9, 128), 5)  # the engine runs 2..8 orbitals
+    with pytest.raises(B.MctdhbError):
+        B.Batch.job_bytes(job(1, 4, 128), 5)  # and at least two bosons
