@@ -1,9 +1,9 @@
 """Builds libmctdhb_b200.so (the C ABI of include/mctdhb_gpu.h) for sm_100a.
 
 Every csrc/*.cu file is compiled by nvcc with
-`-gencode arch=compute_100a,code=sm_100a` in parallel (an object newer than
-its source and every header is kept), then linked into one shared library
-next to this file.  Works without a GPU (cross-compile).
+`-gencode arch=compute_100a,code=sm_100a` in parallel (an object is kept when
+its source and headers are unchanged since its compile started), then linked
+into one shared library next to this file.  Works without a GPU (cross-compile).
 
     python build.py [--verbose-ptxas] [--jobs N]
 """
@@ -41,15 +41,20 @@ def headers_mtime():
 
 def compile_one(src, verbose_ptxas, newest_header=0.0):
     obj = os.path.join(OBJ, os.path.basename(src).replace(".cu", ".o"))
-    if not verbose_ptxas and os.path.exists(obj) and \
-            os.path.getmtime(obj) > max(os.path.getmtime(src), newest_header):
-        return obj, ""  # up to date: newer than its source and every header
+    stamp = obj + ".inputs"  # newest input mtime when the object's compile started
+    newest = max(os.path.getmtime(src), newest_header)
+    if not verbose_ptxas and os.path.exists(obj) and os.path.exists(stamp):
+        with open(stamp) as f:
+            if float(f.read() or 0) >= newest:
+                return obj, ""  # up to date: built from the current source and headers
     cmd = [nvcc(), *ARCH, *FLAGS, "-c", src, "-o", obj]
     if verbose_ptxas:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
+    with open(stamp, "w") as f:
+        f.write(repr(newest))
     return obj, r.stderr
 
 

@@ -22,12 +22,13 @@ constexpr int kGramThreads = 256;
 constexpr int kGramMaxBlocks = 296;  // 2 x 148: fixed, so the sums depend on (N, M) only
 constexpr int kGramSmemBudget = 96 * 1024;  // A tile bytes: two blocks per SM
 
-// A tile layout: the RT-wide column chunks of a row sit RT + 1 words apart
-// and rows an odd number of 16-byte words apart, so the chunk reads of a
-// warp (different chunks of one row, or one column of consecutive rows)
-// fall in different shared-memory banks
+// A tile layout: the RT-wide column chunks of a row sit an odd number of
+// 16-byte words apart (RT for odd RT, RT + 1 for even RT) and so do the
+// rows, so the chunk reads of a warp (different chunks of one row, or one
+// column of consecutive rows) fall in different shared-memory banks
+__host__ __device__ constexpr int gram_chunk_stride(int RT) { return RT % 2 ? RT : RT + 1; }
 __host__ __device__ constexpr int gram_row_stride(int M, int R) {
-    return (gram_nt(M, R) * (gram_rt(gram_p(M, R)) + 1)) | 1;
+    return (gram_nt(M, R) * gram_chunk_stride(gram_rt(gram_p(M, R)))) | 1;
 }
 // rows per tile: the largest of 256 / 128 / 64 whose tile fits the budget
 __host__ __device__ constexpr int gram_rows(int M, int R) {

@@ -107,7 +107,8 @@ struct GramShape {
     static constexpr int GROUPS = (kGramThreads / NTILES) < ROWS ? (kGramThreads / NTILES) : ROWS;
     static_assert(ENT <= ROWS * PS, "the group reduction reuses the A tile");
     // word of column p in a row of the A tile
-    __host__ __device__ static constexpr int col(int p) { return (p / RT) * (RT + 1) + p % RT; }
+    static constexpr int CS = gram_chunk_stride(RT);
+    __host__ __device__ static constexpr int col(int p) { return (p / RT) * CS + p % RT; }
 };
 
 // Per-thread role in the Gram accumulation: group and upper-triangle tile.
@@ -185,8 +186,8 @@ __device__ __forceinline__ void gram_accumulate(const double2* As, const GramRol
         double2 a[RT], b[RT];
 #pragma unroll
         for (int x = 0; x < RT; x++) {
-            a[x] = As[r * PS + role.ti * (RT + 1) + x];
-            b[x] = As[r * PS + role.tj * (RT + 1) + x];
+            a[x] = As[r * PS + role.ti * S::CS + x];
+            b[x] = As[r * PS + role.tj * S::CS + x];
         }
 #pragma unroll
         for (int x = 0; x < RT; x++)

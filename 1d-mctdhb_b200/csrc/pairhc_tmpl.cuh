@@ -37,9 +37,11 @@ struct PairHcShape {
     static constexpr int PG = P <= 21 ? P : P / 2;   // Y outputs per consumer thread
     static constexpr int NPG = P / PG;               // consumer threads per row (1 or 2)
     static constexpr int CONSUMERS = 256;            // 8 warps: the contraction
-    static constexpr int PRODUCERS = 128;            // 4 warps: unrank and gather
-    static constexpr int THREADS = CONSUMERS + PRODUCERS;
     static constexpr int ROWS = CONSUMERS / NPG;     // rows of A per tile
+    // unrank and gather: one producer thread per row (M <= 6 has less
+    // contraction per row, so a tile needs the gather of 256 rows as fast)
+    static constexpr int PRODUCERS = ROWS;
+    static constexpr int THREADS = CONSUMERS + PRODUCERS;
     static constexpr size_t SMEM = (2 * (size_t)ROWS * PS + (size_t)P * P) * sizeof(double2);
 };
 

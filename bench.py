@@ -862,16 +862,20 @@ def run_profile():
     print("profile run done")
 
 
-def run_profile_kernels():
-    """the single-system kernels of the N=30 M=8 quench for ncu: set-up and
-    one untimed H.C + density outside the profiled range, then one H.C and
-    one density launch inside it (cudaProfilerStart/Stop; use
+def run_profile_kernels(size):
+    """single-system kernels for ncu at size "N,M" (30,8: the quench; other
+    sizes: grid 512 on [-10, 10], double well, g = 0.1): set-up and one
+    untimed H.C + density outside the profiled range, then one H.C and one
+    density launch inside it (cudaProfilerStart/Stop; use
     --profile-from-start off)"""
     import torch
 
     import mctdhb_b200 as mb
 
-    c = SINGLE["quench_n30_m8"]
+    N, M = (int(x) for x in size.split(","))
+    c = dict(SINGLE["quench_n30_m8"])
+    if (N, M) != (c["N"], c["M"]):
+        c.update(N=N, M=M, G=512, xi=BXI, xf=BXF)
     hob, hint, c0 = single_inputs(mb, c)
     sp = mb.Space(c["N"], c["M"])
     d_c = torch.from_numpy(c0).cuda()
@@ -909,13 +913,13 @@ def main():
     ap.add_argument("--serve-nmax", type=int, default=30)
     ap.add_argument("--profile", action="store_true",
                     help="one profiled batch step of a small mix (for ncu captures)")
-    ap.add_argument("--profile-kernels", action="store_true",
-                    help="one profiled H.C and density launch at N=30 M=8 (for ncu captures)")
+    ap.add_argument("--profile-kernels", metavar="N,M", nargs="?", const="30,8",
+                    help="one profiled H.C and density launch of one system (for ncu captures)")
     args = ap.parse_args()
     if args.profile:
         run_profile()
     elif args.profile_kernels:
-        run_profile_kernels()
+        run_profile_kernels(args.profile_kernels)
     elif args.impl == "reference":
         run_reference(args)
     else:
