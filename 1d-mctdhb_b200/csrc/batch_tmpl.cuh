@@ -33,8 +33,9 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
     constexpr int P = PS_::P, PS = PS_::PS, ROWS = PS_::ROWS;
     static_assert(ROWS == batch_pair_rows(M), "tile rows of the host lists");
     extern __shared__ double2 smem[];
-    double2* Wb = smem;              // two buffers of P x P
-    double2* Ab = smem + 2 * P * P;  // two buffers of ROWS x PS
+    constexpr int WS = PS_::WS;
+    double2* Wb = smem;               // two buffers of P x WS
+    double2* Ab = smem + 2 * P * WS;  // two buffers of ROWS x PS
     const int nt = batch_cnt(cnt, LIST_HY, M);
     const BatchTile* list = tiles + batch_off(cnt, LIST_HY, M);
     const int t = threadIdx.x;
@@ -44,7 +45,7 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
         const BatchTile tl = list[k];
         const BatchSlot& S = slots[tl.slot];
         if (!bt_hc_active(S)) return;
-        for (int i = pt; i < P * P; i += PS_::PRODUCERS) Wb[buf * P * P + i] = S.sp.pair_w[i];
+        pair_stage_w<M>(S.sp.pair_w, Wb + buf * P * WS, pt, PS_::PRODUCERS);
         pair_gather<M>(S.sp, S.V + (size_t)iter * S.nc, tl.idx, Ab + (size_t)buf * ROWS * PS, pt,
                        PS_::PRODUCERS);
     };
@@ -57,11 +58,9 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
         } else {
             const BatchTile tl = list[k];
             const BatchSlot& S = slots[tl.slot];
-            if (bt_hc_active(S)) {
-                const int r = t % ROWS, part = t / ROWS;  // part is warp-uniform
-                pair_contract<M>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * P, r, part,
-                                 tl.idx * ROWS + r, S.sp.dim2, S.sp.pair_y);
-            }
+            if (bt_hc_active(S))
+                pair_consume<M>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * WS, t,
+                                tl.idx * ROWS, S.sp.dim2, S.sp.pair_y);
         }
         __syncthreads();
     }
@@ -158,7 +157,7 @@ __global__ void __launch_bounds__(kBatchVecThreads)
 template <int M>
 constexpr size_t batch_y_smem() {
     using PS_ = PairHcShape<M>;
-    return (2 * (size_t)PS_::P * PS_::P + 2 * (size_t)PS_::ROWS * PS_::PS) * sizeof(double2);
+    return (2 * (size_t)PS_::P * PS_::WS + 2 * (size_t)PS_::ROWS * PS_::PS) * sizeof(double2);
 }
 
 template <int M>

@@ -42,8 +42,32 @@ struct PairHcShape {
     // contraction per row, so a tile needs the gather of 256 rows as fast)
     static constexpr int PRODUCERS = ROWS;
     static constexpr int THREADS = CONSUMERS + PRODUCERS;
-    static constexpr size_t SMEM = (2 * (size_t)ROWS * PS + (size_t)P * P) * sizeof(double2);
+    static constexpr int WS = P | 1;                 // odd row stride of the staged W
+    static constexpr size_t SMEM = (2 * (size_t)ROWS * PS + (size_t)P * WS) * sizeof(double2);
+    // tensor-core contraction: 8-wide output tiles, 4-deep k steps
+    static constexpr int NN = (P + 7) / 8;
+    static constexpr int NK = (P + 3) / 4;
 };
+
+// Contraction on the FP64 tensor cores (mma.sync m8n8k4 f64) rather than
+// FP64 FMA in the consumer threads.
+constexpr bool kPairMma = true;
+
+// FP64 mma.sync m8n8k4: D(8x8) += A(8x4) B(4x8); lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2(l%4)], D[l/4][2(l%4)+1]
+__device__ __forceinline__ void dmma84(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// W (P x P, global) staged into Ws[p * WS + q] by threads t, t + nt, ...
+template <int M>
+__device__ __forceinline__ void pair_stage_w(const double2* __restrict__ W, double2* Ws, int t,
+                                             int nt) {
+    using S = PairHcShape<M>;
+    for (int i = t; i < S::P * S::P; i += nt) Ws[(i / S::P) * S::WS + i % S::P] = W[i];
+}
 
 // ---------------------------------------------------------------------------
 // building blocks (shared with the batched engine, batch_tmpl.cuh)
@@ -103,11 +127,75 @@ __device__ __forceinline__ void pair_contract(const double2* As, const double2* 
     for (int q = 0; q < P; q++) {
         const double2 a = As[r * PS + q];
 #pragma unroll
-        for (int g = 0; g < PG; g++) acc[g] = cfma(Ws[(part * PG + g) * P + q], a, acc[g]);
+        for (int g = 0; g < PG; g++) acc[g] = cfma(Ws[(part * PG + g) * S::WS + q], a, acc[g]);
     }
     if (row < D2) {
 #pragma unroll
         for (int g = 0; g < PG; g++) Y[(size_t)(part * PG + g) * D2 + row] = acc[g];
+    }
+}
+
+// The same contraction for a whole tile by the consumer warps on the FP64
+// tensor cores, with three real products per complex product (Gauss):
+// T1 = Ar Wr^T, T2 = Ai Wi^T, T3 = (Ar + Ai)(Wr + Wi)^T, then Yr = T1 - T2,
+// Yi = T3 - T1 - T2.  Warp cw takes the 8-row strips cw, cw + 8, ... of the
+// tile; per 4-deep k step one A fragment (real and imaginary part in one
+// 16-byte load) and, per 8-wide output tile, one W fragment and three MMAs.
+// Columns q >= P are zero (A side); outputs p >= P are not stored.
+template <int M>
+__device__ __forceinline__ void pair_contract_mma(const double2* As, const double2* Ws, int cw,
+                                                  int lane, uint32_t row0, uint32_t D2,
+                                                  double2* __restrict__ Y) {
+    using S = PairHcShape<M>;
+    constexpr int P = S::P, PS = S::PS, WS = S::WS, NN = S::NN, NK = S::NK;
+    constexpr int STRIPS = S::ROWS / 8, CW = S::CONSUMERS / 32;
+    const int lr = lane >> 2, lk = lane & 3;
+    for (int st = cw; st < STRIPS; st += CW) {
+        double t1[NN][2], t2[NN][2], t3[NN][2];
+#pragma unroll
+        for (int n = 0; n < NN; n++)
+#pragma unroll
+            for (int j = 0; j < 2; j++) t1[n][j] = t2[n][j] = t3[n][j] = 0.0;
+        const double2* arow = As + (st * 8 + lr) * PS;
+#pragma unroll
+        for (int k = 0; k < NK; k++) {
+            const int q = k * 4 + lk;
+            const double2 a = q < P ? arow[q] : make_double2(0.0, 0.0);
+            const double as = a.x + a.y;
+#pragma unroll
+            for (int n = 0; n < NN; n++) {
+                const int p = n * 8 + lr;
+                const double2 w = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)];
+                dmma84(t1[n][0], t1[n][1], a.x, w.x);
+                dmma84(t2[n][0], t2[n][1], a.y, w.y);
+                dmma84(t3[n][0], t3[n][1], as, w.x + w.y);
+            }
+        }
+        const uint32_t m = row0 + st * 8 + lr;
+        if (m < D2) {
+#pragma unroll
+            for (int n = 0; n < NN; n++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int p = n * 8 + 2 * lk + j;
+                    if (p < P)
+                        Y[(size_t)p * D2 + m] =
+                            make_double2(t1[n][j] - t2[n][j], t3[n][j] - t1[n][j] - t2[n][j]);
+                }
+        }
+    }
+}
+
+// consumer thread t (0 .. CONSUMERS-1) of a tile whose first row is row0
+template <int M>
+__device__ __forceinline__ void pair_consume(const double2* As, const double2* Ws, int t,
+                                             uint32_t row0, uint32_t D2, double2* __restrict__ Y) {
+    using S = PairHcShape<M>;
+    if constexpr (kPairMma) {
+        pair_contract_mma<M>(As, Ws, t >> 5, t & 31, row0, D2, Y);
+    } else {
+        const int r = t % S::ROWS, part = t / S::ROWS;  // part is warp-uniform
+        pair_contract<M>(As, Ws, r, part, row0 + r, D2, Y);
     }
 }
 
@@ -195,11 +283,11 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
     using S = PairHcShape<M>;
     constexpr int P = S::P, PS = S::PS, ROWS = S::ROWS;
     extern __shared__ double2 smem[];
-    double2* Ws = smem;          // Ws[p * P + q]
-    double2* Ab = smem + P * P;  // two buffers of ROWS x PS
+    double2* Ws = smem;               // Ws[p * WS + q]
+    double2* Ab = smem + P * S::WS;   // two buffers of ROWS x PS
     if (ep.flag != nullptr && *ep.flag != 0) return;  // Lanczos breakdown: no-op
     const int t = threadIdx.x;
-    for (int i = t; i < P * P; i += S::THREADS) Ws[i] = W[i];
+    pair_stage_w<M>(W, Ws, t, S::THREADS);
     const uint32_t ntiles = (sp.dim2 + ROWS - 1) / ROWS;
     const bool producer = t >= S::CONSUMERS;
     const int pt = t - S::CONSUMERS;
@@ -212,8 +300,7 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
             if (nx < ntiles)
                 pair_gather<M>(sp, C, nx, Ab + (size_t)(buf ^ 1) * ROWS * PS, pt, S::PRODUCERS);
         } else {
-            const int r = t % ROWS, part = t / ROWS;  // part is warp-uniform
-            pair_contract<M>(Ab + (size_t)buf * ROWS * PS, Ws, r, part, tr * ROWS + r, sp.dim2, Y);
+            pair_consume<M>(Ab + (size_t)buf * ROWS * PS, Ws, t, tr * ROWS, sp.dim2, Y);
         }
         __syncthreads();
     }
