@@ -273,15 +273,15 @@ int rebuild_lists(mctdhb_batch_s* b) {
 
 // H.C of Lanczos iteration `iter` of the slots of orbital count M
 int hc_group(int M, const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
-             const int* cnt, int iter, cudaStream_t st) {
+             const int* cnt, int iter, cudaStream_t st, int parts = 3) {
     switch (M) {
-        case 2: return hcp_batch_launch<2>(slots, hy, hg, cnt, iter, st);
-        case 3: return hcp_batch_launch<3>(slots, hy, hg, cnt, iter, st);
-        case 4: return hcp_batch_launch<4>(slots, hy, hg, cnt, iter, st);
-        case 5: return hcp_batch_launch<5>(slots, hy, hg, cnt, iter, st);
-        case 6: return hcp_batch_launch<6>(slots, hy, hg, cnt, iter, st);
-        case 7: return hcp_batch_launch<7>(slots, hy, hg, cnt, iter, st);
-        case 8: return hcp_batch_launch<8>(slots, hy, hg, cnt, iter, st);
+        case 2: return hcp_batch_launch<2>(slots, hy, hg, cnt, iter, parts, st);
+        case 3: return hcp_batch_launch<3>(slots, hy, hg, cnt, iter, parts, st);
+        case 4: return hcp_batch_launch<4>(slots, hy, hg, cnt, iter, parts, st);
+        case 5: return hcp_batch_launch<5>(slots, hy, hg, cnt, iter, parts, st);
+        case 6: return hcp_batch_launch<6>(slots, hy, hg, cnt, iter, parts, st);
+        case 7: return hcp_batch_launch<7>(slots, hy, hg, cnt, iter, parts, st);
+        case 8: return hcp_batch_launch<8>(slots, hy, hg, cnt, iter, parts, st);
     }
     return 0;
 }
@@ -836,15 +836,16 @@ size_t mctdhb_batch_free_bytes(mctdhb_batch b) {
 
 int mctdhb_batch_kernel_count(mctdhb_batch b) { return b ? b->kernels : 0; }
 
-int mctdhb_batch_launch_hc(mctdhb_batch b, int norb) {
-    if (!b || norb < kBatchMinOrb || norb > kBatchMaxOrb) {
+int mctdhb_batch_launch_hc(mctdhb_batch b, int norb, int parts) {
+    if (!b || norb < kBatchMinOrb || norb > kBatchMaxOrb || parts < 1 || parts > 3) {
         set_error("mctdhb_batch_launch_hc: invalid argument");
         return -1;
     }
     std::lock_guard<std::mutex> lk(b->mu);
     if (b->lists_dirty && rebuild_lists(b)) return -1;
     if (prepare_group(norb)) return -1;
-    return hc_group(norb, b->d_slots, b->d_tl[LIST_HY], b->d_tl[LIST_HG], b->d_cnt, 0, b->st);
+    return hc_group(norb, b->d_slots, b->d_tl[LIST_HY], b->d_tl[LIST_HG], b->d_cnt, 0, b->st,
+                    parts);
 }
 
 void* mctdhb_batch_stream(mctdhb_batch b) { return b ? (void*)b->st : nullptr; }

@@ -107,13 +107,14 @@ __host__ __device__ constexpr int batch_pair_rows(int M) {
 
 // batch_m*.cu: per-M kernels over the tile lists.
 //   hcp_batch_launch   out = H V[iter] (- beta V[iter-1]) of every running
-//                      slot of orbital count M: pair contraction, gather-back
+//                      slot of orbital count M: pair contraction (parts & 1),
+//                      gather-back (parts & 2)
 //   gram_batch_launch  rho1 / rho2 of V[0] of the slots of orbital count M
 //                      (`list` / `nlist`: the slots, one finalize block each)
 //   batch_prepare      launch attributes (call before any stream capture)
 template <int M>
 int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
-                     const int* cnt, int iter, cudaStream_t st);
+                     const int* cnt, int iter, int parts, cudaStream_t st);
 template <int M>
 int gram_batch_launch(const BatchSlot* slots, const BatchTile* g2, const BatchTile* g1,
                       const int* cnt, const int* list, const int* nlist, int nblocks,

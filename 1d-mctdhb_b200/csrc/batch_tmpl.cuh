@@ -179,12 +179,16 @@ int batch_prepare() {
 
 template <int M>
 int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
-                     const int* cnt, int iter, cudaStream_t st) {
-    bhcp_y_kernel<M><<<num_sms(), PairHcShape<M>::THREADS, batch_y_smem<M>(), st>>>(slots, hy,
-                                                                                 cnt, iter);
-    MCTDHB_CUDA_TRY(cudaGetLastError());
-    bhcp_g_kernel<M><<<num_sms() * 8, kBatchHcRows, 0, st>>>(slots, hg, cnt, iter);
-    MCTDHB_CUDA_TRY(cudaGetLastError());
+                     const int* cnt, int iter, int parts, cudaStream_t st) {
+    if (parts & 1) {
+        bhcp_y_kernel<M><<<num_sms(), PairHcShape<M>::THREADS, batch_y_smem<M>(), st>>>(
+            slots, hy, cnt, iter);
+        MCTDHB_CUDA_TRY(cudaGetLastError());
+    }
+    if (parts & 2) {
+        bhcp_g_kernel<M><<<num_sms() * 8, kBatchHcRows, 0, st>>>(slots, hg, cnt, iter);
+        MCTDHB_CUDA_TRY(cudaGetLastError());
+    }
     return 0;
 }
 

@@ -41,6 +41,7 @@ EXPORTED = [
     "mctdhb_batch_free_bytes", "mctdhb_batch_admit", "mctdhb_batch_step", "mctdhb_batch_sync",
     "mctdhb_batch_poll", "mctdhb_batch_fetch", "mctdhb_batch_release",
     "mctdhb_batch_kernel_count", "mctdhb_batch_stream", "mctdhb_batch_launch_hc",
+    "mctdhb_fp64_mma_probe",
     "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
     "mctdhb_step_create", "mctdhb_step_launch", "mctdhb_step_kernel_count",
     "mctdhb_step_destroy",
@@ -200,7 +201,9 @@ def load(path=LIB_PATH):
     L.mctdhb_batch_stream.restype = vp
     L.mctdhb_batch_stream.argtypes = [vp]
     L.mctdhb_batch_launch_hc.restype = i
-    L.mctdhb_batch_launch_hc.argtypes = [vp, i]
+    L.mctdhb_batch_launch_hc.argtypes = [vp, i, i]
+    L.mctdhb_fp64_mma_probe.restype = i
+    L.mctdhb_fp64_mma_probe.argtypes = [i, i, vp, vp]
     _lib = L
     return L
 
@@ -603,5 +606,15 @@ class Batch:
 
         return torch.cuda.ExternalStream(int(load().mctdhb_batch_stream(self.h)))
 
-    def launch_hc(self, norb):
-        _check(load().mctdhb_batch_launch_hc(self.h, norb), "mctdhb_batch_launch_hc")
+    def launch_hc(self, norb, parts=3):
+        """one batched H.C launch of the jobs with norb orbitals: parts = 1
+        the pair contraction, 2 the gather-back, 3 both"""
+        _check(load().mctdhb_batch_launch_hc(self.h, norb, parts), "mctdhb_batch_launch_hc")
+
+
+def fp64_mma_probe(blocks, iters, out, stream=None):
+    """launch the FP64 tensor-core throughput probe (mctdhb_fp64_mma_probe):
+    out is a float64 device tensor of at least blocks * 256 elements; the
+    launch does blocks * 8 * iters * 8 * 512 FLOPs"""
+    _check(load().mctdhb_fp64_mma_probe(blocks, iters, _ptr(out), _stream_ptr(stream)),
+           "mctdhb_fp64_mma_probe")

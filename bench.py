@@ -425,24 +425,61 @@ def arena_bytes(mb, jobs, slack=1.02):
     return int(sum(mb.Batch.job_bytes(j, LZ) for j in jobs) * slack) + (64 << 20)
 
 
+def fp64_mma_peak(mb, torch, reps=5):
+    """measured FP64 tensor-core throughput (TFLOP/s) of this GPU: the
+    library's mma.sync f64 probe, 4 blocks of 256 threads per SM, timed with
+    CUDA events; the best of `reps` launches"""
+    blocks, iters = 4 * torch.cuda.get_device_properties(0).multi_processor_count, 2048
+    out = torch.empty(blocks * 256, dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream()
+    mb.fp64_mma_probe(blocks, iters, out, st)
+    best = float("inf")
+    for _ in range(reps):
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        mb.fp64_mma_probe(blocks, iters, out, st)
+        c.record(st)
+        torch.cuda.synchronize()
+        best = min(best, a.elapsed_time(c))
+    return blocks * 8 * iters * 8 * 512 / (best / 1000.0) / 1e12
+
+
+def pair_work(jobs, M):
+    """per launch of the batched H.C of the jobs with M orbitals:
+    contraction FLOPs (8 per complex multiply-add of Y = A W^T over the
+    N-2 boson space) and gather-back bytes (every Y value read once, H.C
+    written once)"""
+    from math import comb
+
+    P = M * (M + 1) // 2
+    d2 = sum(comb(j["npar"] - 2 + M - 1, M - 1) for j in jobs if j["norb"] == M)
+    nc = sum(dim(j["npar"], M) for j in jobs if j["norb"] == M)
+    return 8.0 * d2 * P * P, 16.0 * d2 * P + 16.0 * nc, d2
+
+
 def batch_hc_roofline(mb, torch, b, jobs, reps=5):
-    """time each orbital count's batched H.C launch on the engine's stream;
-    algorithmic bytes = sum over its jobs of 32 nc + 16 G(N, M)"""
+    """time each orbital count's batched H.C on the engine's stream, the pair
+    contraction and the gather-back separately"""
     st = b.stream
-    out = {}
-    for M in sorted({j["norb"] for j in jobs}):
-        byts = sum(32.0 * dim(j["npar"], M) + 16.0 * distinct_couplings(j["npar"], M)
-                   for j in jobs if j["norb"] == M)
-        b.launch_hc(M)
+
+    def timed(M, parts):
+        b.launch_hc(M, parts)
         a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(st)
         for _ in range(reps):
-            b.launch_hc(M)
+            b.launch_hc(M, parts)
         c.record(st)
         torch.cuda.synchronize()
-        ms = a.elapsed_time(c) / reps
-        out[M] = {"ms_per_launch": ms, "algorithmic_bytes": byts,
-                  "achieved_gbs": byts / (ms / 1000.0) / 1e9}
+        return a.elapsed_time(c) / reps
+
+    out = {}
+    for M in sorted({j["norb"] for j in jobs}):
+        flops, byts, d2 = pair_work(jobs, M)
+        ty, tg = timed(M, 1), timed(M, 2)
+        out[M] = {"contraction_ms": ty, "contraction_flops": flops,
+                  "contraction_tflops": flops / (ty / 1000.0) / 1e12,
+                  "gather_back_ms": tg, "gather_back_bytes": byts,
+                  "gather_back_gbs": byts / (tg / 1000.0) / 1e9, "rows_n_minus_2": d2}
     return out
 
 
@@ -709,20 +746,30 @@ def run_single(mb, torch, name, steps, warmup):
     t_dn = a.elapsed_time(b) / reps / 1000.0
     G = distinct_couplings(N, M)
     b_hc = 32.0 * nc + 16.0 * G
-    b_dn = 16.0 * nc + 16.0 * G
-    peak, kind = peaks()
+    from math import comb
+
+    P = M * (M + 1) // 2
+    d2, d1 = comb(N - 2 + M - 1, M - 1), comb(N - 1 + M - 1, M - 1)
+    f_hc = 8.0 * d2 * P * P
+    f_dn = 8.0 * (d2 * P * (P + 1) / 2 + d1 * M * (M + 1) / 2)
     sp.close()
     del sp, d_c, hc_out
     torch.cuda.empty_cache()
     return {"workload": c["workload"],
             "step": f"SIL({c['m']} H.C) + rho1 + rho2, one CUDA graph",
             "steps_per_s": 1000.0 / t_step, "ms_per_step": t_step, "norm_after": norm,
-            "hc": {"kernel": f"hc_kernel<{M}>", "ms_per_launch": t_hc * 1e3,
-                   "algorithmic_bytes_per_launch": b_hc, "achieved_gbs": b_hc / t_hc / 1e9,
-                   "peak": peak, "frac": b_hc / t_hc / 1e9 / peak, "peak_source": kind,
-                   "traffic": ncu_traffic().get(f"hc_n{N}_m{M}_bytes_per_launch")},
-            "density": {"ms_per_launch": t_dn * 1e3, "algorithmic_bytes_per_launch": b_dn,
-                        "achieved_gbs": b_dn / t_dn / 1e9}}
+            "hc": {"kernels": f"hcp_y_kernel<{M}> (pair contraction, FP64 mma.sync) + "
+                              f"hcp_g_kernel<{M}> (gather-back)",
+                   "ms_per_launch": t_hc * 1e3, "contraction_flops": f_hc,
+                   "contraction_tflops": f_hc / t_hc / 1e12,
+                   "pair_scratch_bytes": 16.0 * d2 * P,
+                   "gather_model_gbs": b_hc / t_hc / 1e9,
+                   "gather_model_note": "32 nc + 16 G bytes (one 16-byte gather per distinct "
+                                        "coupling) / time: the rate a gather-per-coupling H.C "
+                                        "would need to match this launch"},
+            "density": {"kernels": f"gram_kernel<{M},2> + gram_kernel<{M},1> + finalize",
+                        "ms_per_launch": t_dn * 1e3, "gram_flops": f_dn,
+                        "gram_tflops": f_dn / t_dn / 1e12}}
 
 
 # ---------------------------------------------------------------------------
@@ -804,17 +851,30 @@ def run_gpu(args):
     # roofline: the dominant kernel of the step, the batched H.C per M
     peak, kind = peaks()
     groups = batch_hc_roofline(mb, torch, b, jobs)
-    Mtop = max(groups, key=lambda m: groups[m]["ms_per_launch"])
+    mma_peak = fp64_mma_peak(mb, torch)
+    Mtop = max(groups, key=lambda m: groups[m]["contraction_ms"] + groups[m]["gather_back_ms"])
     gt = groups[Mtop]
+    tr = ncu_traffic()
+    traffic = None
+    if tr.get("bhcp_y_m6_bytes_per_launch") and Mtop == 6:  # scaled by the rows processed
+        traffic = tr["bhcp_y_m6_bytes_per_launch"] * gt["rows_n_minus_2"] / tr["bhcp_y_m6_rows"]
     line["roofline"] = {
-        "bound": "hbm", "kernel": f"hc_batch_kernel<{Mtop}>", "achieved": gt["achieved_gbs"],
-        "peak": peak, "unit": "GB/s", "frac": gt["achieved_gbs"] / peak, "peak_source": kind,
-        "traffic": ncu_traffic().get(f"hc_batch_m{Mtop}_bytes_per_launch"),
-        "algorithmic_bytes_per_launch": gt["algorithmic_bytes"],
-        "ms_per_launch": gt["ms_per_launch"],
+        "bound": "tensor", "kernel": f"bhcp_y_kernel<{Mtop}> (pair contraction, FP64 mma.sync)",
+        "achieved": gt["contraction_tflops"], "peak": mma_peak, "unit": "TFLOP/s",
+        "frac": gt["contraction_tflops"] / mma_peak,
+        "peak_source": "measured in this run: FP64 mma.sync probe (mctdhb_fp64_mma_probe)",
+        "traffic": traffic, "algorithmic_flops_per_launch": gt["contraction_flops"],
+        "ms_per_launch": gt["contraction_ms"],
+        "gather_back": {"kernel": f"bhcp_g_kernel<{Mtop}>", "bound": "hbm",
+                        "achieved": gt["gather_back_gbs"], "peak": peak, "unit": "GB/s",
+                        "frac": gt["gather_back_gbs"] / peak, "peak_source": kind,
+                        "ms_per_launch": gt["gather_back_ms"],
+                        "algorithmic_bytes_per_launch": gt["gather_back_bytes"]},
         "groups": {str(m): g for m, g in groups.items()},
-        "note": "achieved = algorithmic bytes (32 nc + 16 G per job) / launch time; the "
-                "gathers are served from L2 and L1, so this can exceed the DRAM copy peak"}
+        "note": "H.C = pair contraction Y = A W^T over the (N-2)-boson space (8 FLOPs per "
+                "complex multiply-add counted) + gather-back (each Y value read once, H.C "
+                "written once); traffic: ncu DRAM bytes of the contraction on a 24-job case "
+                "scaled by the rows processed"}
     # energies of a few jobs after warmup + steps, for the agreement check
     cmp_idx = {i: int(s1[slots[i]]) for i in range(0, len(jobs), 37)}
     e_batch = {i: float(energy[slots[i]]) for i in cmp_idx}

@@ -261,11 +261,19 @@ int    mctdhb_batch_fetch(mctdhb_batch b, int slot, void* orbitals, void* coef, 
 /* frees the slot and its arena range */
 int    mctdhb_batch_release(mctdhb_batch b, int slot);
 int    mctdhb_batch_kernel_count(mctdhb_batch b); /* kernels per step graph */
-/* one launch of the batched H.C kernel of the running jobs with norb
- * orbitals (out = H C of each job, on the engine's stream): a measurement
- * hook for timing the dominant kernel of a step */
-int    mctdhb_batch_launch_hc(mctdhb_batch b, int norb);
+/* one launch of the batched H.C of the running jobs with norb orbitals
+ * (out = H C of each job, on the engine's stream): parts = 1 the pair
+ * contraction, 2 the gather-back, 3 both; a measurement hook for timing the
+ * dominant kernels of a step */
+int    mctdhb_batch_launch_hc(mctdhb_batch b, int norb, int parts);
 void*  mctdhb_batch_stream(mctdhb_batch b);       /* the engine's cudaStream_t */
+
+/* Throughput probe of the FP64 tensor cores (no counterpart in the
+ * reference): `blocks` blocks of 256 threads, every warp running `iters`
+ * rounds of eight independent mma.sync m8n8k4 f64 chains, i.e.
+ * blocks * 8 * iters * 8 * 512 FLOPs; d_out receives blocks * 256 doubles.
+ * The roofline denominator of the pair contraction. */
+int    mctdhb_fp64_mma_probe(int blocks, int iters, void* d_out, void* stream);
 
 /* rho1 and rho2 of C, as mctdhb_dev_density_matrices computes them, with no
  * device allocation at all.  This entry point has no counterpart in the

@@ -51,6 +51,8 @@ MIX = [  # N, M, G, imag, rk, dt, g, steps
     (5, 2, 64, False, 2, 0.005, 0.3, 4),
     (8, 6, 128, False, 5, 0.005, 0.1, 3),
     (7, 5, 80, True, 5, 0.01, 0.2, 5),
+    (6, 7, 96, True, 5, 0.01, 0.3, 3),
+    (5, 8, 64, False, 5, 0.005, 0.2, 3),
 ]
 
 
