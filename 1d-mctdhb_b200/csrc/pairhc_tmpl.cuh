@@ -13,8 +13,8 @@
 //     Y_m(P) = sum_Q W[P][Q] A_m(Q)                 (hcp_y_kernel)
 //     (HC)_i = sum_{P in i} <i|a+_P|i-P> Y_{i-P}(P)  (hcp_g_kernel)
 // At N=30, M=8 this is 6.7 M x 36 gathers, a 36 x 36 complex matrix-vector
-// product per m (FP64 FMA, W staged in shared memory; gather and contraction
-// overlapped by warp specialisation) and 10.3 M x 36
+// product per m (FP64 tensor cores, W staged in shared memory; gather and
+// contraction overlapped by warp specialisation) and 10.3 M x 36
 // coalesced reads of Y, instead of ~576 scattered coefficient gathers per
 // row.  Y (D(N-2, M) x P complex, pair-major so that both kernels access it
 // with consecutive lanes on consecutive m) is scratch owned by the Fock
@@ -30,28 +30,37 @@
 
 namespace mctdhb {
 
+__host__ __device__ constexpr int pair_stride4(int x) { return x + ((12 - x % 8) % 8); }
+
 template <int M>
 struct PairHcShape {
     static constexpr int P = M * (M + 1) / 2;
-    static constexpr int PS = P | 1;                 // odd row stride: conflict-free columns
-    static constexpr int PG = P <= 21 ? P : P / 2;   // Y outputs per consumer thread
-    static constexpr int NPG = P / PG;               // consumer threads per row (1 or 2)
-    static constexpr int CONSUMERS = 256;            // 8 warps: the contraction
-    static constexpr int ROWS = CONSUMERS / NPG;     // rows of A per tile
-    // unrank and gather: one producer thread per row (M <= 6 has less
-    // contraction per row, so a tile needs the gather of 256 rows as fast)
+    static constexpr int CONSUMERS = 256;  // 8 warps: the contraction on the tensor cores
+    // Rows of A per tile, one producer thread per row (unrank and gather).
+    // Up to 6 orbitals a row carries little contraction, so a tile must
+    // keep 256 rows of gathers in flight for the tensor cores; at 7 and 8
+    // orbitals 128 rows do.
+    static constexpr bool WIDE = P <= 21;
+    static constexpr int ROWS = WIDE ? 256 : 128;
     static constexpr int PRODUCERS = ROWS;
     static constexpr int THREADS = CONSUMERS + PRODUCERS;
-    static constexpr int WS = P | 1;                 // odd row stride of the staged W
+    // Shared-memory strides in 16-byte words.  An 8-lane phase of a fragment
+    // load reads 4 consecutive words of 2 rows: with strides = 4 (mod 8)
+    // they fall in 8 different bank groups.  At 128 rows a row r starts at
+    // r * PS + ((r >> 1) & 3), so the 8 consecutive rows stored by 8
+    // producer lanes also fall in different bank groups; at 256 rows the
+    // tile takes an odd stride (conflict-free stores, two-way conflicts in
+    // the fragment loads) to fit two buffers in shared memory.
+    static constexpr int PS = WIDE ? (P | 1) : pair_stride4(P + 3);
+    static constexpr int WS = pair_stride4(P);
     static constexpr size_t SMEM = (2 * (size_t)ROWS * PS + (size_t)P * WS) * sizeof(double2);
     // tensor-core contraction: 8-wide output tiles, 4-deep k steps
     static constexpr int NN = (P + 7) / 8;
     static constexpr int NK = (P + 3) / 4;
+    __host__ __device__ static constexpr int row_at(int r) {
+        return WIDE ? r * PS : r * PS + ((r >> 1) & 3);
+    }
 };
-
-// Contraction on the FP64 tensor cores (mma.sync m8n8k4 f64) rather than
-// FP64 FMA in the consumer threads.
-constexpr bool kPairMma = true;
 
 // FP64 mma.sync m8n8k4: D(8x8) += A(8x4) B(4x8); lane l holds A[l/4][l%4],
 // B[l%4][l/4] and D[l/4][2(l%4)], D[l/4][2(l%4)+1]
@@ -73,12 +82,12 @@ __device__ __forceinline__ void pair_stage_w(const double2* __restrict__ W, doub
 // building blocks (shared with the batched engine, batch_tmpl.cuh)
 // ---------------------------------------------------------------------------
 // Rows r = r0, r0 + rstep, ... < ROWS of tile `tr` of the (N-2)-boson space
-// into As[r * PS + p]: A_m(Q) = sqrt((m_q+1)(m_l+1+[q=l])) C[m + e_q + e_l].
+// into As[row_at(r) + p]: A_m(Q) = sqrt((m_q+1)(m_l+1+[q=l])) C[m + e_q + e_l].
 template <int M>
 __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* __restrict__ C,
                                             uint32_t tr, double2* As, int r0, int rstep) {
     using S = PairHcShape<M>;
-    constexpr int P = S::P, PS = S::PS, ROWS = S::ROWS;
+    constexpr int P = S::P, ROWS = S::ROWS;
     const int N = sp.N;
     const uint32_t D2 = sp.dim2;
     const uint32_t jbase = sp.dim - D2;
@@ -107,36 +116,13 @@ __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* 
                     f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
                 v = cscale(__ldg(C + j), f);
             }
-            As[r * PS + p] = v;
+            As[S::row_at(r) + p] = v;
         });
     }
 }
 
-// Y_m(P) = sum_Q W[P][Q] A_m(Q) for row r of the tile and the PG outputs
-// P = part * PG + g, stored to Y[P * D2 + row] when row < D2
-template <int M>
-__device__ __forceinline__ void pair_contract(const double2* As, const double2* Ws, int r,
-                                              int part, uint32_t row, uint32_t D2,
-                                              double2* __restrict__ Y) {
-    using S = PairHcShape<M>;
-    constexpr int P = S::P, PS = S::PS, PG = S::PG;
-    double2 acc[PG];
-#pragma unroll
-    for (int g = 0; g < PG; g++) acc[g] = make_double2(0.0, 0.0);
-#pragma unroll 4
-    for (int q = 0; q < P; q++) {
-        const double2 a = As[r * PS + q];
-#pragma unroll
-        for (int g = 0; g < PG; g++) acc[g] = cfma(Ws[(part * PG + g) * S::WS + q], a, acc[g]);
-    }
-    if (row < D2) {
-#pragma unroll
-        for (int g = 0; g < PG; g++) Y[(size_t)(part * PG + g) * D2 + row] = acc[g];
-    }
-}
-
-// The same contraction for a whole tile by the consumer warps on the FP64
-// tensor cores, with three real products per complex product (Gauss):
+// Y_m(P) = sum_Q W[P][Q] A_m(Q) for a whole tile by the consumer warps on
+// the FP64 tensor cores, with three real products per complex product (Gauss):
 // T1 = Ar Wr^T, T2 = Ai Wi^T, T3 = (Ar + Ai)(Wr + Wi)^T, then Yr = T1 - T2,
 // Yi = T3 - T1 - T2.  Warp cw takes the 8-row strips cw, cw + 8, ... of the
 // tile; per 4-deep k step one A fragment (real and imaginary part in one
@@ -147,7 +133,7 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
                                                   int lane, uint32_t row0, uint32_t D2,
                                                   double2* __restrict__ Y) {
     using S = PairHcShape<M>;
-    constexpr int P = S::P, PS = S::PS, WS = S::WS, NN = S::NN, NK = S::NK;
+    constexpr int P = S::P, WS = S::WS, NN = S::NN, NK = S::NK;
     constexpr int STRIPS = S::ROWS / 8, CW = S::CONSUMERS / 32;
     const int lr = lane >> 2, lk = lane & 3;
     for (int st = cw; st < STRIPS; st += CW) {
@@ -156,7 +142,7 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
         for (int n = 0; n < NN; n++)
 #pragma unroll
             for (int j = 0; j < 2; j++) t1[n][j] = t2[n][j] = t3[n][j] = 0.0;
-        const double2* arow = As + (st * 8 + lr) * PS;
+        const double2* arow = As + S::row_at(st * 8 + lr);
 #pragma unroll
         for (int k = 0; k < NK; k++) {
             const int q = k * 4 + lk;
@@ -190,13 +176,7 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
 template <int M>
 __device__ __forceinline__ void pair_consume(const double2* As, const double2* Ws, int t,
                                              uint32_t row0, uint32_t D2, double2* __restrict__ Y) {
-    using S = PairHcShape<M>;
-    if constexpr (kPairMma) {
-        pair_contract_mma<M>(As, Ws, t >> 5, t & 31, row0, D2, Y);
-    } else {
-        const int r = t % S::ROWS, part = t / S::ROWS;  // part is warp-uniform
-        pair_contract<M>(As, Ws, r, part, row0 + r, D2, Y);
-    }
+    pair_contract_mma<M>(As, Ws, t >> 5, t & 31, row0, D2, Y);
 }
 
 // (HC)_row = sum over pairs P = {k <= s} present in the row of
