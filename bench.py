@@ -925,8 +925,9 @@ def run_profile():
 def run_profile_kernels(size):
     """single-system kernels for ncu at size "N,M" (30,8: the quench; other
     sizes: grid 512 on [-10, 10], double well, g = 0.1): set-up and one
-    untimed H.C + density outside the profiled range, then one H.C and one
-    density launch inside it (cudaProfilerStart/Stop; use
+    untimed H.C, density and configurational step outside the profiled
+    range, then one H.C, one density and one step (SIL + rho1 + rho2, one
+    CUDA graph) inside it (cudaProfilerStart/Stop; use
     --profile-from-start off)"""
     import torch
 
@@ -943,14 +944,19 @@ def run_profile_kernels(size):
     r1 = torch.empty(c["M"] ** 2, dtype=torch.complex128, device="cuda")
     r2 = torch.empty(c["M"] ** 4, dtype=torch.complex128, device="cuda")
     out = torch.empty_like(d_c)
+    stream = torch.cuda.current_stream()
+    step = mb.Step(sp, d_c, r1, r2, c["m"], c["dt"], False)
     sp.apply_hamiltonian(d_c, out)
     sp.density_matrices(d_c, r1, r2)
+    step.launch(stream)
     torch.cuda.synchronize()
     torch.cuda.profiler.start()
     sp.apply_hamiltonian(d_c, out)
     sp.density_matrices(d_c, r1, r2)
+    step.launch(stream)  # one configurational step (SIL + rho1 + rho2, one CUDA graph)
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
+    step.close()
     sp.close()
     print("profile run done")
 
