@@ -64,6 +64,32 @@ struct RowState {
     uint32_t F[M > 1 ? M - 1 : 1][4];  // T_m(L_m+d) - T_m(L_m), d = -2,-1,+1,+2
 };
 
+// One level of the greedy CNS decode: the largest L in [0, Lmax] with
+// T_x(L) = C(L+x, x+1) <= S.  A closed-form estimate -- exact for x = 0, the
+// root of the quadratic for x = 1, the (x+1)-th root of (x+1)! S less x/2
+// (T_x(L) ~ (L + x/2)^(x+1) / (x+1)!) for x >= 2 -- then corrected against
+// the table; the estimate is within one step for every S < 2^32 and x <= 6
+// (M <= 8, the templated kernels; the runtime-M kernels keep a binary
+// search), so a level costs two table loads instead of a binary search.
+// The corrections make the result exact whatever the estimate.
+__device__ __forceinline__ int cns_level(const uint32_t* __restrict__ Tx, int x, int Lmax,
+                                         uint32_t S) {
+    if (x == 0) return S < (uint32_t)Lmax ? (int)S : Lmax;
+    float est;
+    if (x == 1) {
+        est = (sqrtf(8.0f * (float)S + 1.0f) - 1.0f) * 0.5f;
+    } else {
+        float f = 1.0f;  // (x+1)!
+        for (int k = 2; k <= x + 1; k++) f *= (float)k;
+        est = powf(f * (float)S, 1.0f / (float)(x + 1)) - 0.5f * (float)x;
+    }
+    int L = est > 0.0f ? (int)est : 0;
+    L = L < Lmax ? L : Lmax;
+    while (L < Lmax && __ldg(Tx + L + 1) <= S) L++;
+    while (L > 0 && __ldg(Tx + L) > S) L--;
+    return L;
+}
+
 // Unrank `row` (greedy CNS decode, identical to set_config of space.c:138)
 // and fill the jump offsets.
 template <int M>
@@ -76,14 +102,7 @@ __device__ __forceinline__ void load_row(const SpaceView& sp, uint32_t row,
 #pragma unroll
     for (int m = M - 2; m >= 0; m--) {
         const uint32_t* Tm = sp.T + m * (N + 1);
-        int lo = 0, hi = Lnext;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (__ldg(Tm + mid) <= S)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
+        const int lo = cns_level(Tm, m, Lnext, S);
         S -= __ldg(Tm + lo);
         st.n[m + 1] = Lnext - lo;
         L[m] = lo;

@@ -66,14 +66,7 @@ __device__ __forceinline__ void gram_unrank(const uint32_t* __restrict__ T, int 
 #pragma unroll
     for (int x = M - 2; x >= 0; x--) {
         const uint32_t* Tx = T + x * (N + 1);
-        int lo = 0, hi = Lnext;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(Tx + mid) <= S)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
+        const int lo = cns_level(Tx, x, Lnext, S);
         S -= __ldg(Tx + lo);
         n[x + 1] = Lnext - lo;
         L[x] = lo;

@@ -41,6 +41,9 @@ struct PairHcShape {
     // keep 256 rows of gathers in flight for the tensor cores; at 7 and 8
     // orbitals 128 rows do.
     static constexpr bool WIDE = P <= 21;
+    // W fragments held in registers by the consumers (up to 5 orbitals; at 6
+    // they would spill under the 128-register budget of a 512-thread block)
+    static constexpr bool WREG = P <= 15;
     static constexpr int ROWS = WIDE ? 256 : 128;
     static constexpr int PRODUCERS = ROWS;
     static constexpr int THREADS = CONSUMERS + PRODUCERS;
@@ -136,6 +139,17 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
     constexpr int P = S::P, WS = S::WS, NN = S::NN, NK = S::NK;
     constexpr int STRIPS = S::ROWS / 8, CW = S::CONSUMERS / 32;
     const int lr = lane >> 2, lk = lane & 3;
+    // up to 5 orbitals the W fragments of the whole tile stay in registers
+    double2 wf[S::WREG ? NK : 1][S::WREG ? NN : 1];
+    if constexpr (S::WREG) {
+#pragma unroll
+        for (int k = 0; k < NK; k++)
+#pragma unroll
+            for (int n = 0; n < NN; n++) {
+                const int p = n * 8 + lr, q = k * 4 + lk;
+                wf[k][n] = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)];
+            }
+    }
     for (int st = cw; st < STRIPS; st += CW) {
         double t1[NN][2], t2[NN][2], t3[NN][2];
 #pragma unroll
@@ -150,8 +164,13 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
             const double as = a.x + a.y;
 #pragma unroll
             for (int n = 0; n < NN; n++) {
-                const int p = n * 8 + lr;
-                const double2 w = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)];
+                double2 w;
+                if constexpr (S::WREG) {
+                    w = wf[k][n];
+                } else {
+                    const int p = n * 8 + lr;
+                    w = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)];
+                }
                 dmma84(t1[n][0], t1[n][1], a.x, w.x);
                 dmma84(t2[n][0], t2[n][1], a.y, w.y);
                 dmma84(t3[n][0], t3[n][1], as, w.x + w.y);
@@ -199,14 +218,7 @@ __device__ __forceinline__ double2 pair_gather_back(const SpaceView& sp,
 #pragma unroll
         for (int x = M - 2; x >= 0; x--) {
             const uint32_t* Tx = sp.T + x * (N + 1);
-            int lo = 0, hi = Lnext;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (__ldg(Tx + mid) <= S)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
+            const int lo = cns_level(Tx, x, Lnext, S);
             S -= __ldg(Tx + lo);
             n[x + 1] = Lnext - lo;
             L[x] = lo;
