@@ -362,7 +362,7 @@ int enqueue_step(mctdhb_batch_s* b, unsigned mask) {
     bt_dot_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV, 0);
     bt_reduce_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 1, BS_DIAG, 0);
     for (int i = 0; i < lz - 1; i++) {
-        bt_subdots_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV, i);
+        bt_subdots(i, vgrid, st, S, V, nV);
         bt_reduce_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, i + 1, BS_ORTHO, 1);
         bt_orth_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV, i);
         bt_norm_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, i);

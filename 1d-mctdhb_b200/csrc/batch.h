@@ -18,7 +18,7 @@
 
 namespace mctdhb {
 
-constexpr int kBatchVecRows = 1024;  // rows of one vector tile (256 threads x 4)
+constexpr int kBatchVecRows = 4096;  // rows of one vector tile (256 threads x 16)
 constexpr int kBatchVecThreads = 256;
 constexpr int kBatchHcRows = 256;    // rows of one H.C gather-back tile (one 256-thread block)
 constexpr int kBatchMaxSlices = 1024;  // Gram slices per slot and annihilation order

@@ -282,30 +282,42 @@ __global__ void __launch_bounds__(kBatchVecThreads)
 
 // out -= alpha_i V[i]; part[k * vtiles + tile] = <V[k], out>, k <= i
 // (multiconfig_lanczos.c:46, :57-62)
+// (the iteration is a template parameter: only the i + 1 accumulators in
+// use take registers, which keeps enough warps resident)
+template <int I>
 __global__ void __launch_bounds__(kBatchVecThreads)
     bt_subdots_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
-                      const int* __restrict__ ntiles, int i) {
+                      const int* __restrict__ ntiles) {
     BT_TILE_LOOP
     if (!slot_running(S) || S.flags[BF_BREAK]) continue;
-    const double2 alpha = S.scal[BS_DIAG + i];
-    double2 acc[kBatchMaxLz];
+    const double2 alpha = S.scal[BS_DIAG + I];
+    double2 acc[I + 1];
 #pragma unroll
-    for (int k = 0; k < kBatchMaxLz; k++) acc[k] = make_double2(0.0, 0.0);
+    for (int k = 0; k <= I; k++) acc[k] = make_double2(0.0, 0.0);
     BT_ROWS(r) {
         double2 o = S.out[r];
-        const double2 av = cmul(alpha, S.V[(size_t)i * nc + r]);
+        const double2 av = cmul(alpha, S.V[(size_t)I * nc + r]);
         o.x -= av.x;
         o.y -= av.y;
         S.out[r] = o;
 #pragma unroll
-        for (int k = 0; k < kBatchMaxLz; k++)
-            if (k <= i) acc[k] = cfma_conj(S.V[(size_t)k * nc + r], o, acc[k]);
+        for (int k = 0; k <= I; k++) acc[k] = cfma_conj(S.V[(size_t)k * nc + r], o, acc[k]);
     }
-    for (int k = 0; k <= i; k++) {
+#pragma unroll
+    for (int k = 0; k <= I; k++) {
         const double2 s = block_sum(acc[k]);
         if (threadIdx.x == 0) S.part[(size_t)k * S.vtiles + tl.idx] = s;
     }
     }
+}
+
+template <int I>
+static void subdots_launch(int i, int grid, cudaStream_t st, const BatchSlot* slots,
+                           const BatchTile* tiles, const int* ntiles) {
+    if (i == I)
+        bt_subdots_kernel<I><<<grid, kBatchVecThreads, 0, st>>>(slots, tiles, ntiles);
+    else if constexpr (I > 0)
+        subdots_launch<I - 1>(i, grid, st, slots, tiles, ntiles);
 }
 
 // out -= sum_{k<=i} o_k V[k]; part[tile] = |out|^2 (multiconfig_lanczos.c:57-64)
@@ -532,5 +544,10 @@ __global__ void __launch_bounds__(kBatchVecThreads)
 }
 
 #undef BT_SLOT
+
+void bt_subdots(int i, int grid, cudaStream_t st, const BatchSlot* slots, const BatchTile* tiles,
+                const int* ntiles) {
+    subdots_launch<kBatchMaxLz - 2>(i, grid, st, slots, tiles, ntiles);
+}
 
 }  // namespace mctdhb

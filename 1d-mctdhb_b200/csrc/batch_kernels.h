@@ -11,9 +11,9 @@ __global__ void bt_orbital_kernel(const BatchSlot* __restrict__ slots, const int
 __global__ void bt_dot_kernel(const BatchSlot* __restrict__ slots,
                               const BatchTile* __restrict__ tiles, const int* __restrict__ ntiles,
                               int i);
-__global__ void bt_subdots_kernel(const BatchSlot* __restrict__ slots,
-                                  const BatchTile* __restrict__ tiles,
-                                  const int* __restrict__ ntiles, int i);
+// out -= alpha_i V[i] and the dots <V[k], out>, k <= i (one launch)
+void bt_subdots(int i, int grid, cudaStream_t st, const BatchSlot* slots, const BatchTile* tiles,
+                const int* ntiles);
 __global__ void bt_orth_kernel(const BatchSlot* __restrict__ slots,
                                const BatchTile* __restrict__ tiles, const int* __restrict__ ntiles,
                                int i);

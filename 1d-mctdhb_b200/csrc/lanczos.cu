@@ -86,16 +86,18 @@ int vec_dot(const double2* a, const double2* b, uint32_t n, double2* part, int g
 }
 
 // out -= a_i v_i (when k0 == 0), and partial dots <v_k, out> for k in [k0, k1]
+// NK = k1 - k0 + 1 dots (compile time: only the accumulators in use take
+// registers, which keeps enough warps resident for a memory-bound pass)
+template <int NK>
 __global__ void __launch_bounds__(256)
-    lz_sub_dots_kernel(int i, int k0, int k1, const double2* __restrict__ V, uint32_t n,
+    lz_sub_dots_kernel(int i, int k0, const double2* __restrict__ V, uint32_t n,
                        double2* __restrict__ out, const double2* __restrict__ scal,
                        const int* __restrict__ iflag, double2* __restrict__ part) {
     if (iflag[0]) return;
     const double2 alpha = scal[S_DIAG + i];
-    double2 acc[kDotChunk];
+    double2 acc[NK];
 #pragma unroll
-    for (int k = 0; k < kDotChunk; k++) acc[k] = make_double2(0.0, 0.0);
-    const int nk = k1 - k0 + 1;
+    for (int k = 0; k < NK; k++) acc[k] = make_double2(0.0, 0.0);
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         double2 o = out[r];
         if (k0 == 0) {
@@ -105,10 +107,20 @@ __global__ void __launch_bounds__(256)
             out[r] = o;
         }
 #pragma unroll
-        for (int k = 0; k < kDotChunk; k++)
-            if (k < nk) acc[k] = cfma_conj(V[(size_t)(k0 + k) * n + r], o, acc[k]);
+        for (int k = 0; k < NK; k++) acc[k] = cfma_conj(V[(size_t)(k0 + k) * n + r], o, acc[k]);
     }
-    for (int k = 0; k < nk; k++) block_reduce_store(acc[k], part + (size_t)k * gridDim.x);
+#pragma unroll
+    for (int k = 0; k < NK; k++) block_reduce_store(acc[k], part + (size_t)k * gridDim.x);
+}
+
+template <int NK>
+static void sub_dots_launch(int nk, int vg, cudaStream_t st, int i, int k0, const double2* V,
+                            uint32_t n, double2* out, const double2* scal, const int* iflag,
+                            double2* part) {
+    if (nk == NK)
+        lz_sub_dots_kernel<NK><<<vg, 256, 0, st>>>(i, k0, V, n, out, scal, iflag, part);
+    else if constexpr (NK > 1)
+        sub_dots_launch<NK - 1>(nk, vg, st, i, k0, V, n, out, scal, iflag, part);
 }
 
 // out -= sum_{k<=i} o_k v_k; partial |out|^2
@@ -307,8 +319,8 @@ int lanczos_run(const SpaceCtx& s, LanczosWork& w, int m, cudaStream_t st) {
     for (int i = 0; i < m - 1; i++) {
         for (int k0 = 0; k0 <= i; k0 += kDotChunk) {
             const int k1 = std::min(i, k0 + kDotChunk - 1);
-            lz_sub_dots_kernel<<<vg, 256, 0, st>>>(i, k0, k1, w.V, n, w.out, w.scal, w.iflag,
-                                                   w.part);
+            sub_dots_launch<kDotChunk>(k1 - k0 + 1, vg, st, i, k0, w.V, n, w.out, w.scal,
+                                       w.iflag, w.part);
             MCTDHB_CUDA_TRY(cudaGetLastError());
             if (reduce_rows(w.part, k1 - k0 + 1, vg, w.scal + S_ORTHO + k0, st)) return -1;
         }
