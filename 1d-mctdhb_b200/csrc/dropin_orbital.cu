@@ -189,6 +189,10 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
         mctdhb_solver_set_potential(s, eq->pot_grid) || mctdhb_solver_set_interaction(s, eq->g) ||
         mctdhb_solver_set_regularization(s, get_current_regularization_factor()))
         return;
+    // the projector the reference's driver selected (orbital_integration.c:219-227)
+    if (mctdhb->orb_workspace &&
+        mctdhb_solver_set_orthogonality(s, mctdhb->orb_workspace->impr_ortho ? 1 : 0))
+        return;
     cudaStream_t st = 0;
     if (mctdhb_solver_phase(s, 0, st)) return;
     // driver.c:175-177: time advances, trap and interaction follow in real time

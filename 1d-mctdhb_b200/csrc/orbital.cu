@@ -7,7 +7,9 @@
 //                        with the finite-difference linear part
 //                        (split_linear_orbitals.c:210-255), the interacting
 //                        part (split_nonlinear_orbitals.c:4-61) and the simple
-//                        projector (orbital_integration.c:95-131)
+//                        projector (orbital_integration.c:95-131) or, once
+//                        the orbitals drift from orthonormality, the robust
+//                        one (orbital_integration.c:22-92)
 //   Runge-Kutta step     propagate_fullstep_orb_rk (orbital_integration.c:284)
 //                        with the named tableaux Heun / classical RK4 /
 //                        Butcher RK5
@@ -148,6 +150,30 @@ __global__ void orb_overlap_kernel(OrbView o, const double2* __restrict__ y,
     if (threadIdx.x == 0) P[s * M + k] = r;
 }
 
+// robust projector (orbital_integration.c:22-92): P <- S^{-1} P with the full
+// overlap matrix S_sl = <f_s|f_l> (the reference's set_overlap_matrix,
+// orbital_matrices.c:7-19, starts its inner loop at 2 and leaves S_01 and
+// S_10 unset; the full matrix is its evident intent).  One thread: M <= 30.
+// A singular S sets *fail and leaves P as the simple projector's.
+__global__ void orb_robust_kernel(int M, const double2* __restrict__ S, double2* __restrict__ P,
+                                  double2* __restrict__ work, int* __restrict__ fail) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int M2 = M * M;
+    double2 *a = work, *inv = work + M2, *t = work + 2 * M2;
+    for (int i = 0; i < M2; i++) a[i] = S[i];
+    if (herm_inverse(M, a, inv)) {
+        *fail = 1;
+        return;
+    }
+    for (int s = 0; s < M; s++)
+        for (int k = 0; k < M; k++) {
+            double2 z = make_double2(0.0, 0.0);
+            for (int l = 0; l < M; l++) z = cfma(inv[s * M + l], P[l * M + k], z);
+            t[s * M + k] = z;
+        }
+    for (int i = 0; i < M2; i++) P[i] = t[i];
+}
+
 // dy/dt = -i tf (H_k - sum_s f_s <f_s|H_k>)
 __global__ void orb_rhs_finish_kernel(OrbView o, const double2* __restrict__ y,
                                       const double2* __restrict__ H,
@@ -232,6 +258,9 @@ int orb_init(OrbCtx& c, int M, int G, double xi, double xf, double a2, double2 a
     MCTDHB_CUDA_TRY(cudaMalloc(&c.d_Q, (size_t)M * M * M * M * sizeof(double2)));
     MCTDHB_CUDA_TRY(cudaMalloc(&c.d_g, sizeof(double)));
     MCTDHB_CUDA_TRY(cudaMalloc(&c.d_work, (3 * (size_t)M * M + M + 2) * sizeof(double2)));
+    MCTDHB_CUDA_TRY(cudaMalloc(&c.d_S, (size_t)M * M * sizeof(double2)));
+    MCTDHB_CUDA_TRY(cudaMalloc(&c.d_fail, sizeof(int)));
+    MCTDHB_CUDA_TRY(cudaMemset(c.d_fail, 0, sizeof(int)));
     c.view.M = M;
     c.view.G = G;
     c.view.dx = dx;
@@ -253,6 +282,8 @@ void orb_release(OrbCtx& c) {
     cudaFree(c.d_Q);
     cudaFree(c.d_g);
     cudaFree(c.d_work);
+    cudaFree(c.d_S);
+    cudaFree(c.d_fail);
     c = OrbCtx();
 }
 
@@ -271,6 +302,10 @@ static int orb_rhs(const OrbCtx& c, const double2* y, double2* out, cudaStream_t
     const int n = c.M * c.G;
     orb_haction_kernel<<<(n + 127) / 128, 128, 0, st>>>(c.view, y, c.d_Q, c.d_H);
     orb_overlap_kernel<<<c.M * c.M, 256, 0, st>>>(c.view, y, c.d_H, c.d_P);
+    if (c.robust) {
+        orb_overlap_kernel<<<c.M * c.M, 256, 0, st>>>(c.view, y, y, c.d_S);
+        orb_robust_kernel<<<1, 32, 0, st>>>(c.M, c.d_S, c.d_P, c.d_work, c.d_fail);
+    }
     orb_rhs_finish_kernel<<<(n + 255) / 256, 256, 0, st>>>(c.view, y, c.d_H, c.d_P, out);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
@@ -344,6 +379,12 @@ int orb_rhs_eval(const OrbCtx& c, const double2* rinv, const double2* rho2, cons
 
 int orb_periodic(const OrbCtx& c, double2* orb, cudaStream_t st) {
     periodic_kernel<<<1, 32, 0, st>>>(c.M, c.G, orb);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int orb_overlap_matrix(const OrbCtx& c, const double2* orb, cudaStream_t st) {
+    orb_overlap_kernel<<<c.M * c.M, 256, 0, st>>>(c.view, orb, orb, c.d_S);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -29,7 +29,10 @@ struct OrbCtx {
     double2* d_H = nullptr;        // H phi
     double2* d_P = nullptr;        // projector overlaps
     double2* d_Q = nullptr;        // g rho1^{-1} rho2
-    double2* d_work = nullptr;     // small dense work (rho1 synchronisation)
+    double2* d_work = nullptr;     // small dense work (rho1 synchronisation, projector)
+    double2* d_S = nullptr;        // orbital overlap matrix <f_s|f_l>
+    int* d_fail = nullptr;         // set when the robust projector met a singular overlap
+    int robust = 0;                // robust projector (orbital_integration.c:22-92)
 };
 
 std::vector<double> simpson_weights(int n, double h);
@@ -43,6 +46,8 @@ int orb_rhs_eval(const OrbCtx& c, const double2* rinv, const double2* rho2, cons
 int orb_rk_step(const OrbCtx& c, int order, double dt, const double2* rinv, const double2* rho2,
                 const double2* y, double2* ynext, cudaStream_t st);
 int orb_periodic(const OrbCtx& c, double2* orb, cudaStream_t st);
+// S_sl = <f_s|f_l> (Simpson) into c.d_S
+int orb_overlap_matrix(const OrbCtx& c, const double2* orb, cudaStream_t st);
 int orb_orthonormalize(const OrbCtx& c, double2* orb, cudaStream_t st);
 int orb_sync_rho1(const OrbCtx& c, double2* rho1, double2* rinv, double reg_fac, int* d_info,
                   cudaStream_t st);

@@ -217,6 +217,8 @@ int mctdhb_solver_set_potential(mctdhb_solver s, const double* pot) {
         set_error("mctdhb_solver_set_potential: null argument");
         return -1;
     }
+    // the steps may still run on a caller stream that this copy does not order with
+    MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
     MCTDHB_CUDA_TRY(cudaMemcpy(s->orb.d_pot, pot, s->G * sizeof(double), cudaMemcpyHostToDevice));
     return 0;
 }
@@ -226,6 +228,7 @@ int mctdhb_solver_set_interaction(mctdhb_solver s, double g) {
         set_error("mctdhb_solver_set_interaction: null solver");
         return -1;
     }
+    MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
     MCTDHB_CUDA_TRY(cudaMemcpy(s->orb.d_g, &g, sizeof(double), cudaMemcpyHostToDevice));
     return 0;
 }
@@ -235,8 +238,27 @@ int mctdhb_solver_set_regularization(mctdhb_solver s, double reg_fac) {
         set_error("mctdhb_solver_set_regularization: factor outside [1E-13, 1E-6]");
         return -1;
     }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (reg_fac == s->reg_fac) return 0;
     s->reg_fac = reg_fac;
     drop_graphs(s);  // the factor is a launch argument: capture again
+    return 0;
+}
+
+// The projector of the orbital equation: 0 the simple one, 1 the robust one
+// with the inverse overlap matrix (orbital_integration.c:22-131; the
+// reference switches when impr_ortho is set, driver.c:70-96).
+int mctdhb_solver_set_orthogonality(mctdhb_solver s, int robust) {
+    if (!s) {
+        set_error("mctdhb_solver_set_orthogonality: null solver");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    robust = robust ? 1 : 0;
+    if (robust == s->orb.robust) return 0;
+    MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
+    s->orb.robust = robust;
+    drop_graphs(s);  // the projector is part of the captured step
     return 0;
 }
 
@@ -284,6 +306,20 @@ int mctdhb_solver_step(mctdhb_solver s, int nsteps, void* stream) {
         s->t += s->dt;
     }
     MCTDHB_CUDA_TRY(cudaEventRecord(s->ev_step, (cudaStream_t)stream));
+    return 0;
+}
+
+// One phase of a step (0: orbitals at the current trap and interaction;
+// 1: matrices of the new orbitals, SIL, densities), for callers that change
+// the trap or the interaction between the two (driver.c:176-177)
+int mctdhb_solver_step_phase(mctdhb_solver s, int phase, void* stream) {
+    if (!s || !s->has_state || phase < 0 || phase > 1) {
+        set_error("mctdhb_solver_step_phase: invalid argument or solver without state");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (mctdhb_solver_phase(s, phase, (cudaStream_t)stream)) return -1;
+    if (phase == 1) s->t += s->dt;
     return 0;
 }
 
@@ -354,6 +390,110 @@ int mctdhb_solver_energy(mctdhb_solver s, double* e) {
     MCTDHB_CUDA_TRY(cudaStreamSynchronize(s->cs));
     e[0] = v.x;
     e[1] = v.y;
+    return 0;
+}
+
+// sum_{k<l} |<f_k|f_l>| / M of the current orbitals (integrator_monitor.c:31-42);
+// fails when a step met a singular overlap matrix in the robust projector
+int mctdhb_solver_overlap_residual(mctdhb_solver s, double* res) {
+    if (!s || !res) {
+        set_error("mctdhb_solver_overlap_residual: null argument");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int M = s->M;
+    std::vector<double2> S((size_t)M * M);
+    int fail = 0;
+    MCTDHB_CUDA_TRY(cudaStreamWaitEvent(s->cs, s->ev_step, 0));
+    if (orb_overlap_matrix(s->orb, s->d_orb, s->cs)) return -1;
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(S.data(), s->orb.d_S, S.size() * sizeof(double2),
+                                    cudaMemcpyDeviceToHost, s->cs));
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(&fail, s->orb.d_fail, sizeof(int), cudaMemcpyDeviceToHost,
+                                    s->cs));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(s->cs));
+    if (fail) {
+        set_error("mctdhb_solver: singular orbital overlap matrix in the robust projector");
+        return -1;
+    }
+    double sum = 0.0;
+    for (int k = 0; k < M; k++)
+        for (int l = k + 1; l < M; l++) sum += std::hypot(S[k * M + l].x, S[k * M + l].y);
+    *res = sum / M;
+    return 0;
+}
+
+namespace {
+// max_i |e c_i - (Hc)_i| over the grid, as the bits of a non-negative double
+__global__ void resid_max_kernel(size_t n, double e, const double2* __restrict__ c,
+                                 const double2* __restrict__ hc,
+                                 unsigned long long* __restrict__ out) {
+    double m = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        m = fmax(m, hypot(e * c[i].x - hc[i].x, e * c[i].y - hc[i].y));
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+}  // namespace
+
+// max_i |e c_i - (H c)_i| / N with the current h, g (integrator_monitor.c:9-28)
+int mctdhb_solver_eig_residual(mctdhb_solver s, double e, double* res) {
+    if (!s || !res || !s->has_state) {
+        set_error("mctdhb_solver_eig_residual: null argument or solver without state");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    const size_t nc = mctdhb_space_dim(s->sp);
+    if (s->M == 1) {  // one configuration: H c = E_gp c exactly
+        *res = 0.0;
+        return 0;
+    }
+    std::lock_guard<std::mutex> lk2(s->sp->mu);
+    SpaceCtx& sc = s->sp->sp;
+    unsigned long long bits = 0;
+    auto* d_bits = reinterpret_cast<unsigned long long*>(s->d_E);
+    MCTDHB_CUDA_TRY(cudaStreamWaitEvent(s->cs, s->ev_step, 0));
+    // the step leaves h, g of the current orbitals in the H.C tables
+    HcEpilogue ep;
+    if (hc_apply(sc.view, s->d_coef, s->sp->lw.out, sc.d_tab, ep, s->cs)) return -1;
+    MCTDHB_CUDA_TRY(cudaMemsetAsync(d_bits, 0, sizeof(bits), s->cs));
+    resid_max_kernel<<<592, 256, 0, s->cs>>>(nc, e, s->d_coef, s->sp->lw.out, d_bits);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(&bits, d_bits, sizeof(bits), cudaMemcpyDeviceToHost, s->cs));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(s->cs));
+    double m;
+    std::memcpy(&m, &bits, sizeof(m));
+    *res = m / s->N;
+    return 0;
+}
+
+// Replaces the coefficients by the lowest eigenvector of H in the current
+// orbitals after `niter` Lanczos iterations (multiconfig_lanczos.c,
+// lowest_state_lanczos; the final diagonalisation of driver.c:296-306).  The
+// density matrices are not recomputed, as there; *e is the Lanczos energy.
+int mctdhb_solver_lowest_state(mctdhb_solver s, int niter, double* e) {
+    if (!s || !s->has_state || niter < 1 || niter > 64) {
+        set_error("mctdhb_solver_lowest_state: invalid argument or solver without state");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->M == 1) {
+        if (e) *e = NAN;
+        return 0;
+    }
+    std::lock_guard<std::mutex> lk2(s->sp->mu);
+    MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
+    if (s->sp->lw.mmax < niter) {  // the step graphs hold the old Lanczos buffers
+        drop_graphs(s);
+        lanczos_free(s->sp->lw);
+        if (lanczos_alloc(s->sp->lw, s->sp->sp, niter)) return -1;
+    }
+    double* d_e = reinterpret_cast<double*>(s->d_E);
+    if (lowest_state(s->sp->sp, s->sp->lw, s->d_coef, niter, d_e, s->cs)) return -1;
+    double v = NAN;
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(&v, d_e, sizeof(v), cudaMemcpyDeviceToHost, s->cs));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(s->cs));
+    if (e) *e = v;
     return 0;
 }
 

@@ -44,6 +44,7 @@ EXPORTED = [
     "mctdhb_fp64_mma_probe",
     "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
     "mctdhb_step_create", "mctdhb_step_launch", "mctdhb_step_kernel_count",
+    "mctdhb_solver_step_phase",
     "mctdhb_step_destroy",
     "set_orbital_hob", "set_orbital_hint", "sync_orbital_matrices", "mctdhb_propagate_step",
     "mctdhb_solver_create", "mctdhb_solver_destroy", "mctdhb_solver_set_potential",
@@ -51,6 +52,8 @@ EXPORTED = [
     "mctdhb_solver_set_state", "mctdhb_solver_step", "mctdhb_solver_kernel_count",
     "mctdhb_solver_get", "mctdhb_solver_put", "mctdhb_solver_energy",
     "mctdhb_solver_device_coef", "mctdhb_solver_device_orbitals", "mctdhb_solver_time",
+    "mctdhb_solver_set_orthogonality", "mctdhb_solver_overlap_residual",
+    "mctdhb_solver_eig_residual", "mctdhb_solver_lowest_state",
 ]
 
 _lib = None
@@ -170,6 +173,14 @@ def load(path=LIB_PATH):
     L.mctdhb_solver_put.argtypes = [vp] + [vp] * 4
     L.mctdhb_solver_energy.restype = i
     L.mctdhb_solver_energy.argtypes = [vp, C.POINTER(d)]
+    L.mctdhb_solver_set_orthogonality.restype = i
+    L.mctdhb_solver_set_orthogonality.argtypes = [vp, i]
+    L.mctdhb_solver_overlap_residual.restype = i
+    L.mctdhb_solver_overlap_residual.argtypes = [vp, C.POINTER(d)]
+    L.mctdhb_solver_eig_residual.restype = i
+    L.mctdhb_solver_eig_residual.argtypes = [vp, d, C.POINTER(d)]
+    L.mctdhb_solver_lowest_state.restype = i
+    L.mctdhb_solver_lowest_state.argtypes = [vp, i, C.POINTER(d)]
     L.mctdhb_solver_device_coef.restype = vp
     L.mctdhb_solver_device_coef.argtypes = [vp]
     L.mctdhb_solver_device_orbitals.restype = vp
@@ -202,6 +213,8 @@ def load(path=LIB_PATH):
     L.mctdhb_batch_stream.argtypes = [vp]
     L.mctdhb_batch_launch_hc.restype = i
     L.mctdhb_batch_launch_hc.argtypes = [vp, i, i]
+    L.mctdhb_solver_step_phase.restype = i
+    L.mctdhb_solver_step_phase.argtypes = [vp, i, vp]
     L.mctdhb_fp64_mma_probe.restype = i
     L.mctdhb_fp64_mma_probe.argtypes = [i, i, vp, vp]
     _lib = L
@@ -361,6 +374,11 @@ class Solver:
     def step(self, n=1, stream=None):
         _check(load().mctdhb_solver_step(self.h, n, _stream_ptr(stream)), "mctdhb_solver_step")
 
+    def step_phase(self, phase, stream=None):
+        """one half of a step: 0 the orbitals, 1 matrices + SIL + densities"""
+        _check(load().mctdhb_solver_step_phase(self.h, phase, _stream_ptr(stream)),
+               "mctdhb_solver_step_phase")
+
     @property
     def kernels(self):
         return int(load().mctdhb_solver_kernel_count(self.h))
@@ -380,6 +398,33 @@ class Solver:
         e = (C.c_double * 2)()
         _check(load().mctdhb_solver_energy(self.h, e), "mctdhb_solver_energy")
         return complex(e[0], e[1])
+
+    def set_regularization(self, reg_fac):
+        _check(load().mctdhb_solver_set_regularization(self.h, reg_fac),
+               "mctdhb_solver_set_regularization")
+
+    def set_orthogonality(self, robust):
+        """projector of the orbital equation: False simple, True robust"""
+        _check(load().mctdhb_solver_set_orthogonality(self.h, int(bool(robust))),
+               "mctdhb_solver_set_orthogonality")
+
+    def overlap_residual(self):
+        r = C.c_double()
+        _check(load().mctdhb_solver_overlap_residual(self.h, C.byref(r)),
+               "mctdhb_solver_overlap_residual")
+        return r.value
+
+    def eig_residual(self, e):
+        r = C.c_double()
+        _check(load().mctdhb_solver_eig_residual(self.h, e, C.byref(r)),
+               "mctdhb_solver_eig_residual")
+        return r.value
+
+    def lowest_state(self, niter):
+        e = C.c_double()
+        _check(load().mctdhb_solver_lowest_state(self.h, niter, C.byref(e)),
+               "mctdhb_solver_lowest_state")
+        return e.value
 
 
 class DropIn:

@@ -179,12 +179,35 @@ int  mctdhb_solver_set_regularization(mctdhb_solver s, double reg_fac);
 /* initial orbitals + coefficients, then rho1, rho2, rho1^{-1}, h, g */
 int  mctdhb_solver_set_state(mctdhb_solver s, const void* orb, const void* coef);
 int  mctdhb_solver_step(mctdhb_solver s, int nsteps, void* stream);
+/* one half of a step (mctdhb_propagate_step, driver.c:159-201): phase 0
+ * advances the orbitals with the current trap and interaction, phase 1
+ * forms h and g of the new orbitals and runs the SIL step and the
+ * densities; a caller that follows time-dependent parameters sets the trap
+ * and interaction of the new time in between (sync_equation_params,
+ * synchronize.c:59-68) */
+int  mctdhb_solver_step_phase(mctdhb_solver s, int phase, void* stream);
 int  mctdhb_solver_kernel_count(mctdhb_solver s); /* kernels per step */
 int  mctdhb_solver_get(mctdhb_solver s, void* orb, void* coef, void* hob, void* hint, void* rho1,
                        void* rho2, void* rinv);
 int  mctdhb_solver_put(mctdhb_solver s, const void* orb, const void* coef, const void* rho2,
                        const void* rinv);
 int  mctdhb_solver_energy(mctdhb_solver s, double* e_re_im); /* Tr(rho1 h) + rho2 g / 2 */
+/* Monitor of the reference's integration_driver (src/integrator/driver.c:46-96,
+ * 296-306), on the device-resident state:
+ *   set_orthogonality  0: simple projector, 1: robust projector with the
+ *                      inverse overlap matrix (impr_ortho,
+ *                      src/integrator/orbital_integration.c:22-131)
+ *   overlap_residual   sum_{k<l} |<f_k|f_l>| / M (overlap_residual,
+ *                      src/assistant/integrator_monitor.c:31-42)
+ *   eig_residual       max_i |e c_i - (H c)_i| / N (eig_residual,
+ *                      src/assistant/integrator_monitor.c:9-28)
+ *   lowest_state       coefficients <- lowest Lanczos eigenvector in the
+ *                      current orbitals (lowest_state_lanczos,
+ *                      include/linalg/multiconfig_lanczos.h); densities kept */
+int  mctdhb_solver_set_orthogonality(mctdhb_solver s, int robust);
+int  mctdhb_solver_overlap_residual(mctdhb_solver s, double* res);
+int  mctdhb_solver_eig_residual(mctdhb_solver s, double e, double* res);
+int  mctdhb_solver_lowest_state(mctdhb_solver s, int niter, double* e);
 void*  mctdhb_solver_device_coef(mctdhb_solver s);
 void*  mctdhb_solver_device_orbitals(mctdhb_solver s);
 double mctdhb_solver_time(mctdhb_solver s);

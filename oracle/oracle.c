@@ -1476,12 +1476,19 @@ linear_fd(int G, double dx, double a2, ocplx a1, int periodic, const double* pot
     }
 }
 
-/* orbital_integration.c:179-240 (FINITEDIFF, simple projector) */
-void
+/* orbital_integration.c:179-240 (FINITEDIFF).  robust = 0: the simple
+ * projector (:95-131), P_k = sum_s f_s <f_s|H f_k>; robust = 1: the robust
+ * projector (:22-92), P_k = sum_{s,l} f_s (S^-1)_{sl} <f_l|H f_k> with the
+ * overlap matrix S_{sl} = <f_s|f_l> (orbital_matrices.c:7-19, all entries:
+ * that loop starts its inner index at 2, which leaves S_01 and S_10 as
+ * uninitialised heap memory in the reference; the full matrix is its
+ * evident intent).  Returns 0, or the inversion's error code with dodt
+ * untouched. */
+int
 orc_orbital_rhs(int M, int G, double dx, double a2, ocplx a1, double g,
                 int periodic, ocplx time_fac, const double* pot,
                 const ocplx* rinv, const ocplx* rho2, const ocplx* orb,
-                ocplx* dodt)
+                ocplx* dodt, int robust)
 {
     ocplx* lin = malloc(sizeof(ocplx) * M * G);
     ocplx* ha = malloc(sizeof(ocplx) * M * G);
@@ -1497,22 +1504,47 @@ orc_orbital_rhs(int M, int G, double dx, double a2, ocplx a1, double g,
     for (int k = 0; k < M; k++)
         for (int s = 0; s < M; s++)
             po[s * M + k] = sprod(G, dx, orb + s * G, ha + k * G, w);
-    for (int k = 0; k < M; k++)
-        for (int i = 0; i < G; i++)
-        {
-            ocplx proj = 0;
-            for (int s = 0; s < M; s++) proj += orb[s * G + i] * po[s * M + k];
-            dodt[k * G + i] = -I * time_fac * (ha[k * G + i] - proj);
-        }
+    int info = 0;
+    if (robust)
+    {
+        ocplx* ov = malloc(sizeof(ocplx) * M * M);
+        ocplx* inv = malloc(sizeof(ocplx) * M * M);
+        ocplx* pr = malloc(sizeof(ocplx) * M * M);
+        for (int s = 0; s < M; s++)
+            for (int l = 0; l < M; l++)
+                ov[s * M + l] = sprod(G, dx, orb + s * G, orb + l * G, w);
+        info = orc_herm_inverse(M, ov, inv);
+        for (int s = 0; s < M; s++)
+            for (int k = 0; k < M; k++)
+            {
+                ocplx z = 0;
+                for (int l = 0; l < M; l++) z += inv[s * M + l] * po[l * M + k];
+                pr[s * M + k] = z;
+            }
+        memcpy(po, pr, sizeof(ocplx) * M * M);
+        free(ov);
+        free(inv);
+        free(pr);
+    }
+    if (info == 0)
+        for (int k = 0; k < M; k++)
+            for (int i = 0; i < G; i++)
+            {
+                ocplx proj = 0;
+                for (int s = 0; s < M; s++)
+                    proj += orb[s * G + i] * po[s * M + k];
+                dodt[k * G + i] = -I * time_fac * (ha[k * G + i] - proj);
+            }
     free(lin);
     free(ha);
     free(po);
     free(w);
+    return info;
 }
 
 typedef struct
 {
-    int           M, G, periodic;
+    int           M, G, periodic, robust;
     double        dx, a2, g;
     ocplx         a1, tf;
     const double* pot;
@@ -1523,7 +1555,7 @@ static void
 rhs_eval(const rhs_args* a, const ocplx* y, ocplx* out)
 {
     orc_orbital_rhs(a->M, a->G, a->dx, a->a2, a->a1, a->g, a->periodic, a->tf,
-                    a->pot, a->rinv, a->rho2, y, out);
+                    a->pot, a->rinv, a->rho2, y, out, a->robust);
 }
 
 /* the named tableaux of shim/odesys.h (Heun, classical RK4, Butcher RK5) */
@@ -1585,12 +1617,12 @@ orc_propagate_step(int npar, int M, int G, double dx, double dt, double a2,
                    ocplx a1, double g, int periodic, int imagtime, int rk_order,
                    int lanczos_m, double reg_fac, const double* pot, ocplx* orb,
                    ocplx* coef, ocplx* hob, ocplx* hint, ocplx* rho1,
-                   ocplx* rho2, ocplx* rinv)
+                   ocplx* rho2, ocplx* rinv, int robust)
 {
     int      n = M * G;
     ocplx    tf = imagtime ? -I : 1.0;
     ocplx    prop_dt = imagtime ? -I * dt : dt;
-    rhs_args a = {M, G, periodic, dx, a2, g, a1, tf, pot, rinv, rho2};
+    rhs_args a = {M, G, periodic, robust, dx, a2, g, a1, tf, pot, rinv, rho2};
     if (periodic)
         for (int k = 0; k < M; k++) orb[k * G + G - 1] = orb[k * G];
     ocplx* next = malloc(sizeof(ocplx) * n);

@@ -111,18 +111,22 @@ void orc_sync_density_matrices(int npar, int norb, const ocplx* coef,
                                ocplx* rho1_inv);
 /* orbital_integration.c:179-240 with FINITEDIFF linear part
  * (split_linear_orbitals.c:210-255), orb_interacting_part
- * (split_nonlinear_orbitals.c:4-61) and simple projector (:95-131) */
-void orc_orbital_rhs(int norb, int npts, double dx, double d2coef,
-                     ocplx d1coef, double g, int periodic, ocplx time_fac,
-                     const double* pot, const ocplx* rho1_inv,
-                     const ocplx* rho2, const ocplx* orb, ocplx* dodt);
+ * (split_nonlinear_orbitals.c:4-61) and the simple projector (:95-131), or
+ * with robust != 0 the robust projector (:22-92).  Returns 0, or the
+ * overlap inversion's error code. */
+int orc_orbital_rhs(int norb, int npts, double dx, double d2coef,
+                    ocplx d1coef, double g, int periodic, ocplx time_fac,
+                    const double* pot, const ocplx* rho1_inv,
+                    const ocplx* rho2, const ocplx* orb, ocplx* dodt,
+                    int robust);
 /* one full step of driver.c:159-201 (FULLSTEP_RUNGEKUTTA + LANCZOS, FD,
  * time-independent trap and interaction).  rk_order in {2,4,5} with the
- * named tableaux of shim/odesys.h.  State arrays are updated in place. */
+ * named tableaux of shim/odesys.h; robust selects the projector as in
+ * orc_orbital_rhs.  State arrays are updated in place. */
 void orc_propagate_step(int npar, int norb, int npts, double dx, double dt,
                         double d2coef, ocplx d1coef, double g, int periodic,
                         int imagtime, int rk_order, int lanczos_m,
                         double reg_fac, const double* pot, ocplx* orb,
                         ocplx* coef, ocplx* hob, ocplx* hint, ocplx* rho1,
-                        ocplx* rho2, ocplx* rho1_inv);
+                        ocplx* rho2, ocplx* rho1_inv, int robust);
 #endif

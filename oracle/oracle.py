@@ -92,11 +92,12 @@ class Oracle:
         L.orc_herm_inverse.restype = i
         L.orc_herm_inverse.argtypes = [i, _c128p, _c128p]
         L.orc_sync_density_matrices.argtypes = [i, i, _c128p, C.c_double, _c128p, _c128p, _c128p]
+        L.orc_orbital_rhs.restype = i
         L.orc_orbital_rhs.argtypes = [i, i, C.c_double, C.c_double, _C128, C.c_double, i, _C128,
-                                      _f64p, _c128p, _c128p, _c128p, _c128p]
+                                      _f64p, _c128p, _c128p, _c128p, _c128p, i]
         L.orc_propagate_step.argtypes = [i, i, i, C.c_double, C.c_double, C.c_double, _C128,
                                          C.c_double, i, i, i, i, C.c_double, _f64p,
-                                         _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, _c128p]
+                                         _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, i]
 
     # ---- space -------------------------------------------------------
     def dim(self, N, M):
@@ -257,16 +258,20 @@ class Oracle:
         self.lib.orc_sync_density_matrices(N, M, cvec(c), reg_fac, r1, r2, ri)
         return r1.reshape(M, M), r2, ri.reshape(M, M)
 
-    def orbital_rhs(self, orb, dx, d2coef, d1coef, g, periodic, time_fac, pot, rinv, rho2):
+    def orbital_rhs(self, orb, dx, d2coef, d1coef, g, periodic, time_fac, pot, rinv, rho2,
+                    robust=False):
         M, G = orb.shape
         out = np.zeros(M * G, np.complex128)
-        self.lib.orc_orbital_rhs(M, G, dx, d2coef, _c(d1coef), g, int(periodic), _c(time_fac),
-                                 np.ascontiguousarray(pot, np.float64), cvec(rinv).reshape(-1),
-                                 cvec(rho2).reshape(-1), cvec(orb).reshape(-1), out)
+        info = self.lib.orc_orbital_rhs(M, G, dx, d2coef, _c(d1coef), g, int(periodic),
+                                        _c(time_fac), np.ascontiguousarray(pot, np.float64),
+                                        cvec(rinv).reshape(-1), cvec(rho2).reshape(-1),
+                                        cvec(orb).reshape(-1), out, int(robust))
+        if info:
+            raise ValueError(f"singular overlap matrix (column {info - 1})")
         return out.reshape(M, G)
 
     def propagate_step(self, st, N, dx, dt, d2coef, d1coef, g, periodic, imagtime, rk_order,
-                       lanczos_m, pot, reg_fac=1e-9):
+                       lanczos_m, pot, reg_fac=1e-9, robust=False):
         """One full step; `st` is a dict of numpy arrays updated in place:
         orb (M,G), coef, hob (M,M), hint, rho1 (M,M), rho2, rinv (M,M)."""
         M, G = st["orb"].shape
@@ -276,7 +281,7 @@ class Oracle:
         self.lib.orc_propagate_step(N, M, G, dx, dt, d2coef, _c(d1coef), g, int(periodic),
                                     int(imagtime), rk_order, lanczos_m, reg_fac,
                                     np.ascontiguousarray(pot, np.float64),
-                                    *[a.reshape(-1) for a in args])
+                                    *[a.reshape(-1) for a in args], int(robust))
 
 
 class Reference:
@@ -377,15 +382,17 @@ class Reference:
         return C.cast(getattr(self.lib, name), C.c_void_p).value
 
     def make_mctdhb(self, N, M, G, xi, xf, imagtime, rk_order, lanczos_m, dt, omega, g,
-                    periodic=True):
+                    periodic=True, omega_f=None, pot_period=0.0, g_f=None, g_period=0.0):
         """A reference MCTDHBDataStruct from its own constructor
         (types_definition.c:247): FULLSTEP_RUNGEKUTTA orbitals, FINITEDIFF
         derivatives, LANCZOS coefficients, harmonic trap
-        (builtin_potential.c:37) and constant g (builtin_time_parameter.c:7).
-        Returns (struct pointer, keep-alive list)."""
+        (builtin_potential.c:37) swept omega -> omega_f over pot_period and
+        g ramped g -> g_f over g_period (builtin_time_parameter.c:7); constant
+        by default.  Returns (struct pointer, keep-alive list)."""
         L = self.lib
-        pot_args = (C.c_double * 3)(omega, omega, 0.0)
-        g_args = (C.c_double * 3)(g, g, 0.0)
+        pot_args = (C.c_double * 5)(omega, omega if omega_f is None else omega_f, pot_period,
+                                    0.0, 0.0)
+        g_args = (C.c_double * 5)(g, g if g_f is None else g_f, g_period, 0.0, 0.0)
         ms = L.get_mctdhb_struct(
             T.IMAGTIME if imagtime else T.REALTIME, T.LANCZOS, T.FULLSTEP_RUNGEKUTTA,
             T.FINITEDIFF, rk_order, lanczos_m, N, M, b"harmonic",

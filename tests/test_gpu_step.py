@@ -162,6 +162,129 @@ def test_dropin_step_vs_reference(gpu, reference, imag, rk):
         reference.destroy_mctdhb(B)
 
 
+def skewed_orbitals(M, G, xi, xf, seed, amp=0.02):
+    """Hermite functions plus a periodic perturbation: not orthonormal"""
+    orb, dx = hermite_orbitals(M, G, xi, xf)
+    rng = np.random.default_rng(seed)
+    orb = orb + amp * (rng.normal(size=orb.shape) + 1j * rng.normal(size=orb.shape))
+    orb[:, -1] = orb[:, 0]
+    return np.ascontiguousarray(orb), dx
+
+
+@pytest.mark.parametrize("M,imag", [(3, False), (4, True), (6, False)])
+def test_solver_robust_projector_vs_oracle(gpu, oracle, M, imag):
+    """the robust projector (inverse overlap matrix, orbital_integration.c:
+    22-92) on non-orthonormal orbitals against the oracle's, then back to
+    the simple projector"""
+    N, G, dt, g, steps = 6, 96, 0.005, 0.6, 4
+    xi, xf = -8.0, 8.0
+    orb, dx = skewed_orbitals(M, G, xi, xf, 70 + M)
+    coef = rand_coef(np.random.default_rng(M), oracle.dim(N, M))
+    pot = harmonic(G, xi, xf)
+    s = gpu.Solver(N, M, G, xi, xf, dt, imag, 5, 5)
+    s.set_potential(pot)
+    s.set_interaction(g)
+    s.set_state(orb, coef)
+    s.set_orthogonality(True)
+    st = oracle_init(oracle, N, orb, coef, dx, pot, g)
+    for _ in range(steps):
+        oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, imag, 5, 5, pot, robust=True)
+    s.step(steps)
+    d = s.get()
+    assert rel_err(d["orb"], st["orb"]) < 1e-10
+    assert rel_err(d["coef"], st["coef"]) < 1e-10
+    assert rel_err(d["rho1"], st["rho1"]) < 1e-10
+    s.set_orthogonality(False)
+    for _ in range(2):
+        oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, imag, 5, 5, pot)
+    s.step(2)
+    d = s.get()
+    assert rel_err(d["orb"], st["orb"]) < 1e-10
+    assert rel_err(d["coef"], st["coef"]) < 1e-10
+    s.close()
+
+
+def test_solver_monitor_vs_oracle(gpu, oracle):
+    """overlap residual, eigen-residual and the final lowest-state
+    diagonalisation of the reference's driver on the device state"""
+    N, M, G, dt, g, m = 8, 4, 128, 0.01, 0.5, 5
+    xi, xf = -8.0, 8.0
+    orb, dx = skewed_orbitals(M, G, xi, xf, 11)
+    coef = rand_coef(np.random.default_rng(12), oracle.dim(N, M))
+    pot = harmonic(G, xi, xf)
+    s = gpu.Solver(N, M, G, xi, xf, dt, False, 5, m)
+    s.set_potential(pot)
+    s.set_interaction(g)
+    s.set_state(orb, coef)
+    s.step(3)
+    d = s.get()
+    S = np.array([[oracle.simpson(dx, np.conj(d["orb"][k]) * d["orb"][l]) for l in range(M)]
+                  for k in range(M)])
+    want = sum(abs(S[k, l]) for k in range(M) for l in range(k + 1, M)) / M
+    assert want > 1e-3
+    assert abs(s.overlap_residual() - want) < 1e-12 * want
+    e = s.energy().real
+    r = s.eig_residual(e)
+    r_or = oracle.eig_residual(N, M, d["coef"], d["hob"], d["hint"], e)
+    assert r_or > 1e-6 and abs(r - r_or) < 1e-10 * r_or
+    it = 20  # more than the solver's 16 Lanczos buffers: they are reallocated
+    e_l = s.lowest_state(it)
+    e_o, c_o = oracle.lowest_state_lanczos(N, M, d["hob"], d["hint"], it, d["coef"])
+    assert abs(e_l - e_o) < 1e-10 * abs(e_o)
+    d2 = s.get()
+    ph = np.vdot(d2["coef"], c_o)
+    ph /= abs(ph)
+    assert rel_err(d2["coef"] * ph, c_o) < 1e-8
+    assert np.array_equal(d2["rho1"], d["rho1"])  # densities kept, as in driver.c:296-306
+    assert abs(s.energy().real - e) < 1e-14 * abs(e)
+    r_l = s.eig_residual(e_l)
+    assert r_l < r
+    assert abs(r_l - oracle.eig_residual(N, M, d2["coef"], d["hob"], d["hint"], e_l)) < 1e-8 * r_l
+    # the step graphs were captured with the old Lanczos buffers: stepping
+    # again after the larger diagonalisation must still match the oracle
+    st = oracle_init(oracle, N, d2["orb"], d2["coef"], dx, pot, g)
+    st["rho1"], st["rho2"], st["rinv"] = d2["rho1"].copy(), d2["rho2"].copy(), d2["rinv"].copy()
+    oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, False, 5, m, pot)
+    s.step(1)
+    d3 = s.get()
+    assert rel_err(d3["coef"], st["coef"]) < 1e-10
+    s.close()
+
+
+def test_dropin_step_honours_impr_ortho(gpu, reference, oracle):
+    """a reference-built struct with impr_ortho set, stepped by the GPU
+    drop-in, against the oracle's robust projector (the reference's own
+    robust path reads two uninitialised overlap entries,
+    orbital_matrices.c:13, and cannot serve as the check here)"""
+    N, M, G, m, dt, g = 5, 3, 64, 5, 0.01, 0.5
+    xi, xf = -8.0, 8.0
+    orb, dx = skewed_orbitals(M, G, xi, xf, 3)
+    coef = rand_coef(np.random.default_rng(43), reference.lib.space_dimension(N, M))
+    B, kb = reference.make_mctdhb(N, M, G, xi, xf, False, 5, m, dt, 1.0, g)
+    try:
+        reference.set_state(B, orb, coef)
+        r0 = reference.get_state(B)
+        st = {k: np.ascontiguousarray(r0[k].copy()) for k in
+              ("orb", "coef", "hob", "hint", "rho1", "rho2", "rinv")}
+        B.contents.orb_workspace.contents.impr_ortho = 1
+        L = gpu.load()
+        import mctdhb_types as T
+
+        for k in range(3):
+            ow = np.zeros(M * G, np.complex128)
+            cw = np.zeros(len(coef), np.complex128)
+            L.mctdhb_gpu_clear_error()
+            L.mctdhb_propagate_step(B, T.carray(ow), T.carray(cw), k)
+            assert gpu.last_error() == "", gpu.last_error()
+            oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, False, 5, m, r0["pot"],
+                                  robust=True)
+        b = reference.get_state(B)
+        for key in ("orb", "coef", "rho1"):
+            assert rel_err(b[key], st[key]) < 1e-10, key
+    finally:
+        reference.destroy_mctdhb(B)
+
+
 def relax(gpu, oracle, G, steps=1000):
     N, M, xi, xf, dt, g, m = 10, 4, -10.0, 10.0, 0.01, 0.5, 5
     orb, dx = hermite_orbitals(M, G, xi, xf)

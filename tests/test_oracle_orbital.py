@@ -91,3 +91,33 @@ def test_rk5_is_fifth_order(oracle):
         errs.append(abs(y - np.exp(1j * h)))
     assert 50 < errs[0] / errs[1] < 80  # 2^6 = 64
     importlib.invalidate_caches()
+
+
+def test_robust_projector_oracle(oracle):
+    """The oracle's robust projector (orbital_integration.c:22-92) leaves the
+    right-hand side orthogonal to every orbital, also for orbitals that are
+    not orthonormal, where the simple projector does not; on orthonormal
+    orbitals the two agree.  (The reference's orthonormalize, calculus.c:
+    171-191, re-evaluates the scalar product inside the grid loop, so its
+    output is not orthonormal for skewed input; the oracle keeps that.)"""
+    N, M, G, xi, xf, g = 6, 3, 96, -8.0, 8.0, 0.8
+    orb, dx = hermite_orbitals(M, G, xi, xf)
+    rng = np.random.default_rng(5)
+    skew = orb + 0.05 * (rng.normal(size=orb.shape) + 1j * rng.normal(size=orb.shape))
+    skew[:, -1] = skew[:, 0]
+    pot = 0.5 * np.linspace(xi, xf, G) ** 2
+    _, r2, ri = oracle.sync_density_matrices(N, M, rand_coef(rng, oracle.dim(N, M)))
+    args = (dx, -0.5, 0.0, g, True, 1.0, pot, ri, r2)
+
+    def overlaps(f, d):
+        return np.array([[oracle.simpson(dx, np.conj(f[j]) * d[k]) for k in range(M)]
+                         for j in range(M)])
+
+    rob = oracle.orbital_rhs(skew, *args, robust=True)
+    simple = oracle.orbital_rhs(skew, *args)
+    scale = np.abs(rob).max()
+    assert np.abs(overlaps(skew, rob)).max() < 1e-12 * scale
+    assert np.abs(overlaps(skew, simple)).max() > 1e-4 * scale
+    # the Hermite functions are orthonormal under the Simpson rule to 1e-15
+    assert rel_err(oracle.orbital_rhs(orb, *args, robust=True), oracle.orbital_rhs(orb, *args)) \
+        < 1e-12
