@@ -99,7 +99,7 @@ int job_layout(int N, int M, int G, int lz, JobLayout& L) {
     L.o_Q = take(M4 * z);
     L.o_hob = take(M2 * z);
     L.o_hint = take(M4 * z);
-    L.o_pw = take(P * P * z);
+    L.o_pw = take((P * P + 1) * z);  // + the real-W flag (pairhc_tmpl.cuh)
     L.o_rho1 = take(M2 * z);
     L.o_rho2 = take(M4 * z);
     L.o_rinv = take(M2 * z);

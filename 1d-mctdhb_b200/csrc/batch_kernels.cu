@@ -240,10 +240,18 @@ __global__ void __launch_bounds__(kBatchOrbThreads)
     }
     bt_matrices(S);
     __syncthreads();
-    // the pair matrix of H.C for the new h and g (pairhc_tmpl.cuh)
-    for (int e = threadIdx.x; e < M * (M + 1) / 2 * (M * (M + 1) / 2); e += blockDim.x)
-        S.sp.pair_w[e] = pair_w_entry(S.N, M, S.hob, S.hint, e);
+    // the pair matrix of H.C for the new h and g, and its real flag
+    // (pairhc_tmpl.cuh)
+    const int P2 = M * (M + 1) / 2 * (M * (M + 1) / 2);
+    bool real = true;
+    for (int e = threadIdx.x; e < P2; e += blockDim.x) {
+        const double2 w = pair_w_entry(S.N, M, S.hob, S.hint, e);
+        real = real && w.y == 0.0;
+        S.sp.pair_w[e] = w;
+    }
+    real = __syncthreads_and(real);
     if (threadIdx.x == 0) {
+        S.sp.pair_w[P2] = make_double2(real ? 1.0 : 0.0, 0.0);
         // Lanczos set-up of this step (multiconfig_lanczos.c:30-41)
         S.flags[BF_BREAK] = 0;
         S.flags[BF_ITERS] = S.lz;

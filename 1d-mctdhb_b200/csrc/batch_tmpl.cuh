@@ -22,9 +22,18 @@ __device__ __forceinline__ bool bt_hc_active(const BatchSlot& S) {
 }
 
 // Pair contraction Y = A W^T of V[iter] for every tile of list LIST_HY:
-// warp-specialised and double-buffered as hcp_y_kernel; the producer warps
-// stage each tile's W with its A, since consecutive tiles may belong to
-// different slots.
+// warp-specialised and double-buffered as hcp_y_kernel.  Consecutive tiles
+// may belong to different slots, so the producer warps stage a tile's W with
+// its A (skipped when the buffer already holds that slot's W) and publish
+// the tile's output row, size, Y plane and real-W flag in shared memory; the
+// consumers start on the tensor cores without a chain of global loads.  The
+// next tile's descriptor is loaded one tile ahead.
+struct PairTileMeta {
+    double2* Y;
+    uint32_t row0, D2;
+    int active, real;
+};
+
 template <int M>
 __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
     bhcp_y_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
@@ -33,6 +42,7 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
     constexpr int P = PS_::P, PS = PS_::PS, ROWS = PS_::ROWS;
     static_assert(ROWS == batch_pair_rows(M), "tile rows of the host lists");
     extern __shared__ double2 smem[];
+    __shared__ PairTileMeta meta[2];
     constexpr int WS = PS_::WS;
     double2* Wb = smem;               // two buffers of P x WS
     double2* Ab = smem + 2 * P * WS;  // two buffers of ROWS x PS
@@ -41,26 +51,40 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
     const int t = threadIdx.x;
     const bool producer = t >= PS_::CONSUMERS;
     const int pt = t - PS_::CONSUMERS;
-    auto fill = [&](int k, int buf) {
-        const BatchTile tl = list[k];
+    int wslot[2] = {-1, -1};  // slot whose W each buffer holds (same in every producer)
+    auto fill = [&](const BatchTile tl, int buf) {
         const BatchSlot& S = slots[tl.slot];
-        if (!bt_hc_active(S)) return;
-        pair_stage_w<M>(S.sp.pair_w, Wb + buf * P * WS, pt, PS_::PRODUCERS);
+        const bool active = bt_hc_active(S);
+        if (pt == 0)
+            meta[buf] = PairTileMeta{S.sp.pair_y, tl.idx * (uint32_t)ROWS, S.sp.dim2, active,
+                                     active && S.sp.pair_w[P * P].x != 0.0};
+        if (!active) return;
+        if (wslot[buf] != tl.slot) {
+            pair_stage_w<M>(S.sp.pair_w, Wb + buf * P * WS, pt, PS_::PRODUCERS);
+            wslot[buf] = tl.slot;
+        }
         pair_gather<M>(S.sp, S.V + (size_t)iter * S.nc, tl.idx, Ab + (size_t)buf * ROWS * PS, pt,
                        PS_::PRODUCERS);
     };
-    if (producer && (int)blockIdx.x < nt) fill(blockIdx.x, 0);
+    BatchTile next{};
+    if (producer) {
+        if ((int)blockIdx.x < nt) fill(list[blockIdx.x], 0);
+        if ((int)(blockIdx.x + gridDim.x) < nt) next = list[blockIdx.x + gridDim.x];
+    }
     __syncthreads();
     int buf = 0;
     for (int k = blockIdx.x; k < nt; k += gridDim.x, buf ^= 1) {
         if (producer) {
-            if (k + (int)gridDim.x < nt) fill(k + gridDim.x, buf ^ 1);
+            if (k + (int)gridDim.x < nt) {
+                const BatchTile cur = next;
+                if (k + 2 * (int)gridDim.x < nt) next = list[k + 2 * gridDim.x];
+                fill(cur, buf ^ 1);
+            }
         } else {
-            const BatchTile tl = list[k];
-            const BatchSlot& S = slots[tl.slot];
-            if (bt_hc_active(S))
-                pair_consume<M>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * WS, t,
-                                tl.idx * ROWS, S.sp.dim2, S.sp.pair_y);
+            const PairTileMeta tm = meta[buf];
+            if (tm.active)
+                pair_consume<M>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * WS, t, tm.row0,
+                                tm.D2, tm.Y, tm.real != 0);
         }
         __syncthreads();
     }

@@ -140,11 +140,19 @@ __global__ void __launch_bounds__(128)
 // ---------------------------------------------------------------------------
 // pair matrix W of H = sum_{P,Q} W[P][Q] a+_P a_Q (pairhc_tmpl.cuh)
 // ---------------------------------------------------------------------------
+// one block; W[P*P].x = 1 when every entry is real (the contraction then
+// runs two real products instead of three)
 __global__ void hcp_w_kernel(int N, int M, const double2* __restrict__ hob,
                              const double2* __restrict__ hint, double2* __restrict__ W) {
     const int P = M * (M + 1) / 2;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < P * P; e += gridDim.x * blockDim.x)
-        W[e] = pair_w_entry(N, M, hob, hint, e);
+    bool real = true;
+    for (int e = threadIdx.x; e < P * P; e += blockDim.x) {
+        const double2 w = pair_w_entry(N, M, hob, hint, e);
+        real = real && w.y == 0.0;
+        W[e] = w;
+    }
+    real = __syncthreads_and(real);
+    if (threadIdx.x == 0) W[P * P] = make_double2(real ? 1.0 : 0.0, 0.0);
 }
 
 bool hcp_eligible(int N, int M) { return N >= 2 && M >= 2 && M <= kMaxTemplOrb; }
@@ -172,8 +180,7 @@ int hc_prep(const SpaceView& sp, const double2* d_hob, const double2* d_hint, do
     hc_prep_kernel<<<1, 32, 0, st>>>(sp.M, d_hob, d_hint, d_tab);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     if (sp.pair_y != nullptr) {
-        const int P = sp.M * (sp.M + 1) / 2;
-        hcp_w_kernel<<<(P * P + 127) / 128, 128, 0, st>>>(sp.N, sp.M, d_hob, d_hint, sp.pair_w);
+        hcp_w_kernel<<<1, 256, 0, st>>>(sp.N, sp.M, d_hob, d_hint, sp.pair_w);
         MCTDHB_CUDA_TRY(cudaGetLastError());
     }
     return 0;

@@ -127,11 +127,14 @@ __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* 
 // Y_m(P) = sum_Q W[P][Q] A_m(Q) for a whole tile by the consumer warps on
 // the FP64 tensor cores, with three real products per complex product (Gauss):
 // T1 = Ar Wr^T, T2 = Ai Wi^T, T3 = (Ar + Ai)(Wr + Wi)^T, then Yr = T1 - T2,
-// Yi = T3 - T1 - T2.  Warp cw takes the 8-row strips cw, cw + 8, ... of the
-// tile; per 4-deep k step one A fragment (real and imaginary part in one
-// 16-byte load) and, per 8-wide output tile, one W fragment and three MMAs.
-// Columns q >= P are zero (A side); outputs p >= P are not stored.
-template <int M>
+// Yi = T3 - T1 - T2.  When W is real (REAL: real orbitals, trap and
+// interaction, e.g. every imaginary-time run from real orbitals) two
+// products do: Yr = Ar Wr^T, Yi = Ai Wr^T.  Warp cw takes the 8-row strips
+// cw, cw + 8, ... of the tile; per 4-deep k step one A fragment (real and
+// imaginary part in one 16-byte load) and, per 8-wide output tile, one W
+// fragment and three (two) MMAs.  Columns q >= P are zero (A side); outputs
+// p >= P are not stored.
+template <int M, bool REAL>
 __device__ __forceinline__ void pair_contract_mma(const double2* As, const double2* Ws, int cw,
                                                   int lane, uint32_t row0, uint32_t D2,
                                                   double2* __restrict__ Y) {
@@ -151,29 +154,43 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
             }
     }
     for (int st = cw; st < STRIPS; st += CW) {
-        double t1[NN][2], t2[NN][2], t3[NN][2];
+        double t1[NN][2], t2[NN][2], t3[REAL ? 1 : NN][2];
 #pragma unroll
         for (int n = 0; n < NN; n++)
 #pragma unroll
-            for (int j = 0; j < 2; j++) t1[n][j] = t2[n][j] = t3[n][j] = 0.0;
+            for (int j = 0; j < 2; j++) {
+                t1[n][j] = t2[n][j] = 0.0;
+                if constexpr (!REAL) t3[n][j] = 0.0;
+            }
         const double2* arow = As + S::row_at(st * 8 + lr);
 #pragma unroll
         for (int k = 0; k < NK; k++) {
             const int q = k * 4 + lk;
             const double2 a = q < P ? arow[q] : make_double2(0.0, 0.0);
-            const double as = a.x + a.y;
 #pragma unroll
             for (int n = 0; n < NN; n++) {
-                double2 w;
-                if constexpr (S::WREG) {
-                    w = wf[k][n];
+                if constexpr (REAL) {
+                    double w;
+                    if constexpr (S::WREG) {
+                        w = wf[k][n].x;
+                    } else {
+                        const int p = n * 8 + lr;
+                        w = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)].x;
+                    }
+                    dmma84(t1[n][0], t1[n][1], a.x, w);
+                    dmma84(t2[n][0], t2[n][1], a.y, w);
                 } else {
-                    const int p = n * 8 + lr;
-                    w = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)];
+                    double2 w;
+                    if constexpr (S::WREG) {
+                        w = wf[k][n];
+                    } else {
+                        const int p = n * 8 + lr;
+                        w = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)];
+                    }
+                    dmma84(t1[n][0], t1[n][1], a.x, w.x);
+                    dmma84(t2[n][0], t2[n][1], a.y, w.y);
+                    dmma84(t3[n][0], t3[n][1], a.x + a.y, w.x + w.y);
                 }
-                dmma84(t1[n][0], t1[n][1], a.x, w.x);
-                dmma84(t2[n][0], t2[n][1], a.y, w.y);
-                dmma84(t3[n][0], t3[n][1], as, w.x + w.y);
             }
         }
         const uint32_t m = row0 + st * 8 + lr;
@@ -183,7 +200,10 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     const int p = n * 8 + 2 * lk + j;
-                    if (p < P)
+                    if (p >= P) continue;
+                    if constexpr (REAL)
+                        Y[(size_t)p * D2 + m] = make_double2(t1[n][j], t2[n][j]);
+                    else
                         Y[(size_t)p * D2 + m] =
                             make_double2(t1[n][j] - t2[n][j], t3[n][j] - t1[n][j] - t2[n][j]);
                 }
@@ -191,11 +211,16 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
     }
 }
 
-// consumer thread t (0 .. CONSUMERS-1) of a tile whose first row is row0
+// consumer thread t (0 .. CONSUMERS-1) of a tile whose first row is row0;
+// `real`: the flag stored after the P x P entries of W
 template <int M>
 __device__ __forceinline__ void pair_consume(const double2* As, const double2* Ws, int t,
-                                             uint32_t row0, uint32_t D2, double2* __restrict__ Y) {
-    pair_contract_mma<M>(As, Ws, t >> 5, t & 31, row0, D2, Y);
+                                             uint32_t row0, uint32_t D2, double2* __restrict__ Y,
+                                             bool real) {
+    if (real)
+        pair_contract_mma<M, true>(As, Ws, t >> 5, t & 31, row0, D2, Y);
+    else
+        pair_contract_mma<M, false>(As, Ws, t >> 5, t & 31, row0, D2, Y);
 }
 
 // (HC)_row = sum over pairs P = {k <= s} present in the row of
@@ -285,6 +310,7 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
     const int pt = t - S::CONSUMERS;
     if (producer && blockIdx.x < ntiles) pair_gather<M>(sp, C, blockIdx.x, Ab, pt, S::PRODUCERS);
     __syncthreads();
+    const bool real = W[P * P].x != 0.0;
     int buf = 0;
     for (uint32_t tr = blockIdx.x; tr < ntiles; tr += gridDim.x, buf ^= 1) {
         if (producer) {
@@ -292,7 +318,7 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
             if (nx < ntiles)
                 pair_gather<M>(sp, C, nx, Ab + (size_t)(buf ^ 1) * ROWS * PS, pt, S::PRODUCERS);
         } else {
-            pair_consume<M>(Ab + (size_t)buf * ROWS * PS, Ws, t, tr * ROWS, sp.dim2, Y);
+            pair_consume<M>(Ab + (size_t)buf * ROWS * PS, Ws, t, tr * ROWS, sp.dim2, Y, real);
         }
         __syncthreads();
     }

@@ -81,7 +81,7 @@ int space_init(SpaceCtx& s, int N, int M) {
     if (hcp_eligible(N, M)) {
         const size_t P = (size_t)M * (M + 1) / 2;
         double2 *w = nullptr, *y = nullptr;
-        if (cudaMalloc(&w, P * P * sizeof(double2)) == cudaSuccess &&
+        if (cudaMalloc(&w, (P * P + 1) * sizeof(double2)) == cudaSuccess &&
             cudaMalloc(&y, hcp_scratch_bytes(N, M)) == cudaSuccess && hcp_prepare(M) == 0) {
             s.view.dim2 = (uint32_t)fock_dimension(N - 2, M);
             s.view.pair_w = w;

@@ -124,6 +124,31 @@ def test_hc_vs_oracle(gpu, oracle, N, M):
     assert rel_err(host(out), ref) < TOL
 
 
+@pytest.mark.parametrize("N,M", [(10, 4), (2, 2), (16, 5), (14, 6), (9, 7), (8, 8), (30, 6)])
+def test_hc_real_matrices_vs_oracle(gpu, oracle, N, M):
+    """real h and g (real orbitals): the contraction's two-product path,
+    complex coefficients"""
+    import torch
+
+    rng = np.random.default_rng(2000 + 37 * N + M)
+    sp = gpu.Space(N, M)
+    nc = sp.dim
+    h = rand_hob(rng, M).real.astype(np.complex128)
+    f = rng.normal(size=(M, 40))
+    t = np.einsum("x,ax,bx,cx,dx->abcd", rng.uniform(0.5, 1.5, 40), f, f, f, f)
+    g = np.ascontiguousarray(t.transpose(3, 2, 1, 0)).reshape(-1).astype(np.complex128)
+    c = rand_coef(rng, nc)
+    sp.set_matrices(dev(h), dev(g))
+    out = torch.empty(nc, dtype=torch.complex128, device="cuda")
+    sp.apply_hamiltonian(dev(c), out)
+    assert rel_err(host(out), oracle.apply_hamiltonian(N, M, c, h, g)) < TOL
+    # a complex g on the same space goes back to three products
+    g2 = g + 1e-3j * rng.normal(size=g.shape)
+    sp.set_matrices(dev(h), dev(g2))
+    sp.apply_hamiltonian(dev(c), out)
+    assert rel_err(host(out), oracle.apply_hamiltonian(N, M, c, h, g2)) < TOL
+
+
 def test_hc_dropin_vs_golden(gpu, gold):
     N, M = int(gold["npar"]), int(gold["norb"])
     D = gpu.DropIn()
