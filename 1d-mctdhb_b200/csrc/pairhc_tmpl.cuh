@@ -47,30 +47,47 @@ struct PairHcShape {
     static constexpr int ROWS = WIDE ? 256 : 128;
     static constexpr int PRODUCERS = ROWS;
     static constexpr int THREADS = CONSUMERS + PRODUCERS;
-    // Shared-memory strides in 16-byte words.  An 8-lane phase of a fragment
-    // load reads 4 consecutive words of 2 rows: with strides = 4 (mod 8)
-    // they fall in 8 different bank groups.  At 128 rows a row r starts at
-    // r * PS + ((r >> 1) & 3), so the 8 consecutive rows stored by 8
-    // producer lanes also fall in different bank groups; at 256 rows the
-    // tile takes an odd stride (conflict-free stores, two-way conflicts in
-    // the fragment loads) to fit two buffers in shared memory.
-    static constexpr int PS = WIDE ? (P | 1) : pair_stride4(P + 3);
+    // contraction depth: P rounded up to 4, in KB8 blocks of 8 and KB4 (0 or
+    // 1) block of 4 (mma.sync m16n8k8 / m16n8k4); 8-wide output tiles
+    static constexpr int KP = (P + 3) / 4 * 4;
+    static constexpr int KB8 = KP / 8;
+    static constexpr int KB4 = (KP % 8) / 4;
+    static constexpr int NN = (P + 7) / 8;
+    // output tiles per pass over a strip: two (three at 8 orbitals) keep
+    // the accumulators of the three products within the register budget
+    static constexpr int NG = NN <= 2 ? NN : (NN == 5 ? 3 : 2);
+    // Shared memory, in 16-byte words.  A row of the A tile takes PS = KP
+    // rounded up to 8 words, and element q of row r sits at
+    // r * PS + (q ^ swz(r)): the 8 rows stored by 8 consecutive producer
+    // lanes fall in 8 different bank groups, and so do the 8 lanes (rows g,
+    // g + 1, columns t = 0..3) of each phase of a fragment load.  W rows take
+    // WS = 4 (mod 8) words.
+    static constexpr int PS = (KP + 7) / 8 * 8;
     static constexpr int WS = pair_stride4(P);
     static constexpr size_t SMEM = (2 * (size_t)ROWS * PS + (size_t)P * WS) * sizeof(double2);
-    // tensor-core contraction: 8-wide output tiles, 4-deep k steps
-    static constexpr int NN = (P + 7) / 8;
-    static constexpr int NK = (P + 3) / 4;
-    __host__ __device__ static constexpr int row_at(int r) {
-        return WIDE ? r * PS : r * PS + ((r >> 1) & 3);
-    }
+    __host__ __device__ static constexpr int swz(int r) { return ((r & 1) << 2) | ((r >> 1) & 3); }
+    __host__ __device__ static constexpr int at(int r, int q) { return r * PS + (q ^ swz(r)); }
 };
 
-// FP64 mma.sync m8n8k4: D(8x8) += A(8x4) B(4x8); lane l holds A[l/4][l%4],
-// B[l%4][l/4] and D[l/4][2(l%4)], D[l/4][2(l%4)+1]
-__device__ __forceinline__ void dmma84(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
+// FP64 mma.sync m16n8k8: D(16x8) += A(16x8) B(8x8).  With g = lane / 4 and
+// t = lane % 4, lane l holds A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4];
+// B[t][g], B[t+4][g]; D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]
+__device__ __forceinline__ void dmma1688(double (&d)[4], double a0, double a1, double a2,
+                                         double a3, double b0, double b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+        "{%8, %9}, {%0, %1, %2, %3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
+// m16n8k4: lane l holds A[g][t], A[g+8][t]; B[t][g]; D as m16n8k8
+__device__ __forceinline__ void dmma1684(double (&d)[4], double a0, double a1, double b0) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, "
+        "{%0, %1, %2, %3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a0), "d"(a1), "d"(b0));
 }
 
 // W (P x P, global) staged into Ws[p * WS + q] by threads t, t + nt, ...
@@ -85,7 +102,7 @@ __device__ __forceinline__ void pair_stage_w(const double2* __restrict__ W, doub
 // building blocks (shared with the batched engine, batch_tmpl.cuh)
 // ---------------------------------------------------------------------------
 // Rows r = r0, r0 + rstep, ... < ROWS of tile `tr` of the (N-2)-boson space
-// into As[row_at(r) + p]: A_m(Q) = sqrt((m_q+1)(m_l+1+[q=l])) C[m + e_q + e_l].
+// into As[at(r, p)]: A_m(Q) = sqrt((m_q+1)(m_l+1+[q=l])) C[m + e_q + e_l].
 template <int M>
 __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* __restrict__ C,
                                             uint32_t tr, double2* As, int r0, int rstep) {
@@ -119,7 +136,7 @@ __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* 
                     f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
                 v = cscale(__ldg(C + j), f);
             }
-            As[S::row_at(r) + p] = v;
+            As[S::at(r, p)] = v;
         });
     }
 }
@@ -127,86 +144,118 @@ __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* 
 // Y_m(P) = sum_Q W[P][Q] A_m(Q) for a whole tile by the consumer warps on
 // the FP64 tensor cores, with three real products per complex product (Gauss):
 // T1 = Ar Wr^T, T2 = Ai Wi^T, T3 = (Ar + Ai)(Wr + Wi)^T, then Yr = T1 - T2,
-// Yi = T3 - T1 - T2.  When W is real (REAL: real orbitals, trap and
-// interaction, e.g. every imaginary-time run from real orbitals) two
-// products do: Yr = Ar Wr^T, Yi = Ai Wr^T.  Warp cw takes the 8-row strips
-// cw, cw + 8, ... of the tile; per 4-deep k step one A fragment (real and
-// imaginary part in one 16-byte load) and, per 8-wide output tile, one W
-// fragment and three (two) MMAs.  Columns q >= P are zero (A side); outputs
-// p >= P are not stored.
+// Yi = T3 - T1 - T2.  When W is real (REAL: real orbitals and coefficients)
+// two products do: Yr = Ar Wr^T, Yi = Ai Wr^T.  Warp cw takes the 16-row
+// strips cw, cw + 8, ... of the tile and, per pass over NG output tiles of
+// 8 pairs, runs m16n8k8 products over the depth (an m16n8k4 one for the
+// last 4 when P rounds to an odd number of 4s).  A fragments hold the real
+// and imaginary part of an element in one 16-byte load.  Columns q >= P
+// read as zero; outputs p >= P and rows m >= D2 are not stored.
 template <int M, bool REAL>
 __device__ __forceinline__ void pair_contract_mma(const double2* As, const double2* Ws, int cw,
                                                   int lane, uint32_t row0, uint32_t D2,
                                                   double2* __restrict__ Y) {
     using S = PairHcShape<M>;
-    constexpr int P = S::P, WS = S::WS, NN = S::NN, NK = S::NK;
-    constexpr int STRIPS = S::ROWS / 8, CW = S::CONSUMERS / 32;
-    const int lr = lane >> 2, lk = lane & 3;
-    // up to 5 orbitals the W fragments of the whole tile stay in registers
-    double2 wf[S::WREG ? NK : 1][S::WREG ? NN : 1];
+    constexpr int P = S::P, WS = S::WS, PS = S::PS, NN = S::NN, NG = S::NG;
+    constexpr int KB8 = S::KB8, KB4 = S::KB4, NPASS = (NN + NG - 1) / NG;
+    constexpr int STRIPS = S::ROWS / 16, CW = S::CONSUMERS / 32;
+    const int g = lane >> 2, t = lane & 3;
+    const int sw = S::swz(g);  // rows g and g + 8 of every strip
+    auto wat = [&](int p, int q) {
+        return (p < P && q < P) ? Ws[p * WS + q] : make_double2(0.0, 0.0);
+    };
+    // up to 5 orbitals the W fragments stay in registers: [k step][tile][2]
+    constexpr int KS = KB8 + KB4;
+    double2 wf[S::WREG ? KS : 1][S::WREG ? NN : 1][2];
     if constexpr (S::WREG) {
 #pragma unroll
-        for (int k = 0; k < NK; k++)
+        for (int k = 0; k < KS; k++)
 #pragma unroll
             for (int n = 0; n < NN; n++) {
-                const int p = n * 8 + lr, q = k * 4 + lk;
-                wf[k][n] = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)];
+                const int p = n * 8 + g, q = k * 8 + t;
+                wf[k][n][0] = wat(p, q);
+                wf[k][n][1] = k < KB8 ? wat(p, q + 4) : make_double2(0.0, 0.0);
             }
     }
     for (int st = cw; st < STRIPS; st += CW) {
-        double t1[NN][2], t2[NN][2], t3[REAL ? 1 : NN][2];
+        const double2* a_g = As + (size_t)(st * 16 + g) * PS;
+        const double2* a_h = a_g + 8 * PS;
+        const uint32_t m0 = row0 + st * 16 + g, m1 = m0 + 8;
+        auto aat = [&](const double2* row, int q) {
+            return q < P ? row[q ^ sw] : make_double2(0.0, 0.0);
+        };
 #pragma unroll
-        for (int n = 0; n < NN; n++)
+        for (int pass = 0; pass < NPASS; pass++) {
+            const int n0 = pass * NG;
+            double t1[NG][4], t2[NG][4], t3[REAL ? 1 : NG][4];
 #pragma unroll
-            for (int j = 0; j < 2; j++) {
-                t1[n][j] = t2[n][j] = 0.0;
-                if constexpr (!REAL) t3[n][j] = 0.0;
-            }
-        const double2* arow = As + S::row_at(st * 8 + lr);
+            for (int n = 0; n < NG; n++)
 #pragma unroll
-        for (int k = 0; k < NK; k++) {
-            const int q = k * 4 + lk;
-            const double2 a = q < P ? arow[q] : make_double2(0.0, 0.0);
+                for (int j = 0; j < 4; j++) {
+                    t1[n][j] = t2[n][j] = 0.0;
+                    if constexpr (!REAL) t3[n][j] = 0.0;
+                }
 #pragma unroll
-            for (int n = 0; n < NN; n++) {
-                if constexpr (REAL) {
-                    double w;
+            for (int k = 0; k < KS; k++) {
+                const bool deep = k < KB8;  // an 8-deep step (else the last 4)
+                const int q = k * 8 + t;
+                const double2 a0 = aat(a_g, q), a1 = aat(a_h, q);
+                const double2 a2 = deep ? aat(a_g, q + 4) : make_double2(0.0, 0.0);
+                const double2 a3 = deep ? aat(a_h, q + 4) : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int n = 0; n < NG; n++) {
+                    const int nt = n0 + n;
+                    if (nt >= NN) continue;
+                    double2 b0, b1;
                     if constexpr (S::WREG) {
-                        w = wf[k][n].x;
+                        b0 = wf[k][nt][0];
+                        b1 = wf[k][nt][1];
                     } else {
-                        const int p = n * 8 + lr;
-                        w = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)].x;
+                        const int p = nt * 8 + g;
+                        b0 = wat(p, q);
+                        b1 = deep ? wat(p, q + 4) : make_double2(0.0, 0.0);
                     }
-                    dmma84(t1[n][0], t1[n][1], a.x, w);
-                    dmma84(t2[n][0], t2[n][1], a.y, w);
-                } else {
-                    double2 w;
-                    if constexpr (S::WREG) {
-                        w = wf[k][n];
+                    if (deep) {
+                        dmma1688(t1[n], a0.x, a1.x, a2.x, a3.x, b0.x, b1.x);
+                        if constexpr (REAL) {
+                            dmma1688(t2[n], a0.y, a1.y, a2.y, a3.y, b0.x, b1.x);
+                        } else {
+                            dmma1688(t2[n], a0.y, a1.y, a2.y, a3.y, b0.y, b1.y);
+                            dmma1688(t3[n], a0.x + a0.y, a1.x + a1.y, a2.x + a2.y, a3.x + a3.y,
+                                     b0.x + b0.y, b1.x + b1.y);
+                        }
                     } else {
-                        const int p = n * 8 + lr;
-                        w = Ws[(p < P ? p : 0) * WS + (q < P ? q : 0)];
+                        dmma1684(t1[n], a0.x, a1.x, b0.x);
+                        if constexpr (REAL) {
+                            dmma1684(t2[n], a0.y, a1.y, b0.x);
+                        } else {
+                            dmma1684(t2[n], a0.y, a1.y, b0.y);
+                            dmma1684(t3[n], a0.x + a0.y, a1.x + a1.y, b0.x + b0.y);
+                        }
                     }
-                    dmma84(t1[n][0], t1[n][1], a.x, w.x);
-                    dmma84(t2[n][0], t2[n][1], a.y, w.y);
-                    dmma84(t3[n][0], t3[n][1], a.x + a.y, w.x + w.y);
                 }
             }
-        }
-        const uint32_t m = row0 + st * 8 + lr;
-        if (m < D2) {
 #pragma unroll
-            for (int n = 0; n < NN; n++)
+            for (int n = 0; n < NG; n++) {
+                const int nt = n0 + n;
+                if (nt >= NN) continue;
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
-                    const int p = n * 8 + 2 * lk + j;
+                    const int p = nt * 8 + 2 * t + j;
                     if (p >= P) continue;
-                    if constexpr (REAL)
-                        Y[(size_t)p * D2 + m] = make_double2(t1[n][j], t2[n][j]);
-                    else
-                        Y[(size_t)p * D2 + m] =
-                            make_double2(t1[n][j] - t2[n][j], t3[n][j] - t1[n][j] - t2[n][j]);
+                    double2 y0, y1;
+                    if constexpr (REAL) {
+                        y0 = make_double2(t1[n][j], t2[n][j]);
+                        y1 = make_double2(t1[n][j + 2], t2[n][j + 2]);
+                    } else {
+                        y0 = make_double2(t1[n][j] - t2[n][j], t3[n][j] - t1[n][j] - t2[n][j]);
+                        y1 = make_double2(t1[n][j + 2] - t2[n][j + 2],
+                                          t3[n][j + 2] - t1[n][j + 2] - t2[n][j + 2]);
+                    }
+                    if (m0 < D2) Y[(size_t)p * D2 + m0] = y0;
+                    if (m1 < D2) Y[(size_t)p * D2 + m1] = y1;
                 }
+            }
         }
     }
 }

@@ -427,8 +427,8 @@ def arena_bytes(mb, jobs, slack=1.02):
 
 def fp64_mma_peak(mb, torch, reps=5):
     """measured FP64 tensor-core throughput (TFLOP/s) of this GPU: the
-    library's mma.sync f64 probe, 4 blocks of 256 threads per SM, timed with
-    CUDA events; the best of `reps` launches"""
+    library's mma.sync m16n8k8 f64 probe, 4 blocks of 256 threads per SM,
+    timed with CUDA events; the best of `reps` launches"""
     blocks, iters = 4 * torch.cuda.get_device_properties(0).multi_processor_count, 2048
     out = torch.empty(blocks * 256, dtype=torch.float64, device="cuda")
     st = torch.cuda.current_stream()
@@ -441,7 +441,7 @@ def fp64_mma_peak(mb, torch, reps=5):
         c.record(st)
         torch.cuda.synchronize()
         best = min(best, a.elapsed_time(c))
-    return blocks * 8 * iters * 8 * 512 / (best / 1000.0) / 1e12
+    return blocks * 8 * iters * 4 * 2048 / (best / 1000.0) / 1e12
 
 
 def pair_work(jobs, M):

@@ -293,8 +293,8 @@ void*  mctdhb_batch_stream(mctdhb_batch b);       /* the engine's cudaStream_t *
 
 /* Throughput probe of the FP64 tensor cores (no counterpart in the
  * reference): `blocks` blocks of 256 threads, every warp running `iters`
- * rounds of eight independent mma.sync m8n8k4 f64 chains, i.e.
- * blocks * 8 * iters * 8 * 512 FLOPs; d_out receives blocks * 256 doubles.
+ * rounds of four independent mma.sync m16n8k8 f64 chains, i.e.
+ * blocks * 8 * iters * 4 * 2048 FLOPs; d_out receives blocks * 256 doubles.
  * The roofline denominator of the pair contraction. */
 int    mctdhb_fp64_mma_probe(int blocks, int iters, void* d_out, void* stream);
 
