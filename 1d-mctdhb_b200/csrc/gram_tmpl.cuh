@@ -143,6 +143,17 @@ __device__ __forceinline__ void gram_gather(const SpaceView& sp, uint32_t Dp,
         for (int x = 0; x < M; x++) n[x] = 0, U1[x] = 0u, U2[x] = 0u;
     }
     const uint32_t j0 = sp.dim - Dp + row;
+    // pairs: sqrt(n_x + 1), sqrt(n_x + 2) loaded once per orbital when a
+    // thread takes at least half of a row's pairs
+    constexpr bool HOIST = R == 2 && PARTS <= 2;
+    double s1[HOIST ? M : 1], s2[HOIST ? M : 1];
+    if constexpr (HOIST) {
+#pragma unroll
+        for (int x = 0; x < M; x++) {
+            s1[x] = __ldg(sp.sq + n[x] + 1);
+            s2[x] = __ldg(sp.sq + n[x] + 2);
+        }
+    }
     static_for<P>([&](auto pi) {
         constexpr int p = decltype(pi)::value;
         if (p % PARTS == part) {
@@ -155,7 +166,9 @@ __device__ __forceinline__ void gram_gather(const SpaceView& sp, uint32_t Dp,
                     constexpr int q = kPairs<M>.q[p], l = kPairs<M>.l[p];
                     const uint32_t j = j0 - (U1[q] - U1[l]) - U2[l];
                     double f;
-                    if constexpr (q == l)
+                    if constexpr (HOIST)
+                        f = q == l ? s1[q] * s2[q] : s1[q] * s1[l];
+                    else if constexpr (q == l)
                         f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[q] + 2);
                     else
                         f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);

@@ -123,17 +123,20 @@ __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* 
             for (int x = 0; x < M; x++) n[x] = 0, U1[x] = 0u, U2[x] = 0u;
         }
         const uint32_t j0 = jbase + row;
+        // sqrt(n_x + 1), sqrt(n_x + 2) once per orbital
+        double s1[M], s2[M];
+#pragma unroll
+        for (int x = 0; x < M; x++) {
+            s1[x] = __ldg(sp.sq + n[x] + 1);
+            s2[x] = __ldg(sp.sq + n[x] + 2);
+        }
         static_for<P>([&](auto pi) {
             constexpr int p = decltype(pi)::value;
             constexpr int q = kPairs<M>.q[p], l = kPairs<M>.l[p];
             double2 v = make_double2(0.0, 0.0);
             if (live) {
                 const uint32_t j = j0 - (U1[q] - U1[l]) - U2[l];
-                double f;
-                if constexpr (q == l)
-                    f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[q] + 2);
-                else
-                    f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
+                const double f = q == l ? s1[q] * s2[q] : s1[q] * s1[l];
                 v = cscale(__ldg(C + j), f);
             }
             As[S::at(r, p)] = v;
