@@ -142,10 +142,9 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
         set_error("mctdhb_propagate_step: incomplete MCTDHBDataStruct");
         return;
     }
-    if (mctdhb->orb_integ_method != FULLSTEP_RUNGEKUTTA || mctdhb->orb_der_method != FINITEDIFF) {
+    if (mctdhb->orb_integ_method != FULLSTEP_RUNGEKUTTA) {
         set_error("mctdhb_propagate_step: the GPU path integrates full-step Runge-Kutta orbitals "
-                  "with finite differences (got methods %d / %d)",
-                  (int)mctdhb->orb_integ_method, (int)mctdhb->orb_der_method);
+                  "(got method %d)", (int)mctdhb->orb_integ_method);
         return;
     }
     if (mctdhb->coef_integ_method != LANCZOS || !mctdhb->coef_workspace ||
@@ -190,9 +189,11 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
         mctdhb_solver_set_regularization(s, get_current_regularization_factor()))
         return;
     // the projector the reference's driver selected (orbital_integration.c:219-227)
+    // and the derivative method of the linear part (:137-176)
     if (mctdhb->orb_workspace &&
         mctdhb_solver_set_orthogonality(s, mctdhb->orb_workspace->impr_ortho ? 1 : 0))
         return;
+    if (mctdhb_solver_set_derivative(s, (int)mctdhb->orb_der_method)) return;
     cudaStream_t st = 0;
     if (mctdhb_solver_phase(s, 0, st)) return;
     // driver.c:175-177: time advances, trap and interaction follow in real time

@@ -4,8 +4,10 @@
 //                        as one (M^2 x G)(G x M^2) complex contraction on the
 //                        FP64 tensor cores (mma.sync m8n8k4 f64)
 //   orbital equation     dodt_fullstep_interface (orbital_integration.c:179-240)
-//                        with the finite-difference linear part
-//                        (split_linear_orbitals.c:210-255), the interacting
+//                        with the linear part of orbital_integration.c:137-176:
+//                        finite differences (split_linear_orbitals.c:210-255),
+//                        or the DVR matrix (:83-166) / spectral derivative
+//                        (:257-287) as one Toeplitz product, the interacting
 //                        part (split_nonlinear_orbitals.c:4-61) and the simple
 //                        projector (orbital_integration.c:95-131) or, once
 //                        the orbitals drift from orthonormality, the robust
@@ -20,6 +22,8 @@
 // an even number of points).
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <complex>
 #include <vector>
 
 #include "common.cuh"
@@ -107,16 +111,39 @@ __global__ void orb_q_kernel(int M, const double* __restrict__ g_dev,
     Q[e] = cscale(acc, *g_dev);
 }
 
-// H phi_k at every grid point: linear part (finite differences) plus the
-// interacting part sum_s conj(f_s) sum_{q,l} Q[k,s,q,l] f_q f_l
+// DVR / spectral linear part (orbital_integration.c:137-176):
+// L_k(x) = sum_j lin_t[j - x + n - 1] f_k(j) + V(x) f_k(x) on the n = G - 1
+// periodic points, L_k(n) = L_k(0).  Block (k, chunk) stages f_k in shared
+// memory; thread x sums over j, reading the kernel at consecutive addresses.
+__global__ void __launch_bounds__(256) orb_toeplitz_kernel(OrbView o, const double2* __restrict__ y,
+                                                           double2* __restrict__ L) {
+    extern __shared__ double2 fs[];  // n values
+    const int G = o.G, n = G - 1;
+    const int k = blockIdx.y;
+    const double2* f = y + (size_t)k * G;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) fs[j] = f[j];
+    __syncthreads();
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x > n) return;
+    const int xr = x == n ? 0 : x;
+    const double2* t = o.lin_t + (n - 1 - xr);
+    double2 acc = make_double2(0.0, 0.0);
+    for (int j = 0; j < n; j++) acc = cfma(__ldg(t + j), fs[j], acc);
+    L[(size_t)k * G + x] = cadd(acc, cscale(fs[xr], o.pot[xr]));
+}
+
+// H phi_k at every grid point: linear part (finite differences, or the
+// precomputed L of DVR / spectral derivatives) plus the interacting part
+// sum_s conj(f_s) sum_{q,l} Q[k,s,q,l] f_q f_l
 __global__ void orb_haction_kernel(OrbView o, const double2* __restrict__ y,
-                                   const double2* __restrict__ Q, double2* __restrict__ H) {
+                                   const double2* __restrict__ Q, const double2* __restrict__ L,
+                                   double2* __restrict__ H) {
     const int M = o.M, G = o.G;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= M * G) return;
     const int k = t / G, x = t % G;
     const double2* f = y + (size_t)k * G;
-    const double2 lin = linear_at(o, f, x);  // split_linear_orbitals.c:210-255
+    const double2 lin = L ? L[t] : linear_at(o, f, x);  // split_linear_orbitals.c:210-255
     // interacting part
     double2 fx[kMaxOrb];
     for (int a = 0; a < M; a++) fx[a] = y[(size_t)a * G + x];
@@ -284,6 +311,8 @@ void orb_release(OrbCtx& c) {
     cudaFree(c.d_work);
     cudaFree(c.d_S);
     cudaFree(c.d_fail);
+    cudaFree(c.d_lin_t);
+    cudaFree(c.d_L);
     c = OrbCtx();
 }
 
@@ -300,7 +329,14 @@ int orb_matrices(const OrbCtx& c, const double2* orb, double2* hob, double2* hin
 
 static int orb_rhs(const OrbCtx& c, const double2* y, double2* out, cudaStream_t st) {
     const int n = c.M * c.G;
-    orb_haction_kernel<<<(n + 127) / 128, 128, 0, st>>>(c.view, y, c.d_Q, c.d_H);
+    const double2* L = nullptr;
+    if (c.view.lin_t) {
+        const dim3 grid((c.G + 255) / 256, c.M);
+        orb_toeplitz_kernel<<<grid, 256, (size_t)(c.G - 1) * sizeof(double2), st>>>(c.view, y,
+                                                                                   c.d_L);
+        L = c.d_L;
+    }
+    orb_haction_kernel<<<(n + 127) / 128, 128, 0, st>>>(c.view, y, c.d_Q, L, c.d_H);
     orb_overlap_kernel<<<c.M * c.M, 256, 0, st>>>(c.view, y, c.d_H, c.d_P);
     if (c.robust) {
         orb_overlap_kernel<<<c.M * c.M, 256, 0, st>>>(c.view, y, y, c.d_S);
@@ -380,6 +416,96 @@ int orb_rhs_eval(const OrbCtx& c, const double2* rinv, const double2* rho2, cons
 int orb_periodic(const OrbCtx& c, double2* orb, cudaStream_t st) {
     periodic_kernel<<<1, 32, 0, st>>>(c.M, c.G, orb);
     MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// Toeplitz kernel of the DVR / spectral derivative part on n = G - 1 points,
+// t[d + n - 1] for d = j - i in (-n, n), with a2, a1 folded in.
+//   DVR (split_linear_orbitals.c:83-166): first and second derivatives in the
+//     exponential basis, kmom = k - n/2; for d > 0 the element is
+//     sum_k g(kmom) e^{2 pi i kmom d / n} / n, for d < 0 the conjugate
+//     (second derivative) or minus the conjugate (first), on the diagonal
+//     sum_k g(kmom) / n, with g1 = -2 pi i kmom / L, g2 = -(2 pi kmom / L)^2.
+//   spectral (split_linear_orbitals.c:257-287, calculus.c:272-285): the
+//     circulant of FFT -> (i freq a1 - freq^2 a2) -> inverse FFT with
+//     1/sqrt(n) both ways: t[d + n - 1] = c[(-d) mod n],
+//     c[e] = sum_m mult_m e^{2 pi i m e / n} / n.
+static std::vector<double2> derivative_toeplitz(int der, int G, double dx, double a2,
+                                                std::complex<double> a1) {
+    using cd = std::complex<double>;
+    const int n = G - 1;
+    const double pi = 3.14159265358979323846, len = n * dx;
+    // e^{2 pi i m / n}, m = 0 .. n-1
+    std::vector<cd> ex(n);
+    for (int m = 0; m < n; m++) ex[m] = std::polar(1.0, 2.0 * pi * m / n);
+    std::vector<double2> t(2 * (size_t)n - 1);
+    auto put = [&](int d, cd v) { t[d + n - 1] = make_double2(v.real(), v.imag()); };
+    if (der == kDerDVR) {
+        for (int d = 0; d < n; d++) {
+            cd s1 = 0.0, s2 = 0.0;
+            for (int k = 0; k < n; k++) {
+                const int kmom = k - n / 2;
+                const cd g1 = cd(0.0, -2.0 * pi * kmom / len);
+                const double g2 = -(2.0 * pi * kmom / len) * (2.0 * pi * kmom / len);
+                const long ph = (((long)kmom * d) % n + n) % n;
+                s1 += g1 * ex[ph] / (double)n;
+                s2 += g2 * ex[ph] / (double)n;
+            }
+            if (d == 0) {
+                put(0, a2 * s2 + a1 * s1);
+            } else {
+                put(d, a2 * s2 + a1 * s1);
+                put(-d, a2 * std::conj(s2) - a1 * std::conj(s1));
+            }
+        }
+    } else {
+        std::vector<cd> mult(n), c(n);
+        for (int m = 0; m < n; m++) {
+            const double freq = m <= (n - 1) / 2 ? 2.0 * pi * m / len : 2.0 * pi * (m - n) / len;
+            mult[m] = freq * cd(0.0, 1.0) * a1 - freq * freq * a2;
+        }
+        for (int e = 0; e < n; e++) {
+            cd z = 0.0;
+            for (int m = 0; m < n; m++) z += mult[m] * ex[((long)m * e) % n];
+            c[e] = z / (double)n;
+        }
+        for (int d = -(n - 1); d < n; d++) put(d, c[((-d) % n + n) % n]);
+    }
+    return t;
+}
+
+int orb_set_derivative(OrbCtx& c, int der) {
+    if (der == c.der) return 0;
+    if (der != kDerFiniteDiff && der != kDerDVR && der != kDerSpectral) {
+        set_error("orbital derivative method %d not in {300 DVR, 301 SPECTRAL, 302 FINITEDIFF}",
+                  der);
+        return -1;
+    }
+    if (der != kDerFiniteDiff && !c.view.periodic) {
+        set_error("DVR and spectral derivatives need periodic boundaries");
+        return -1;
+    }
+    if (der != kDerFiniteDiff && c.G - 1 > 8191) {
+        set_error("DVR / spectral derivatives: grid of %d points above 8192", c.G);
+        return -1;
+    }
+    cudaFree(c.d_lin_t);
+    cudaFree(c.d_L);
+    c.d_lin_t = c.d_L = nullptr;
+    c.view.lin_t = nullptr;
+    c.der = kDerFiniteDiff;
+    if (der == kDerFiniteDiff) return 0;
+    const std::vector<double2> t = derivative_toeplitz(
+        der, c.G, c.view.dx, c.view.a2, std::complex<double>(c.view.a1.x, c.view.a1.y));
+    MCTDHB_CUDA_TRY(cudaMalloc(&c.d_lin_t, t.size() * sizeof(double2)));
+    MCTDHB_CUDA_TRY(cudaMalloc(&c.d_L, (size_t)c.M * c.G * sizeof(double2)));
+    MCTDHB_CUDA_TRY(
+        cudaMemcpy(c.d_lin_t, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    MCTDHB_CUDA_TRY(cudaFuncSetAttribute(orb_toeplitz_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)((size_t)(c.G - 1) * sizeof(double2))));
+    c.view.lin_t = c.d_lin_t;
+    c.der = der;
     return 0;
 }
 

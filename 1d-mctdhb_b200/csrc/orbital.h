@@ -17,7 +17,14 @@ struct OrbView {
     double2 a1, tf;  // tf: time factor, 1 (real time) or -i (imaginary time)
     const double* w;
     const double* pot;
+    // DVR / spectral derivatives: Toeplitz kernel on the n = G - 1 periodic
+    // points, (D f)_i = sum_j lin_t[j - i + n - 1] f_j; null: finite
+    // differences
+    const double2* lin_t;
 };
+
+// derivative methods of the orbital equation (mctdhb_types.h OrbDerivative)
+constexpr int kDerDVR = 300, kDerSpectral = 301, kDerFiniteDiff = 302;
 
 struct OrbCtx {
     int M = 0, G = 0;
@@ -33,6 +40,9 @@ struct OrbCtx {
     double2* d_S = nullptr;        // orbital overlap matrix <f_s|f_l>
     int* d_fail = nullptr;         // set when the robust projector met a singular overlap
     int robust = 0;                // robust projector (orbital_integration.c:22-92)
+    int der = kDerFiniteDiff;      // derivative method of the linear part
+    double2* d_lin_t = nullptr;    // Toeplitz kernel of DVR / spectral derivatives
+    double2* d_L = nullptr;        // linear part of every orbital (DVR / spectral)
 };
 
 std::vector<double> simpson_weights(int n, double h);
@@ -46,6 +56,9 @@ int orb_rhs_eval(const OrbCtx& c, const double2* rinv, const double2* rho2, cons
 int orb_rk_step(const OrbCtx& c, int order, double dt, const double2* rinv, const double2* rho2,
                 const double2* y, double2* ynext, cudaStream_t st);
 int orb_periodic(const OrbCtx& c, double2* orb, cudaStream_t st);
+// derivative method: kDerFiniteDiff, or kDerDVR / kDerSpectral on a
+// periodic grid (the Toeplitz kernel is set up on the host)
+int orb_set_derivative(OrbCtx& c, int der);
 // S_sl = <f_s|f_l> (Simpson) into c.d_S
 int orb_overlap_matrix(const OrbCtx& c, const double2* orb, cudaStream_t st);
 int orb_orthonormalize(const OrbCtx& c, double2* orb, cudaStream_t st);

@@ -245,6 +245,21 @@ int mctdhb_solver_set_regularization(mctdhb_solver s, double reg_fac) {
     return 0;
 }
 
+// Derivative method of the orbital equation's linear part
+// (orbital_integration.c:137-176): 302 finite differences (the default),
+// 300 DVR, 301 spectral; the last two need periodic boundaries.
+int mctdhb_solver_set_derivative(mctdhb_solver s, int der_method) {
+    if (!s) {
+        set_error("mctdhb_solver_set_derivative: null solver");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (der_method == s->orb.der) return 0;
+    MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
+    drop_graphs(s);  // the linear part is part of the captured step
+    return orb_set_derivative(s->orb, der_method);
+}
+
 // The projector of the orbital equation: 0 the simple one, 1 the robust one
 // with the inverse overlap matrix (orbital_integration.c:22-131; the
 // reference switches when impr_ortho is set, driver.c:70-96).

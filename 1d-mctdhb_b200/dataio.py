@@ -365,8 +365,9 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
     <out_dir>/<prefix>_mctdhb_parameters.dat.
 
     `integrator`: the descriptor dict (read_integrator_descriptor); the GPU
-    solver runs FULLSTEP_RUNGEKUTTA orbitals with FINITEDIFF derivatives and
-    LANCZOS coefficients.  `monitor`: the dict of read_monitor_config.  Every
+    solver runs FULLSTEP_RUNGEKUTTA orbitals with DVR (the reference's
+    default), SPECTRAL or FINITEDIFF derivatives and LANCZOS coefficients.
+    `monitor`: the dict of read_monitor_config.  Every
     monitor_nsteps steps, in imaginary time with auto_check the run stops
     once E/N changed by less than 10^-digits relative and the eigen-residual
     is below eig_residue; in real time the robust projector is switched on
@@ -384,10 +385,10 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
 
     desc = dict(DEFAULT_INTEGRATOR, **(integrator or {}))
     mon = dict(DEFAULT_MONITOR, **(monitor or {}))
-    if desc["orb_method"] != FULLSTEP_RUNGEKUTTA or desc["der_method"] != FINITEDIFF or \
-            desc["coef_method"] != LANCZOS:
-        raise ValueError("the GPU solver runs FULLSTEP_RUNGEKUTTA orbitals with FINITEDIFF "
-                         "derivatives and LANCZOS coefficients")
+    if desc["orb_method"] != FULLSTEP_RUNGEKUTTA or desc["coef_method"] != LANCZOS or \
+            desc["der_method"] not in (DVR, SPECTRAL, FINITEDIFF):
+        raise ValueError("the GPU solver runs FULLSTEP_RUNGEKUTTA orbitals (DVR, SPECTRAL or "
+                         "FINITEDIFF derivatives) and LANCZOS coefficients")
     imag = desc["integ_type"] == IMAGTIME
     rec_n, mon_n = mon["rec_nsteps"], mon["monitor_nsteps"]
     os.makedirs(out_dir, exist_ok=True)
@@ -405,6 +406,7 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
                       desc["rk_order"], desc["lanczos_iter"], d2coef=job.d2coef,
                       d1coef=job.d1coef, periodic=desc["bounds"] == PERIODIC_BOUNDS)
         try:
+            s.set_derivative(desc["der_method"])
             if mon["reg_factor"] is not None:
                 s.set_regularization(mon["reg_factor"])
             pot = builtin_potential(job.pot_func, 0.0, x, job.pot_params)

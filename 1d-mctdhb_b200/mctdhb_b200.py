@@ -53,7 +53,7 @@ EXPORTED = [
     "mctdhb_solver_get", "mctdhb_solver_put", "mctdhb_solver_energy",
     "mctdhb_solver_device_coef", "mctdhb_solver_device_orbitals", "mctdhb_solver_time",
     "mctdhb_solver_set_orthogonality", "mctdhb_solver_overlap_residual",
-    "mctdhb_solver_eig_residual", "mctdhb_solver_lowest_state",
+    "mctdhb_solver_eig_residual", "mctdhb_solver_lowest_state", "mctdhb_solver_set_derivative",
 ]
 
 _lib = None
@@ -175,6 +175,8 @@ def load(path=LIB_PATH):
     L.mctdhb_solver_energy.argtypes = [vp, C.POINTER(d)]
     L.mctdhb_solver_set_orthogonality.restype = i
     L.mctdhb_solver_set_orthogonality.argtypes = [vp, i]
+    L.mctdhb_solver_set_derivative.restype = i
+    L.mctdhb_solver_set_derivative.argtypes = [vp, i]
     L.mctdhb_solver_overlap_residual.restype = i
     L.mctdhb_solver_overlap_residual.argtypes = [vp, C.POINTER(d)]
     L.mctdhb_solver_eig_residual.restype = i
@@ -402,6 +404,12 @@ class Solver:
     def set_regularization(self, reg_fac):
         _check(load().mctdhb_solver_set_regularization(self.h, reg_fac),
                "mctdhb_solver_set_regularization")
+
+    def set_derivative(self, der_method):
+        """linear part of the orbital equation: 302 finite differences,
+        300 DVR, 301 spectral"""
+        _check(load().mctdhb_solver_set_derivative(self.h, int(der_method)),
+               "mctdhb_solver_set_derivative")
 
     def set_orthogonality(self, robust):
         """projector of the orbital equation: False simple, True robust"""

@@ -205,6 +205,12 @@ int  mctdhb_solver_energy(mctdhb_solver s, double* e_re_im); /* Tr(rho1 h) + rho
  *                      current orbitals (lowest_state_lanczos,
  *                      include/linalg/multiconfig_lanczos.h); densities kept */
 int  mctdhb_solver_set_orthogonality(mctdhb_solver s, int robust);
+/* Derivative method of the orbital equation's linear part, as the
+ * reference's orb_der_method (src/integrator/orbital_integration.c:137-176):
+ * 302 FINITEDIFF (default), 300 DVR (the matrix of
+ * src/integrator/split_linear_orbitals.c:83-166), 301 SPECTRAL (:257-287).
+ * DVR and SPECTRAL need periodic boundaries and at most 8192 grid points. */
+int  mctdhb_solver_set_derivative(mctdhb_solver s, int der_method);
 int  mctdhb_solver_overlap_residual(mctdhb_solver s, double* res);
 int  mctdhb_solver_eig_residual(mctdhb_solver s, double e, double* res);
 int  mctdhb_solver_lowest_state(mctdhb_solver s, int niter, double* e);

@@ -1476,6 +1476,100 @@ linear_fd(int G, double dx, double a2, ocplx a1, int periodic, const double* pot
     }
 }
 
+/* The DVR matrix of split_linear_orbitals.c:83-166 on the n = G - 1
+ * periodic points (row-major n x n): first and second derivatives in the
+ * exponential basis, kmom = k - n/2, each element summed over k in order,
+ * with d1coef / d2coef applied as there. */
+static ocplx*
+dvr_matrix(int n, double dx, double a2, ocplx a1)
+{
+    const double pi = 3.14159265358979323846, length = n * dx;
+    ocplx*       d1 = malloc(sizeof(ocplx) * n * n);
+    ocplx*       d2 = malloc(sizeof(ocplx) * n * n);
+    ocplx*       out = malloc(sizeof(ocplx) * n * n);
+    for (int i = 0; i < n; i++)
+    {
+        for (int j = i + 1; j < n; j++)
+        {
+            ocplx s1 = 0, s2 = 0;
+            for (int k = 0; k < n; k++)
+            {
+                const int    kmom = k - n / 2;
+                const ocplx  e = cexp(2 * I * kmom * (j - i) * pi / n);
+                const ocplx  g1 = -(2 * I * pi * kmom / length);
+                const double g2 = -(2 * pi * kmom / length) * (2 * pi * kmom / length);
+                s1 += g1 * e / n;
+                s2 += g2 * e / n;
+            }
+            d1[i * n + j] = s1;
+            d1[j * n + i] = -conj(s1);
+            d2[i * n + j] = s2;
+            d2[j * n + i] = conj(s2);
+        }
+        ocplx s1 = 0, s2 = 0;
+        for (int k = 0; k < n; k++)
+        {
+            const int kmom = k - n / 2;
+            s1 = s1 + (-(2 * I * pi * kmom / length)) / n;
+            s2 = s2 + (-(2 * pi * kmom / length) * (2 * pi * kmom / length)) / n;
+        }
+        d1[i * n + i] = s1;
+        d2[i * n + i] = s2;
+    }
+    for (int i = 0; i < n * n; i++) out[i] = a2 * d2[i] + a1 * d1[i];
+    free(d1);
+    free(d2);
+    return out;
+}
+
+/* linear part a2 f'' + a1 f' + V f (orbital_integration.c:137-176):
+ * der = 302 finite differences (split_linear_orbitals.c:210-255); 300 the
+ * DVR matrix; 301 spectral (split_linear_orbitals.c:257-287): forward DFT
+ * with 1/sqrt(n) scaling, multiplication by freq i d1coef - freq^2 d2coef
+ * (calculus.c:272-285), backward DFT with 1/sqrt(n), restated here as the
+ * direct transform sums.  The last point repeats the first. */
+static void
+linear_part(int der, int G, double dx, double a2, ocplx a1, int periodic,
+            const double* pot, const ocplx* dvr, const ocplx* f, ocplx* out)
+{
+    const int n = G - 1;
+    if (der == 300)
+    {
+        for (int i = 0; i < n; i++)
+        {
+            ocplx z = 0;
+            for (int j = 0; j < n; j++) z += dvr[i * n + j] * f[j];
+            out[i] = z + pot[i] * f[i];
+        }
+        out[n] = out[0];
+    }
+    else if (der == 301)
+    {
+        const double pi = 3.14159265358979323846, sc = 1.0 / sqrt((double) n);
+        ocplx*       F = malloc(sizeof(ocplx) * n);
+        for (int k = 0; k < n; k++)
+        {
+            ocplx z = 0;
+            for (int x = 0; x < n; x++)
+                z += f[x] * cexp(-2 * I * pi * (double) (((long) k * x) % n) / n);
+            const double freq = k <= (n - 1) / 2 ? 2 * pi * k / (n * dx)
+                                                 : 2 * pi * (k - n) / (n * dx);
+            F[k] = z * sc * (freq * I * a1 - freq * freq * a2);
+        }
+        for (int x = 0; x < n; x++)
+        {
+            ocplx z = 0;
+            for (int k = 0; k < n; k++)
+                z += F[k] * cexp(2 * I * pi * (double) (((long) k * x) % n) / n);
+            out[x] = z * sc + pot[x] * f[x];
+        }
+        out[n] = out[0];
+        free(F);
+    }
+    else
+        linear_fd(G, dx, a2, a1, periodic, pot, f, out);
+}
+
 /* orbital_integration.c:179-240 (FINITEDIFF).  robust = 0: the simple
  * projector (:95-131), P_k = sum_s f_s <f_s|H f_k>; robust = 1: the robust
  * projector (:22-92), P_k = sum_{s,l} f_s (S^-1)_{sl} <f_l|H f_k> with the
@@ -1488,14 +1582,16 @@ int
 orc_orbital_rhs(int M, int G, double dx, double a2, ocplx a1, double g,
                 int periodic, ocplx time_fac, const double* pot,
                 const ocplx* rinv, const ocplx* rho2, const ocplx* orb,
-                ocplx* dodt, int robust)
+                ocplx* dodt, int robust, int der)
 {
     ocplx* lin = malloc(sizeof(ocplx) * M * G);
     ocplx* ha = malloc(sizeof(ocplx) * M * G);
     ocplx* po = malloc(sizeof(ocplx) * M * M);
     ocplx* w = malloc(sizeof(ocplx) * G);
+    ocplx* dvr = der == 300 ? dvr_matrix(G - 1, dx, a2, a1) : NULL;
     for (int k = 0; k < M; k++)
-        linear_fd(G, dx, a2, a1, periodic, pot, orb + k * G, lin + k * G);
+        linear_part(der, G, dx, a2, a1, periodic, pot, dvr, orb + k * G, lin + k * G);
+    free(dvr);
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < M; k++)
         for (int j = 0; j < G; j++)
@@ -1544,7 +1640,7 @@ orc_orbital_rhs(int M, int G, double dx, double a2, ocplx a1, double g,
 
 typedef struct
 {
-    int           M, G, periodic, robust;
+    int           M, G, periodic, robust, der;
     double        dx, a2, g;
     ocplx         a1, tf;
     const double* pot;
@@ -1555,7 +1651,7 @@ static void
 rhs_eval(const rhs_args* a, const ocplx* y, ocplx* out)
 {
     orc_orbital_rhs(a->M, a->G, a->dx, a->a2, a->a1, a->g, a->periodic, a->tf,
-                    a->pot, a->rinv, a->rho2, y, out, a->robust);
+                    a->pot, a->rinv, a->rho2, y, out, a->robust, a->der);
 }
 
 /* the named tableaux of shim/odesys.h (Heun, classical RK4, Butcher RK5) */
@@ -1617,12 +1713,12 @@ orc_propagate_step(int npar, int M, int G, double dx, double dt, double a2,
                    ocplx a1, double g, int periodic, int imagtime, int rk_order,
                    int lanczos_m, double reg_fac, const double* pot, ocplx* orb,
                    ocplx* coef, ocplx* hob, ocplx* hint, ocplx* rho1,
-                   ocplx* rho2, ocplx* rinv, int robust)
+                   ocplx* rho2, ocplx* rinv, int robust, int der)
 {
     int      n = M * G;
     ocplx    tf = imagtime ? -I : 1.0;
     ocplx    prop_dt = imagtime ? -I * dt : dt;
-    rhs_args a = {M, G, periodic, robust, dx, a2, g, a1, tf, pot, rinv, rho2};
+    rhs_args a = {M, G, periodic, robust, der, dx, a2, g, a1, tf, pot, rinv, rho2};
     if (periodic)
         for (int k = 0; k < M; k++) orb[k * G + G - 1] = orb[k * G];
     ocplx* next = malloc(sizeof(ocplx) * n);

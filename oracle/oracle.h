@@ -109,24 +109,26 @@ int orc_herm_inverse(int n, const ocplx* a, ocplx* inv);
 void orc_sync_density_matrices(int npar, int norb, const ocplx* coef,
                                double reg_fac, ocplx* rho1, ocplx* rho2,
                                ocplx* rho1_inv);
-/* orbital_integration.c:179-240 with FINITEDIFF linear part
- * (split_linear_orbitals.c:210-255), orb_interacting_part
- * (split_nonlinear_orbitals.c:4-61) and the simple projector (:95-131), or
- * with robust != 0 the robust projector (:22-92).  Returns 0, or the
- * overlap inversion's error code. */
+/* orbital_integration.c:179-240 with the linear part of der = 302
+ * FINITEDIFF (split_linear_orbitals.c:210-255), 300 DVR (the matrix of
+ * split_linear_orbitals.c:83-166) or 301 SPECTRAL (:257-287),
+ * orb_interacting_part (split_nonlinear_orbitals.c:4-61) and the simple
+ * projector (:95-131), or with robust != 0 the robust projector (:22-92).
+ * Returns 0, or the overlap inversion's error code. */
 int orc_orbital_rhs(int norb, int npts, double dx, double d2coef,
                     ocplx d1coef, double g, int periodic, ocplx time_fac,
                     const double* pot, const ocplx* rho1_inv,
                     const ocplx* rho2, const ocplx* orb, ocplx* dodt,
-                    int robust);
+                    int robust, int der);
 /* one full step of driver.c:159-201 (FULLSTEP_RUNGEKUTTA + LANCZOS, FD,
  * time-independent trap and interaction).  rk_order in {2,4,5} with the
- * named tableaux of shim/odesys.h; robust selects the projector as in
- * orc_orbital_rhs.  State arrays are updated in place. */
+ * named tableaux of shim/odesys.h; robust and der select the projector
+ * and the linear part as in orc_orbital_rhs.  State arrays are updated in
+ * place. */
 void orc_propagate_step(int npar, int norb, int npts, double dx, double dt,
                         double d2coef, ocplx d1coef, double g, int periodic,
                         int imagtime, int rk_order, int lanczos_m,
                         double reg_fac, const double* pot, ocplx* orb,
                         ocplx* coef, ocplx* hob, ocplx* hint, ocplx* rho1,
-                        ocplx* rho2, ocplx* rho1_inv, int robust);
+                        ocplx* rho2, ocplx* rho1_inv, int robust, int der);
 #endif

@@ -94,10 +94,11 @@ class Oracle:
         L.orc_sync_density_matrices.argtypes = [i, i, _c128p, C.c_double, _c128p, _c128p, _c128p]
         L.orc_orbital_rhs.restype = i
         L.orc_orbital_rhs.argtypes = [i, i, C.c_double, C.c_double, _C128, C.c_double, i, _C128,
-                                      _f64p, _c128p, _c128p, _c128p, _c128p, i]
+                                      _f64p, _c128p, _c128p, _c128p, _c128p, i, i]
         L.orc_propagate_step.argtypes = [i, i, i, C.c_double, C.c_double, C.c_double, _C128,
                                          C.c_double, i, i, i, i, C.c_double, _f64p,
-                                         _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, i]
+                                         _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, i,
+                                         i]
 
     # ---- space -------------------------------------------------------
     def dim(self, N, M):
@@ -259,19 +260,20 @@ class Oracle:
         return r1.reshape(M, M), r2, ri.reshape(M, M)
 
     def orbital_rhs(self, orb, dx, d2coef, d1coef, g, periodic, time_fac, pot, rinv, rho2,
-                    robust=False):
+                    robust=False, der=302):
+        """der: 302 finite differences, 300 DVR, 301 spectral"""
         M, G = orb.shape
         out = np.zeros(M * G, np.complex128)
         info = self.lib.orc_orbital_rhs(M, G, dx, d2coef, _c(d1coef), g, int(periodic),
                                         _c(time_fac), np.ascontiguousarray(pot, np.float64),
                                         cvec(rinv).reshape(-1), cvec(rho2).reshape(-1),
-                                        cvec(orb).reshape(-1), out, int(robust))
+                                        cvec(orb).reshape(-1), out, int(robust), int(der))
         if info:
             raise ValueError(f"singular overlap matrix (column {info - 1})")
         return out.reshape(M, G)
 
     def propagate_step(self, st, N, dx, dt, d2coef, d1coef, g, periodic, imagtime, rk_order,
-                       lanczos_m, pot, reg_fac=1e-9, robust=False):
+                       lanczos_m, pot, reg_fac=1e-9, robust=False, der=302):
         """One full step; `st` is a dict of numpy arrays updated in place:
         orb (M,G), coef, hob (M,M), hint, rho1 (M,M), rho2, rinv (M,M)."""
         M, G = st["orb"].shape
@@ -281,7 +283,7 @@ class Oracle:
         self.lib.orc_propagate_step(N, M, G, dx, dt, d2coef, _c(d1coef), g, int(periodic),
                                     int(imagtime), rk_order, lanczos_m, reg_fac,
                                     np.ascontiguousarray(pot, np.float64),
-                                    *[a.reshape(-1) for a in args], int(robust))
+                                    *[a.reshape(-1) for a in args], int(robust), int(der))
 
 
 class Reference:
@@ -382,10 +384,11 @@ class Reference:
         return C.cast(getattr(self.lib, name), C.c_void_p).value
 
     def make_mctdhb(self, N, M, G, xi, xf, imagtime, rk_order, lanczos_m, dt, omega, g,
-                    periodic=True, omega_f=None, pot_period=0.0, g_f=None, g_period=0.0):
+                    periodic=True, omega_f=None, pot_period=0.0, g_f=None, g_period=0.0,
+                    der=T.FINITEDIFF):
         """A reference MCTDHBDataStruct from its own constructor
-        (types_definition.c:247): FULLSTEP_RUNGEKUTTA orbitals, FINITEDIFF
-        derivatives, LANCZOS coefficients, harmonic trap
+        (types_definition.c:247): FULLSTEP_RUNGEKUTTA orbitals, `der`
+        derivatives (FINITEDIFF by default), LANCZOS coefficients, harmonic trap
         (builtin_potential.c:37) swept omega -> omega_f over pot_period and
         g ramped g -> g_f over g_period (builtin_time_parameter.c:7); constant
         by default.  Returns (struct pointer, keep-alive list)."""
@@ -395,7 +398,7 @@ class Reference:
         g_args = (C.c_double * 5)(g, g if g_f is None else g_f, g_period, 0.0, 0.0)
         ms = L.get_mctdhb_struct(
             T.IMAGTIME if imagtime else T.REALTIME, T.LANCZOS, T.FULLSTEP_RUNGEKUTTA,
-            T.FINITEDIFF, rk_order, lanczos_m, N, M, b"harmonic",
+            der, rk_order, lanczos_m, N, M, b"harmonic",
             T.PERIODIC_BOUNDS if periodic else T.ZERO_BOUNDS, xi, xf, G, dt, 1.0, -0.5,
             T.dcomplex(0.0, 0.0), C.cast(pot_args, C.c_void_p), C.cast(g_args, C.c_void_p),
             self.fn("potfunc_harmonic"), self.fn("timeparam_linear_ramp"))

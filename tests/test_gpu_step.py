@@ -104,6 +104,72 @@ def test_solver_vs_oracle(gpu, oracle, N, M, G, imag, rk, m, dt, g, steps):
     s.close()
 
 
+@pytest.mark.parametrize("der,imag,G,d1", [(300, True, 64, 0.0), (300, False, 128, 0.0),
+                                           (301, False, 96, 0.0), (301, True, 64, 0.0),
+                                           (300, False, 64, 0.2), (301, False, 64, 0.2)])
+def test_solver_dvr_spectral_vs_oracle(gpu, oracle, der, imag, G, d1):
+    """DVR (300) and spectral (301) derivatives of the orbital equation
+    (orbital_integration.c:137-176): the device Toeplitz product against the
+    oracle's DVR matrix / direct DFT, with and without a first-derivative
+    term (where the two methods differ in its sign)"""
+    N, M, m, dt, g, steps = 5, 3, 5, 0.005, 0.4, 4
+    xi, xf = -8.0, 8.0
+    orb, dx = hermite_orbitals(M, G, xi, xf)
+    coef = rand_coef(np.random.default_rng(G + der), oracle.dim(N, M))
+    pot = harmonic(G, xi, xf)
+    s = gpu.Solver(N, M, G, xi, xf, dt, imag, 5, m, d1coef=1j * d1)
+    s.set_derivative(der)
+    s.set_potential(pot)
+    s.set_interaction(g)
+    s.set_state(orb, coef)
+    st = oracle_init(oracle, N, orb, coef, dx, pot, g)
+    st["hob"] = np.ascontiguousarray(oracle.orbital_hob(orb, dx, -0.5, 1j * d1, pot))
+    for _ in range(steps):
+        oracle.propagate_step(st, N, dx, dt, -0.5, 1j * d1, g, True, imag, 5, m, pot, der=der)
+    s.step(steps)
+    d = s.get()
+    assert rel_err(d["orb"], st["orb"]) < 1e-10
+    assert rel_err(d["coef"], st["coef"]) < 1e-10
+    assert rel_err(d["rho1"], st["rho1"]) < 1e-10
+    # back to finite differences on the same solver
+    s.set_derivative(302)
+    oracle.propagate_step(st, N, dx, dt, -0.5, 1j * d1, g, True, imag, 5, m, pot)
+    s.step(1)
+    assert rel_err(s.get()["orb"], st["orb"]) < 1e-10
+    s.close()
+
+
+@pytest.mark.parametrize("imag", [True, False])
+def test_dropin_dvr_step_vs_reference(gpu, reference, imag):
+    """structs with the reference's default derivative method (DVR) stepped
+    by the reference and by the GPU drop-in"""
+    import mctdhb_types as T
+
+    N, M, G, m, dt, g = 5, 3, 64, 5, 0.005, 0.5
+    xi, xf = -8.0, 8.0
+    orb, _ = hermite_orbitals(M, G, xi, xf)
+    coef = rand_coef(np.random.default_rng(7), reference.lib.space_dimension(N, M))
+    A, ka = reference.make_mctdhb(N, M, G, xi, xf, imag, 5, m, dt, 1.0, g, der=T.DVR)
+    B, kb = reference.make_mctdhb(N, M, G, xi, xf, imag, 5, m, dt, 1.0, g, der=T.DVR)
+    try:
+        reference.set_state(A, orb, coef)
+        reference.set_state(B, orb, coef)
+        L = gpu.load()
+        for k in range(3):
+            reference.step(A, k)
+            ow = np.zeros(M * G, np.complex128)
+            cw = np.zeros(len(coef), np.complex128)
+            L.mctdhb_gpu_clear_error()
+            L.mctdhb_propagate_step(B, T.carray(ow), T.carray(cw), k)
+            assert gpu.last_error() == "", gpu.last_error()
+        a, b = reference.get_state(A), reference.get_state(B)
+        for key in ("orb", "coef", "rho1", "rho2"):
+            assert rel_err(b[key], a[key]) < 1e-10, key
+    finally:
+        reference.destroy_mctdhb(A)
+        reference.destroy_mctdhb(B)
+
+
 @pytest.mark.parametrize("side_stream", [False, True])
 def test_solver_energy_follows_steps_on_any_stream(gpu, oracle, side_stream):
     """energy() read right after step() -- no other synchronisation -- is the

@@ -121,3 +121,57 @@ def test_robust_projector_oracle(oracle):
     # the Hermite functions are orthonormal under the Simpson rule to 1e-15
     assert rel_err(oracle.orbital_rhs(orb, *args, robust=True), oracle.orbital_rhs(orb, *args)) \
         < 1e-12
+
+
+@pytest.mark.parametrize("imag,der", [(True, 300), (False, 300)])
+def test_dvr_step_oracle_vs_reference(oracle, reference, imag, der):
+    """full steps with the DVR derivative matrix (split_linear_orbitals.c:
+    83-166; the reference's default derivative method) against the
+    reference's own mctdhb_propagate_step"""
+    N, M, G, rk, m, dt, g = 4, 3, 64, 5, 5, 0.005, 0.5
+    xi, xf = -8.0, 8.0
+    ms, keep = reference.make_mctdhb(N, M, G, xi, xf, imag, rk, m, dt, 1.0, g, der=der)
+    try:
+        orb, dx = hermite_orbitals(M, G, xi, xf)
+        coef = rand_coef(np.random.default_rng(21), oracle.dim(N, M))
+        reference.set_state(ms, orb, coef)
+        st = oracle_state(reference.get_state(ms), coef)
+        pot = reference.get_state(ms)["pot"]
+        for k in range(3):
+            reference.step(ms, k)
+            oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, imag, rk, m, pot, der=der)
+        rs = reference.get_state(ms)
+        assert rel_err(st["orb"], rs["orb"]) < 1e-10
+        assert rel_err(st["coef"], rs["coef"]) < 1e-10
+        assert rel_err(st["rho1"], rs["rho1"]) < 1e-10
+    finally:
+        reference.destroy_mctdhb(ms)
+
+
+def test_spectral_linear_part_oracle_vs_numpy_fft(oracle):
+    """the spectral linear part (split_linear_orbitals.c:257-287, MKL DFT
+    with 1/sqrt(n) both ways) against numpy's FFT; with d1coef = 0 the DVR
+    matrix is the same operator"""
+    M, G, xi, xf = 3, 64, -8.0, 8.0
+    orb, dx = hermite_orbitals(M, G, xi, xf)
+    rng = np.random.default_rng(8)
+    f = orb + 0.1 * (rng.normal(size=orb.shape) + 1j * rng.normal(size=orb.shape))
+    f[:, -1] = f[:, 0]
+    pot = 0.5 * np.linspace(xi, xf, G) ** 2
+    rinv = np.eye(M, dtype=np.complex128)
+    rho2 = np.zeros(M ** 4, np.complex128)
+    n = G - 1
+    k = np.arange(n)
+    freq = np.where(k <= (n - 1) // 2, 2 * np.pi * k / (n * dx), 2 * np.pi * (k - n) / (n * dx))
+    for a1 in (0.0, 0.3):
+        mult = freq * 1j * a1 - freq ** 2 * (-0.5)
+        lin = np.fft.ifft(np.fft.fft(f[:, :n], axis=1) * mult, axis=1) + pot[:n] * f[:, :n]
+        lin = np.concatenate([lin, lin[:, :1]], axis=1)
+        proj = np.array([[oracle.simpson(dx, np.conj(f[s]) * lin[kk]) for kk in range(M)]
+                         for s in range(M)])
+        want = -1j * (lin - np.einsum("sx,sk->kx", f, proj))
+        got = oracle.orbital_rhs(f, dx, -0.5, a1, 0.0, True, 1.0, pot, rinv, rho2, der=301)
+        assert rel_err(got, want) < 1e-12, a1
+    dvr = oracle.orbital_rhs(f, dx, -0.5, 0.0, 0.0, True, 1.0, pot, rinv, rho2, der=300)
+    spec = oracle.orbital_rhs(f, dx, -0.5, 0.0, 0.0, True, 1.0, pot, rinv, rho2, der=301)
+    assert rel_err(dvr, spec) < 1e-12
