@@ -147,16 +147,20 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
                   "(got method %d)", (int)mctdhb->orb_integ_method);
         return;
     }
-    if (mctdhb->coef_integ_method != LANCZOS || !mctdhb->coef_workspace ||
-        !mctdhb->coef_workspace->lan_work) {
-        set_error("mctdhb_propagate_step: the GPU path propagates coefficients by SIL (LANCZOS)");
+    const bool sil = mctdhb->coef_integ_method == LANCZOS;
+    if ((!sil && mctdhb->coef_integ_method != RUNGEKUTTA) ||
+        (sil && (!mctdhb->coef_workspace || !mctdhb->coef_workspace->lan_work))) {
+        set_error("mctdhb_propagate_step: coefficients by LANCZOS (with its workspace) or "
+                  "RUNGEKUTTA (got %d)", (int)mctdhb->coef_integ_method);
         return;
     }
+    // Lanczos dimension of the SIL step (unused by Runge-Kutta coefficients)
+    const int lz = sil ? (int)mctdhb->coef_workspace->lan_work->iter : 5;
     ManyBodyState psi = mctdhb->state;
     OrbitalEquation eq = mctdhb->orb_eq;
     const int N = psi->npar, M = psi->norb, G = psi->grid_size;
     StepKey key{N, M, G, eq->bounds == PERIODIC_BOUNDS, mctdhb->integ_type == IMAGTIME,
-                (int)mctdhb->rk_order, (int)mctdhb->coef_workspace->lan_work->iter, eq->xi, eq->xf,
+                (int)mctdhb->rk_order, lz, eq->xi, eq->xf,
                 eq->d2coef, std::real(eq->d1coef), std::imag(eq->d1coef), eq->tstep};
     StepCtx* c;
     {
@@ -193,7 +197,9 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
     if (mctdhb->orb_workspace &&
         mctdhb_solver_set_orthogonality(s, mctdhb->orb_workspace->impr_ortho ? 1 : 0))
         return;
-    if (mctdhb_solver_set_derivative(s, (int)mctdhb->orb_der_method)) return;
+    if (mctdhb_solver_set_derivative(s, (int)mctdhb->orb_der_method) ||
+        mctdhb_solver_set_coef_method(s, (int)mctdhb->coef_integ_method))
+        return;
     cudaStream_t st = 0;
     if (mctdhb_solver_phase(s, 0, st)) return;
     // driver.c:175-177: time advances, trap and interaction follow in real time
@@ -228,7 +234,7 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
             set_error("mctdhb_propagate_step: copy of the coefficients failed");
             return;
         }
-        if (mctdhb->integ_type == IMAGTIME) {  // the combination before renormalisation
+        if (mctdhb->integ_type == IMAGTIME) {  // the step's result before renormalisation
             double nrm2 = 1.0;
             if (sil_norm2(mctdhb_solver_space(s)->lw, &nrm2)) return;
             const double scale = std::sqrt(nrm2);

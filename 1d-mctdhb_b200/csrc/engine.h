@@ -52,7 +52,13 @@ int lanczos_fetch(const LanczosWork& w, int m, int* iters, double2* diag, double
 // renormalised in imaginary time.
 int sil_step(const SpaceCtx& s, LanczosWork& w, double2* d_C, int m, double2 prop_dt,
              int imagtime, cudaStream_t st);
-// |C|^2 of the last imaginary-time SIL step before its renormalisation
+// One Runge-Kutta step of C (device, in/out) with dC/dt = -i tf H C
+// (coefficients_integration.c:15-57), renormalised in imaginary time; the
+// workspace needs 7 vectors.
+int coef_rk_step(const SpaceCtx& s, LanczosWork& w, double2* d_C, int order, double dt,
+                 int imagtime, cudaStream_t st);
+// |C|^2 of the last imaginary-time SIL (or coefficient RK) step before its
+// renormalisation
 int sil_norm2(const LanczosWork& w, double* out);
 // Lowest Ritz pair of an m-step Lanczos started from C (in/out); the Ritz
 // value is written to *d_energy (device).

@@ -18,6 +18,8 @@
 // fixed-order (per-block partials, then one ordered pass), so results are
 // reproducible bit for bit.
 #include <algorithm>
+#include <initializer_list>
+#include <utility>
 
 #include "common.cuh"
 #include "engine.h"
@@ -369,6 +371,93 @@ int sil_step(const SpaceCtx& s, LanczosWork& w, double2* d_C, int m, double2 pro
                                       nullptr);
     lz_combine_kernel<<<w.vec_grid, 256, 0, st>>>(w.V, n, w.scal, w.iflag, d_C);
     MCTDHB_CUDA_TRY(cudaGetLastError());
+    if (imagtime) {
+        norm2_kernel<<<w.vec_grid, 256, 0, st>>>(d_C, n, w.part);
+        if (reduce_rows(w.part, 1, w.vec_grid, w.scal + S_MISC + 3, st)) return -1;
+        renorm_kernel<<<w.vec_grid, 256, 0, st>>>(d_C, n, w.scal + S_MISC + 3);
+        MCTDHB_CUDA_TRY(cudaGetLastError());
+    }
+    return 0;
+}
+
+// out = y + sum_j c_j V_j (complex c_j), up to 6 terms
+struct CoefCombo {
+    double2 c[6];
+    int n;
+};
+__global__ void coef_combo_kernel(const double2* __restrict__ y, const double2* __restrict__ V,
+                                  uint32_t n, CoefCombo cb, double2* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double2 acc = y[i];
+        for (int j = 0; j < cb.n; j++) acc = cfma(cb.c[j], V[(size_t)j * n + i], acc);
+        out[i] = acc;
+    }
+}
+
+// One Runge-Kutta step of the coefficients (coefficients_integration.c:15-57):
+// dC/dt = -i tf H C with the named tableaux (classical RK4, Butcher's RK5;
+// order 2 takes the RK5 tableau as there, :44-47).  Stage H.C products go to
+// V[0..5], the stage input to V[6]; in imaginary time C is renormalised and
+// |C|^2 before it kept for sil_norm2.
+int coef_rk_step(const SpaceCtx& s, LanczosWork& w, double2* d_C, int order, double dt,
+                 int imagtime, cudaStream_t st) {
+    const uint32_t n = s.dim;
+    if (w.mmax < 7) {
+        set_error("coef_rk_step: workspace of %d vectors, 7 needed", w.mmax);
+        return -1;
+    }
+    double2* V = w.V;
+    double2* tmp = w.V + (size_t)6 * n;
+    // -i tf dt: tf = 1 (real time) or -i (imaginary time)
+    const double2 f = imagtime ? make_double2(-dt, 0.0) : make_double2(0.0, -dt);
+    HcEpilogue ep;
+    auto H = [&](const double2* in, int j) {
+        return hc_apply(s.view, in, V + (size_t)j * n, s.d_tab, ep, st);
+    };
+    auto combo = [&](std::initializer_list<std::pair<int, double>> t, double2* out) {
+        CoefCombo cb{};
+        cb.n = 0;
+        for (auto& p : t) {
+            // terms j index V rows in order 0..n-1; absent rows get weight 0
+            while (cb.n < p.first) cb.c[cb.n++] = make_double2(0.0, 0.0);
+            cb.c[cb.n++] = make_double2(f.x * p.second, f.y * p.second);
+        }
+        coef_combo_kernel<<<w.vec_grid, 256, 0, st>>>(d_C, V, n, cb, out);
+        return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    };
+    int rc = 0;
+    if (order == 4) {
+        rc |= H(d_C, 0);
+        rc |= combo({{0, 0.5}}, tmp);
+        rc |= H(tmp, 1);
+        rc |= combo({{1, 0.5}}, tmp);
+        rc |= H(tmp, 2);
+        rc |= combo({{2, 1.0}}, tmp);
+        rc |= H(tmp, 3);
+        rc |= combo({{0, 1.0 / 6}, {1, 2.0 / 6}, {2, 2.0 / 6}, {3, 1.0 / 6}}, d_C);
+    } else if (order == 5 || order == 2) {
+        rc |= H(d_C, 0);
+        rc |= combo({{0, 0.25}}, tmp);
+        rc |= H(tmp, 1);
+        rc |= combo({{0, 0.125}, {1, 0.125}}, tmp);
+        rc |= H(tmp, 2);
+        rc |= combo({{1, -0.5}, {2, 1.0}}, tmp);
+        rc |= H(tmp, 3);
+        rc |= combo({{0, 3.0 / 16}, {3, 9.0 / 16}}, tmp);
+        rc |= H(tmp, 4);
+        rc |= combo({{0, -3.0 / 7}, {1, 2.0 / 7}, {2, 12.0 / 7}, {3, -12.0 / 7}, {4, 8.0 / 7}},
+                    tmp);
+        rc |= H(tmp, 5);
+        rc |= combo({{0, 7.0 / 90}, {2, 32.0 / 90}, {3, 12.0 / 90}, {4, 32.0 / 90}, {5, 7.0 / 90}},
+                    d_C);
+    } else {
+        set_error("coefficient Runge-Kutta order %d not in {2, 4, 5}", order);
+        return -1;
+    }
+    if (rc) {
+        set_error("coef_rk_step: launch failed");
+        return -1;
+    }
     if (imagtime) {
         norm2_kernel<<<w.vec_grid, 256, 0, st>>>(d_C, n, w.part);
         if (reduce_rows(w.part, 1, w.vec_grid, w.scal + S_MISC + 3, st)) return -1;

@@ -25,6 +25,7 @@ struct mctdhb_solver_s {
     mctdhb_space sp = nullptr;
     OrbCtx orb;
     int N = 0, M = 0, G = 0, imagtime = 0, rk_order = 5, lanczos_m = 5;
+    int coef_method = 20;  // 20 LANCZOS (SIL), 21 RUNGEKUTTA
     double dt = 0.0, reg_fac = 1e-9, t = 0.0;
     double2 *d_orb = nullptr, *d_orb_next = nullptr, *d_coef = nullptr, *d_hob = nullptr,
             *d_hint = nullptr, *d_rho1 = nullptr, *d_rho2 = nullptr, *d_rinv = nullptr,
@@ -67,8 +68,13 @@ int phase_coefficients(mctdhb_solver_s* s, cudaStream_t st) {
     if (s->M == 1) return 0;  // Gross-Pitaevskii: the coefficient is trivial
     SpaceCtx& sc = s->sp->sp;
     if (hc_prep(sc.view, s->d_hob, s->d_hint, sc.d_tab, st)) return -1;
-    const double2 pdt = s->imagtime ? make_double2(0.0, -s->dt) : make_double2(s->dt, 0.0);
-    if (sil_step(sc, s->sp->lw, s->d_coef, s->lanczos_m, pdt, s->imagtime, st)) return -1;
+    if (s->coef_method == 21) {
+        if (coef_rk_step(sc, s->sp->lw, s->d_coef, s->rk_order, s->dt, s->imagtime, st))
+            return -1;
+    } else {
+        const double2 pdt = s->imagtime ? make_double2(0.0, -s->dt) : make_double2(s->dt, 0.0);
+        if (sil_step(sc, s->sp->lw, s->d_coef, s->lanczos_m, pdt, s->imagtime, st)) return -1;
+    }
     if (dens_apply(sc.view, s->d_coef, sc.d_dens_part, s->d_rho1, s->d_rho2, sc.d_dens_desc, st))
         return -1;
     return orb_sync_rho1(o, s->d_rho1, s->d_rinv, s->reg_fac, s->d_info, st);
@@ -242,6 +248,22 @@ int mctdhb_solver_set_regularization(mctdhb_solver s, double reg_fac) {
     if (reg_fac == s->reg_fac) return 0;
     s->reg_fac = reg_fac;
     drop_graphs(s);  // the factor is a launch argument: capture again
+    return 0;
+}
+
+// Coefficient integrator (driver.c:190-198): 20 LANCZOS (short iterative
+// Lanczos, the default) or 21 RUNGEKUTTA (coefficients_integration.c:29-57,
+// the solver's Runge-Kutta order).
+int mctdhb_solver_set_coef_method(mctdhb_solver s, int coef_method) {
+    if (!s || (coef_method != 20 && coef_method != 21)) {
+        set_error("mctdhb_solver_set_coef_method: method not in {20 LANCZOS, 21 RUNGEKUTTA}");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (coef_method == s->coef_method) return 0;
+    MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
+    drop_graphs(s);
+    s->coef_method = coef_method;
     return 0;
 }
 

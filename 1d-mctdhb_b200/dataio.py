@@ -366,7 +366,8 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
 
     `integrator`: the descriptor dict (read_integrator_descriptor); the GPU
     solver runs FULLSTEP_RUNGEKUTTA orbitals with DVR (the reference's
-    default), SPECTRAL or FINITEDIFF derivatives and LANCZOS coefficients.
+    default), SPECTRAL or FINITEDIFF derivatives and LANCZOS or RUNGEKUTTA
+    coefficients.
     `monitor`: the dict of read_monitor_config.  Every
     monitor_nsteps steps, in imaginary time with auto_check the run stops
     once E/N changed by less than 10^-digits relative and the eigen-residual
@@ -385,10 +386,11 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
 
     desc = dict(DEFAULT_INTEGRATOR, **(integrator or {}))
     mon = dict(DEFAULT_MONITOR, **(monitor or {}))
-    if desc["orb_method"] != FULLSTEP_RUNGEKUTTA or desc["coef_method"] != LANCZOS or \
+    if desc["orb_method"] != FULLSTEP_RUNGEKUTTA or \
+            desc["coef_method"] not in (LANCZOS, RUNGEKUTTA) or \
             desc["der_method"] not in (DVR, SPECTRAL, FINITEDIFF):
         raise ValueError("the GPU solver runs FULLSTEP_RUNGEKUTTA orbitals (DVR, SPECTRAL or "
-                         "FINITEDIFF derivatives) and LANCZOS coefficients")
+                         "FINITEDIFF derivatives) and LANCZOS or RUNGEKUTTA coefficients")
     imag = desc["integ_type"] == IMAGTIME
     rec_n, mon_n = mon["rec_nsteps"], mon["monitor_nsteps"]
     os.makedirs(out_dir, exist_ok=True)
@@ -407,6 +409,7 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
                       d1coef=job.d1coef, periodic=desc["bounds"] == PERIODIC_BOUNDS)
         try:
             s.set_derivative(desc["der_method"])
+            s.set_coef_method(desc["coef_method"])
             if mon["reg_factor"] is not None:
                 s.set_regularization(mon["reg_factor"])
             pot = builtin_potential(job.pot_func, 0.0, x, job.pot_params)

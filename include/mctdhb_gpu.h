@@ -211,6 +211,11 @@ int  mctdhb_solver_set_orthogonality(mctdhb_solver s, int robust);
  * src/integrator/split_linear_orbitals.c:83-166), 301 SPECTRAL (:257-287).
  * DVR and SPECTRAL need periodic boundaries and at most 8192 grid points. */
 int  mctdhb_solver_set_derivative(mctdhb_solver s, int der_method);
+/* Coefficient integrator, as the reference's coef_integ_method
+ * (src/integrator/driver.c:190-198): 20 LANCZOS (default), 21 RUNGEKUTTA
+ * (src/integrator/coefficients_integration.c:29-57, the solver's order;
+ * order 2 takes the RK5 tableau as the reference does). */
+int  mctdhb_solver_set_coef_method(mctdhb_solver s, int coef_method);
 int  mctdhb_solver_overlap_residual(mctdhb_solver s, double* res);
 int  mctdhb_solver_eig_residual(mctdhb_solver s, double e, double* res);
 int  mctdhb_solver_lowest_state(mctdhb_solver s, int niter, double* e);

@@ -1707,13 +1707,78 @@ rk_step(int order, const rhs_args* a, int n, double dt, const ocplx* y,
     free(w);
 }
 
+/* coefficients_integration.c:15-57: dC/dt = -i tf H C by the named tableaux
+ * (classical RK4; Butcher's RK5, which order 2 also takes there, :44-47),
+ * then the imaginary-time renormalisation */
+static void
+coef_rk(int npar, int M, const ocplx* hob, const ocplx* hint, int order,
+        double dt, int imagtime, ocplx* coef)
+{
+    const uint64_t nc = orc_space_dimension(npar, M);
+    const ocplx    tf = imagtime ? -I : 1.0;
+    ocplx*         k[6];
+    for (int i = 0; i < 6; i++) k[i] = malloc(sizeof(ocplx) * nc);
+    ocplx* w = malloc(sizeof(ocplx) * nc);
+#define DCDT(in, out)                                           \
+    do                                                          \
+    {                                                           \
+        orc_apply_hamiltonian(npar, M, in, hob, hint, out);     \
+        for (uint64_t i = 0; i < nc; i++) out[i] *= -I * tf;    \
+    } while (0)
+    if (order == 4)
+    {
+        DCDT(coef, k[0]);
+        for (uint64_t i = 0; i < nc; i++) w[i] = coef[i] + 0.5 * dt * k[0][i];
+        DCDT(w, k[1]);
+        for (uint64_t i = 0; i < nc; i++) w[i] = coef[i] + 0.5 * dt * k[1][i];
+        DCDT(w, k[2]);
+        for (uint64_t i = 0; i < nc; i++) w[i] = coef[i] + dt * k[2][i];
+        DCDT(w, k[3]);
+        for (uint64_t i = 0; i < nc; i++)
+            coef[i] += dt / 6.0 * (k[0][i] + 2.0 * k[1][i] + 2.0 * k[2][i] + k[3][i]);
+    }
+    else
+    {
+        DCDT(coef, k[0]);
+        for (uint64_t i = 0; i < nc; i++) w[i] = coef[i] + dt * (0.25 * k[0][i]);
+        DCDT(w, k[1]);
+        for (uint64_t i = 0; i < nc; i++)
+            w[i] = coef[i] + dt * (0.125 * k[0][i] + 0.125 * k[1][i]);
+        DCDT(w, k[2]);
+        for (uint64_t i = 0; i < nc; i++) w[i] = coef[i] + dt * (-0.5 * k[1][i] + k[2][i]);
+        DCDT(w, k[3]);
+        for (uint64_t i = 0; i < nc; i++)
+            w[i] = coef[i] + dt * ((3.0 / 16.0) * k[0][i] + (9.0 / 16.0) * k[3][i]);
+        DCDT(w, k[4]);
+        for (uint64_t i = 0; i < nc; i++)
+            w[i] = coef[i] + dt * ((-3.0 / 7.0) * k[0][i] + (2.0 / 7.0) * k[1][i] +
+                                   (12.0 / 7.0) * k[2][i] - (12.0 / 7.0) * k[3][i] +
+                                   (8.0 / 7.0) * k[4][i]);
+        DCDT(w, k[5]);
+        for (uint64_t i = 0; i < nc; i++)
+            coef[i] += dt * ((7.0 / 90.0) * k[0][i] + (32.0 / 90.0) * k[2][i] +
+                             (12.0 / 90.0) * k[3][i] + (32.0 / 90.0) * k[4][i] +
+                             (7.0 / 90.0) * k[5][i]);
+    }
+#undef DCDT
+    if (imagtime)
+    {
+        double n2 = 0;
+        for (uint64_t i = 0; i < nc; i++) n2 += creal(coef[i] * conj(coef[i]));
+        const double r = 1.0 / sqrt(n2);
+        for (uint64_t i = 0; i < nc; i++) coef[i] *= r;
+    }
+    for (int i = 0; i < 6; i++) free(k[i]);
+    free(w);
+}
+
 /* driver.c:159-201 with orbital_integration.c:284-349 */
 void
 orc_propagate_step(int npar, int M, int G, double dx, double dt, double a2,
                    ocplx a1, double g, int periodic, int imagtime, int rk_order,
                    int lanczos_m, double reg_fac, const double* pot, ocplx* orb,
                    ocplx* coef, ocplx* hob, ocplx* hint, ocplx* rho1,
-                   ocplx* rho2, ocplx* rinv, int robust, int der)
+                   ocplx* rho2, ocplx* rinv, int robust, int der, int coef_method)
 {
     int      n = M * G;
     ocplx    tf = imagtime ? -I : 1.0;
@@ -1731,9 +1796,14 @@ orc_propagate_step(int npar, int M, int G, double dx, double dt, double a2,
     orc_orbital_hob(M, G, dx, a2, a1, pot, orb, hob);
     orc_orbital_hint(M, G, dx, g, orb, hint);
     if (M == 1) return;
-    uint64_t nc = orc_space_dimension(npar, M);
-    ocplx*   lw = malloc(sizeof(ocplx) * nc * lanczos_m);
-    orc_sil_step(npar, M, hob, hint, lanczos_m, prop_dt, imagtime, coef, lw);
-    free(lw);
+    if (coef_method == 21)
+        coef_rk(npar, M, hob, hint, rk_order, dt, imagtime, coef);
+    else
+    {
+        uint64_t nc = orc_space_dimension(npar, M);
+        ocplx*   lw = malloc(sizeof(ocplx) * nc * lanczos_m);
+        orc_sil_step(npar, M, hob, hint, lanczos_m, prop_dt, imagtime, coef, lw);
+        free(lw);
+    }
     orc_sync_density_matrices(npar, M, coef, reg_fac, rho1, rho2, rinv);
 }

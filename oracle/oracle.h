@@ -123,12 +123,14 @@ int orc_orbital_rhs(int norb, int npts, double dx, double d2coef,
 /* one full step of driver.c:159-201 (FULLSTEP_RUNGEKUTTA + LANCZOS, FD,
  * time-independent trap and interaction).  rk_order in {2,4,5} with the
  * named tableaux of shim/odesys.h; robust and der select the projector
- * and the linear part as in orc_orbital_rhs.  State arrays are updated in
- * place. */
+ * and the linear part as in orc_orbital_rhs; coef_method 20 (SIL) or 21
+ * (Runge-Kutta, coefficients_integration.c:15-57).  State arrays are updated
+ * in place. */
 void orc_propagate_step(int npar, int norb, int npts, double dx, double dt,
                         double d2coef, ocplx d1coef, double g, int periodic,
                         int imagtime, int rk_order, int lanczos_m,
                         double reg_fac, const double* pot, ocplx* orb,
                         ocplx* coef, ocplx* hob, ocplx* hint, ocplx* rho1,
-                        ocplx* rho2, ocplx* rho1_inv, int robust, int der);
+                        ocplx* rho2, ocplx* rho1_inv, int robust, int der,
+                        int coef_method);
 #endif

@@ -98,7 +98,7 @@ class Oracle:
         L.orc_propagate_step.argtypes = [i, i, i, C.c_double, C.c_double, C.c_double, _C128,
                                          C.c_double, i, i, i, i, C.c_double, _f64p,
                                          _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, i,
-                                         i]
+                                         i, i]
 
     # ---- space -------------------------------------------------------
     def dim(self, N, M):
@@ -273,7 +273,7 @@ class Oracle:
         return out.reshape(M, G)
 
     def propagate_step(self, st, N, dx, dt, d2coef, d1coef, g, periodic, imagtime, rk_order,
-                       lanczos_m, pot, reg_fac=1e-9, robust=False, der=302):
+                       lanczos_m, pot, reg_fac=1e-9, robust=False, der=302, coef_method=20):
         """One full step; `st` is a dict of numpy arrays updated in place:
         orb (M,G), coef, hob (M,M), hint, rho1 (M,M), rho2, rinv (M,M)."""
         M, G = st["orb"].shape
@@ -283,7 +283,8 @@ class Oracle:
         self.lib.orc_propagate_step(N, M, G, dx, dt, d2coef, _c(d1coef), g, int(periodic),
                                     int(imagtime), rk_order, lanczos_m, reg_fac,
                                     np.ascontiguousarray(pot, np.float64),
-                                    *[a.reshape(-1) for a in args], int(robust), int(der))
+                                    *[a.reshape(-1) for a in args], int(robust), int(der),
+                                    int(coef_method))
 
 
 class Reference:
@@ -385,7 +386,7 @@ class Reference:
 
     def make_mctdhb(self, N, M, G, xi, xf, imagtime, rk_order, lanczos_m, dt, omega, g,
                     periodic=True, omega_f=None, pot_period=0.0, g_f=None, g_period=0.0,
-                    der=T.FINITEDIFF):
+                    der=T.FINITEDIFF, coef=T.LANCZOS):
         """A reference MCTDHBDataStruct from its own constructor
         (types_definition.c:247): FULLSTEP_RUNGEKUTTA orbitals, `der`
         derivatives (FINITEDIFF by default), LANCZOS coefficients, harmonic trap
@@ -397,7 +398,7 @@ class Reference:
                                     0.0, 0.0)
         g_args = (C.c_double * 5)(g, g if g_f is None else g_f, g_period, 0.0, 0.0)
         ms = L.get_mctdhb_struct(
-            T.IMAGTIME if imagtime else T.REALTIME, T.LANCZOS, T.FULLSTEP_RUNGEKUTTA,
+            T.IMAGTIME if imagtime else T.REALTIME, coef, T.FULLSTEP_RUNGEKUTTA,
             der, rk_order, lanczos_m, N, M, b"harmonic",
             T.PERIODIC_BOUNDS if periodic else T.ZERO_BOUNDS, xi, xf, G, dt, 1.0, -0.5,
             T.dcomplex(0.0, 0.0), C.cast(pot_args, C.c_void_p), C.cast(g_args, C.c_void_p),

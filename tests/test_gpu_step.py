@@ -139,18 +139,51 @@ def test_solver_dvr_spectral_vs_oracle(gpu, oracle, der, imag, G, d1):
     s.close()
 
 
-@pytest.mark.parametrize("imag", [True, False])
-def test_dropin_dvr_step_vs_reference(gpu, reference, imag):
-    """structs with the reference's default derivative method (DVR) stepped
-    by the reference and by the GPU drop-in"""
+@pytest.mark.parametrize("imag,rk", [(True, 4), (False, 5), (False, 2)])
+def test_solver_coef_rk_vs_oracle(gpu, oracle, imag, rk):
+    """Runge-Kutta coefficients (coefficients_integration.c:29-57) on the
+    device: stage H.C products on the pair kernels"""
+    N, M, G, m, dt, g, steps = 6, 4, 96, 5, 0.002, 0.7, 3
+    xi, xf = -8.0, 8.0
+    orb, dx = hermite_orbitals(M, G, xi, xf)
+    coef = rand_coef(np.random.default_rng(40 + rk), oracle.dim(N, M))
+    pot = harmonic(G, xi, xf)
+    s = gpu.Solver(N, M, G, xi, xf, dt, imag, rk, m)
+    s.set_coef_method(21)
+    s.set_potential(pot)
+    s.set_interaction(g)
+    s.set_state(orb, coef)
+    st = oracle_init(oracle, N, orb, coef, dx, pot, g)
+    for _ in range(steps):
+        oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, imag, rk, m, pot, coef_method=21)
+    s.step(steps)
+    d = s.get()
+    assert rel_err(d["orb"], st["orb"]) < 1e-10
+    assert rel_err(d["coef"], st["coef"]) < 1e-10
+    assert rel_err(d["rho1"], st["rho1"]) < 1e-10
+    if imag:
+        assert abs(np.linalg.norm(d["coef"]) - 1.0) < 1e-12
+    s.close()
+
+
+@pytest.mark.parametrize("imag,der,coef", [(True, 300, 20), (False, 300, 20), (True, 302, 21),
+                                           (False, 301, 21)])
+def test_dropin_methods_step_vs_reference(gpu, reference, imag, der, coef):
+    """structs with the reference's default derivative method (DVR) or
+    Runge-Kutta coefficients, stepped by the reference and by the GPU
+    drop-in (the spectral case checks the drop-in only: the reference's
+    FFT is not available here)"""
     import mctdhb_types as T
 
-    N, M, G, m, dt, g = 5, 3, 64, 5, 0.005, 0.5
+    N, M, G, m, dt, g = 5, 3, 64, 5, 0.002, 0.5
     xi, xf = -8.0, 8.0
     orb, _ = hermite_orbitals(M, G, xi, xf)
-    coef = rand_coef(np.random.default_rng(7), reference.lib.space_dimension(N, M))
-    A, ka = reference.make_mctdhb(N, M, G, xi, xf, imag, 5, m, dt, 1.0, g, der=T.DVR)
-    B, kb = reference.make_mctdhb(N, M, G, xi, xf, imag, 5, m, dt, 1.0, g, der=T.DVR)
+    coef0 = rand_coef(np.random.default_rng(7), reference.lib.space_dimension(N, M))
+    ref_der = 300 if der == 301 else der  # the reference runs the spectral case as DVR
+    A, ka = reference.make_mctdhb(N, M, G, xi, xf, imag, 5, m, dt, 1.0, g, der=ref_der,
+                                  coef=coef)
+    B, kb = reference.make_mctdhb(N, M, G, xi, xf, imag, 5, m, dt, 1.0, g, der=der, coef=coef)
+    coef = coef0
     try:
         reference.set_state(A, orb, coef)
         reference.set_state(B, orb, coef)
@@ -163,6 +196,7 @@ def test_dropin_dvr_step_vs_reference(gpu, reference, imag):
             L.mctdhb_propagate_step(B, T.carray(ow), T.carray(cw), k)
             assert gpu.last_error() == "", gpu.last_error()
         a, b = reference.get_state(A), reference.get_state(B)
+        # spectral and DVR are one operator when d1coef = 0 (rounding apart)
         for key in ("orb", "coef", "rho1", "rho2"):
             assert rel_err(b[key], a[key]) < 1e-10, key
     finally:

@@ -175,3 +175,30 @@ def test_spectral_linear_part_oracle_vs_numpy_fft(oracle):
     dvr = oracle.orbital_rhs(f, dx, -0.5, 0.0, 0.0, True, 1.0, pot, rinv, rho2, der=300)
     spec = oracle.orbital_rhs(f, dx, -0.5, 0.0, 0.0, True, 1.0, pot, rinv, rho2, der=301)
     assert rel_err(dvr, spec) < 1e-12
+
+
+@pytest.mark.parametrize("imag,rk", [(True, 4), (False, 5), (False, 2)])
+def test_coef_rk_step_oracle_vs_reference(oracle, reference, imag, rk):
+    """full steps with Runge-Kutta coefficients (coefficients_integration.c:
+    29-57; order 2 runs the RK5 tableau there) against the reference's step"""
+    import mctdhb_types as T
+
+    N, M, G, m, dt, g = 4, 3, 64, 5, 0.002, 0.5
+    xi, xf = -8.0, 8.0
+    ms, keep = reference.make_mctdhb(N, M, G, xi, xf, imag, rk, m, dt, 1.0, g, coef=T.RUNGEKUTTA)
+    try:
+        orb, dx = hermite_orbitals(M, G, xi, xf)
+        coef = rand_coef(np.random.default_rng(31 + rk), oracle.dim(N, M))
+        reference.set_state(ms, orb, coef)
+        r0 = reference.get_state(ms)
+        st = oracle_state(r0, coef)
+        for k in range(3):
+            reference.step(ms, k)
+            oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, imag, rk, m, r0["pot"],
+                                  coef_method=21)
+        rs = reference.get_state(ms)
+        assert rel_err(st["orb"], rs["orb"]) < 1e-10
+        assert rel_err(st["coef"], rs["coef"]) < 1e-10
+        assert rel_err(st["rho1"], rs["rho1"]) < 1e-10
+    finally:
+        reference.destroy_mctdhb(ms)
