@@ -1638,18 +1638,206 @@ orc_orbital_rhs(int M, int G, double dx, double a2, ocplx a1, double g,
     return info;
 }
 
+/* Thomas algorithm: lo[i] A[i][i-1], md[i] A[i][i], up[i] A[i][i+1] */
+static void
+tridiag_solve(int n, const ocplx* lo, const ocplx* md, const ocplx* up,
+              const ocplx* rhs, ocplx* x)
+{
+    ocplx* c = malloc(sizeof(ocplx) * n);
+    ocplx* d = malloc(sizeof(ocplx) * n);
+    c[0] = up[0] / md[0];
+    d[0] = rhs[0] / md[0];
+    for (int i = 1; i < n; i++)
+    {
+        const ocplx den = md[i] - lo[i] * c[i - 1];
+        c[i] = up[i] / den;
+        d[i] = (rhs[i] - lo[i] * d[i - 1]) / den;
+    }
+    x[n - 1] = d[n - 1];
+    for (int i = n - 2; i >= 0; i--) x[i] = d[i] - c[i] * x[i + 1];
+    free(c);
+    free(d);
+}
+
+/* Crank-Nicolson half step of the linear part (split_linear_orbitals.c:
+ * 23-56, 289-373): (i - dth A) f' = (i + dth A) f in the reference's
+ * coefficients, dth = prop_dt / 2; periodic grids solve the cyclic system
+ * on the G - 1 distinct points (Sherman-Morrison) and copy the last point */
+static void
+cn_half_step(int G, double dx, double a2, ocplx a1, int periodic, ocplx dth,
+             ocplx* f)
+{
+    const ocplx mid = I + a2 * dth / dx / dx;
+    const ocplx up = -a2 * dth / dx / dx / 2 - a1 * dth / dx / 4;
+    const ocplx lo = -a2 * dth / dx / dx / 2 + a1 * dth / dx / 4;
+    const ocplx rmid = I - a2 * dth / dx / dx;
+    const ocplx rup = a2 * dth / dx / dx / 2 + a1 * dth / dx / 4;
+    const ocplx rlo = a2 * dth / dx / dx / 2 - a1 * dth / dx / 4;
+    const int   n = periodic ? G - 1 : G;
+    ocplx*      rhs = calloc(n, sizeof(ocplx));
+    ocplx*      L = calloc(n, sizeof(ocplx));
+    ocplx*      D = calloc(n, sizeof(ocplx));
+    ocplx*      U = calloc(n, sizeof(ocplx));
+    ocplx*      x = calloc(n, sizeof(ocplx));
+    for (int i = 0; i < n; i++)
+    {
+        ocplx r = rmid * f[i];
+        if (i + 1 < n) r += rup * f[i + 1];
+        else if (periodic) r += rup * f[0];
+        if (i > 0) r += rlo * f[i - 1];
+        else if (periodic) r += rlo * f[n - 1];
+        rhs[i] = r;
+        L[i] = lo;
+        D[i] = mid;
+        U[i] = up;
+    }
+    if (!periodic)
+        tridiag_solve(n, L, D, U, rhs, x);
+    else
+    {
+        /* corners A[0][n-1] = lo, A[n-1][0] = up: A = T + u v^T with
+         * u = (gam, 0 .., up), v = (1, 0 .., lo / gam) */
+        const ocplx gam = -mid;
+        ocplx*      u = calloc(n, sizeof(ocplx));
+        ocplx*      z = malloc(sizeof(ocplx) * n);
+        D[0] = mid - gam;
+        D[n - 1] = mid - up * lo / gam;
+        u[0] = gam;
+        u[n - 1] = up;
+        tridiag_solve(n, L, D, U, rhs, x);
+        tridiag_solve(n, L, D, U, u, z);
+        const ocplx fac = (x[0] + lo / gam * x[n - 1]) / (1.0 + z[0] + lo / gam * z[n - 1]);
+        for (int i = 0; i < n; i++) x[i] -= fac * z[i];
+        free(u);
+        free(z);
+    }
+    for (int i = 0; i < n; i++) f[i] = x[i];
+    if (periodic) f[G - 1] = f[0];
+    free(rhs);
+    free(L);
+    free(D);
+    free(U);
+    free(x);
+}
+
+/* FFT-exponential half step (split_linear_orbitals.c:57-82, 375-402):
+ * f <- IDFT(exp(-i dth (i freq a1 - freq^2 a2)) DFT(f)) on the n = G - 1
+ * distinct points, 1/sqrt(n) both ways, restated as direct sums */
+static void
+fftexp_half_step(int G, double dx, double a2, ocplx a1, ocplx dth, ocplx* f)
+{
+    const int    n = G - 1;
+    const double pi = 3.14159265358979323846, sc = 1.0 / sqrt((double) n);
+    ocplx*       F = malloc(sizeof(ocplx) * n);
+    for (int k = 0; k < n; k++)
+    {
+        ocplx z = 0;
+        for (int x = 0; x < n; x++)
+            z += f[x] * cexp(-2 * I * pi * (double) (((long) k * x) % n) / n);
+        const double freq = k <= (n - 1) / 2 ? 2 * pi * k / (n * dx)
+                                             : 2 * pi * (k - n) / (n * dx);
+        F[k] = z * sc * cexp(-I * dth * (I * a1 * freq - a2 * freq * freq));
+    }
+    for (int x = 0; x < n; x++)
+    {
+        ocplx z = 0;
+        for (int k = 0; k < n; k++)
+            z += F[k] * cexp(2 * I * pi * (double) (((long) k * x) % n) / n);
+        f[x] = z * sc;
+    }
+    f[n] = f[0];
+    free(F);
+}
+
+void
+orc_linear_half_step(int der, int G, double dx, double a2, ocplx a1, int periodic,
+                     ocplx dth, ocplx* f)
+{
+    if (der == 302) cn_half_step(G, dx, a2, a1, periodic, dth, f);
+    else fftexp_half_step(G, dx, a2, a1, dth, f);
+}
+
 typedef struct
 {
-    int           M, G, periodic, robust, der;
+    int           M, G, periodic, robust, der, split;
     double        dx, a2, g;
     ocplx         a1, tf;
     const double* pot;
-    const ocplx * rinv, *rho2;
+    const ocplx * rinv, *rho2, *hob, *hint;
 } rhs_args;
+
+/* split_nonlinear_orbitals.c:63-160 (orb_full_nonlinear) at point x of
+ * orbital k: the interacting part with its projection through h and g,
+ * over the same index ranges (s >= a, l >= q with the exchange factors) */
+static ocplx
+full_nonlinear(int k, int x, int M, int G, double g, const ocplx* orb,
+               const ocplx* hob, const ocplx* hint, const ocplx* rho,
+               const ocplx* rinv)
+{
+    const int mm = M * M, mmm = mm * M;
+#define O(i) orb[(i) * G + x]
+    ocplx red = 0;
+    for (int a = 0; a < M; a++)
+    {
+        red -= hob[a * M + k] * O(a);
+        for (int q = 0; q < M; q++)
+        {
+            ocplx rm = rinv[k * M + a] * rho[a + M * a + mm * q + mmm * q];
+            red += g * rm * conj(O(a)) * O(q) * O(q);
+            for (int j = 0; j < M; j++) red -= rm * O(j) * hint[j + a * M + q * mm + q * mmm];
+            for (int l = q + 1; l < M; l++)
+            {
+                rm = 2 * rinv[k * M + a] * rho[a + M * a + mm * q + mmm * l];
+                red += g * rm * conj(O(a)) * O(l) * O(q);
+                for (int j = 0; j < M; j++)
+                    red -= rm * O(j) * hint[j + a * M + l * mm + q * mmm];
+            }
+        }
+        for (int s = a + 1; s < M; s++)
+        {
+            for (int q = 0; q < M; q++)
+            {
+                ocplx rm = rinv[k * M + a] * rho[a + M * s + mm * q + mmm * q];
+                ocplx sw = rinv[k * M + s] * rho[a + M * s + mm * q + mmm * q];
+                red += g * (rm * conj(O(s)) + sw * conj(O(a))) * O(q) * O(q);
+                for (int j = 0; j < M; j++)
+                {
+                    red -= rm * O(j) * hint[j + s * M + q * mm + q * mmm];
+                    red -= sw * O(j) * hint[j + a * M + q * mm + q * mmm];
+                }
+                for (int l = q + 1; l < M; l++)
+                {
+                    rm = 2 * rinv[k * M + a] * rho[a + M * s + mm * q + mmm * l];
+                    sw = 2 * rinv[k * M + s] * rho[a + M * s + mm * q + mmm * l];
+                    red += g * (rm * conj(O(s)) + sw * conj(O(a))) * O(l) * O(q);
+                    for (int j = 0; j < M; j++)
+                    {
+                        red -= rm * O(j) * hint[j + s * M + l * mm + q * mmm];
+                        red -= sw * O(j) * hint[j + a * M + l * mm + q * mmm];
+                    }
+                }
+            }
+        }
+    }
+#undef O
+    return red;
+}
 
 static void
 rhs_eval(const rhs_args* a, const ocplx* y, ocplx* out)
 {
+    if (a->split)
+    {
+        /* orbital_integration.c:243-281: -i tf (nonlinear + V f) */
+        for (int k = 0; k < a->M; k++)
+            for (int x = 0; x < a->G; x++)
+                out[k * a->G + x] =
+                    -I * a->tf *
+                    (full_nonlinear(k, x, a->M, a->G, a->g, y, a->hob, a->hint, a->rho2,
+                                    a->rinv) +
+                     a->pot[x] * y[k * a->G + x]);
+        return;
+    }
     orc_orbital_rhs(a->M, a->G, a->dx, a->a2, a->a1, a->g, a->periodic, a->tf,
                     a->pot, a->rinv, a->rho2, y, out, a->robust, a->der);
 }
@@ -1778,17 +1966,42 @@ orc_propagate_step(int npar, int M, int G, double dx, double dt, double a2,
                    ocplx a1, double g, int periodic, int imagtime, int rk_order,
                    int lanczos_m, double reg_fac, const double* pot, ocplx* orb,
                    ocplx* coef, ocplx* hob, ocplx* hint, ocplx* rho1,
-                   ocplx* rho2, ocplx* rinv, int robust, int der, int coef_method)
+                   ocplx* rho2, ocplx* rinv, int robust, int der, int coef_method,
+                   int orb_method)
 {
     int      n = M * G;
     ocplx    tf = imagtime ? -I : 1.0;
     ocplx    prop_dt = imagtime ? -I * dt : dt;
-    rhs_args a = {M, G, periodic, robust, der, dx, a2, g, a1, tf, pot, rinv, rho2};
+    rhs_args a = {M,  G,  periodic, robust, der, orb_method == 31, dx, a2, g,
+                  a1, tf, pot,      rinv,   rho2, hob, hint};
     if (periodic)
         for (int k = 0; k < M; k++) orb[k * G + G - 1] = orb[k * G];
     ocplx* next = malloc(sizeof(ocplx) * n);
-    rk_step(rk_order, &a, n, dt, orb, next);
-    memcpy(orb, next, sizeof(ocplx) * n);
+    if (orb_method == 31)
+    {
+        /* orbital_integration.c:352-434: linear half step, h and g of the
+         * new orbitals, RK of the nonlinear part, linear half step */
+        const ocplx dth = 0.5 * prop_dt;
+        for (int k = 0; k < M; k++)
+        {
+            if (der == 302) cn_half_step(G, dx, a2, a1, periodic, dth, orb + k * G);
+            else fftexp_half_step(G, dx, a2, a1, dth, orb + k * G);
+        }
+        orc_orbital_hob(M, G, dx, a2, a1, pot, orb, hob);
+        orc_orbital_hint(M, G, dx, g, orb, hint);
+        rk_step(rk_order, &a, n, dt, orb, next);
+        memcpy(orb, next, sizeof(ocplx) * n);
+        for (int k = 0; k < M; k++)
+        {
+            if (der == 302) cn_half_step(G, dx, a2, a1, periodic, dth, orb + k * G);
+            else fftexp_half_step(G, dx, a2, a1, dth, orb + k * G);
+        }
+    }
+    else
+    {
+        rk_step(rk_order, &a, n, dt, orb, next);
+        memcpy(orb, next, sizeof(ocplx) * n);
+    }
     free(next);
     if (imagtime) orc_orthonormalize(G, dx, M, orb);
     if (periodic)

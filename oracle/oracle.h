@@ -120,17 +120,24 @@ int orc_orbital_rhs(int norb, int npts, double dx, double d2coef,
                     const double* pot, const ocplx* rho1_inv,
                     const ocplx* rho2, const ocplx* orb, ocplx* dodt,
                     int robust, int der);
+/* one linear half step of the split-step integrator on one orbital (in
+ * place): der 302 Crank-Nicolson (split_linear_orbitals.c:23-56, 289-373),
+ * otherwise the FFT exponential (:57-82, 375-402); dth = prop_dt / 2 */
+void orc_linear_half_step(int der, int npts, double dx, double d2coef, ocplx d1coef,
+                          int periodic, ocplx dth, ocplx* f);
 /* one full step of driver.c:159-201 (FULLSTEP_RUNGEKUTTA + LANCZOS, FD,
  * time-independent trap and interaction).  rk_order in {2,4,5} with the
  * named tableaux of shim/odesys.h; robust and der select the projector
  * and the linear part as in orc_orbital_rhs; coef_method 20 (SIL) or 21
- * (Runge-Kutta, coefficients_integration.c:15-57).  State arrays are updated
- * in place. */
+ * (Runge-Kutta, coefficients_integration.c:15-57); orb_method 30 full
+ * step or 31 split step (orbital_integration.c:352-434: Crank-Nicolson for
+ * finite differences, the FFT exponential otherwise).  State arrays are
+ * updated in place. */
 void orc_propagate_step(int npar, int norb, int npts, double dx, double dt,
                         double d2coef, ocplx d1coef, double g, int periodic,
                         int imagtime, int rk_order, int lanczos_m,
                         double reg_fac, const double* pot, ocplx* orb,
                         ocplx* coef, ocplx* hob, ocplx* hint, ocplx* rho1,
                         ocplx* rho2, ocplx* rho1_inv, int robust, int der,
-                        int coef_method);
+                        int coef_method, int orb_method);
 #endif

@@ -92,13 +92,15 @@ class Oracle:
         L.orc_herm_inverse.restype = i
         L.orc_herm_inverse.argtypes = [i, _c128p, _c128p]
         L.orc_sync_density_matrices.argtypes = [i, i, _c128p, C.c_double, _c128p, _c128p, _c128p]
+        L.orc_linear_half_step.argtypes = [i, i, C.c_double, C.c_double, _C128, i, _C128,
+                                           _c128p]
         L.orc_orbital_rhs.restype = i
         L.orc_orbital_rhs.argtypes = [i, i, C.c_double, C.c_double, _C128, C.c_double, i, _C128,
                                       _f64p, _c128p, _c128p, _c128p, _c128p, i, i]
         L.orc_propagate_step.argtypes = [i, i, i, C.c_double, C.c_double, C.c_double, _C128,
                                          C.c_double, i, i, i, i, C.c_double, _f64p,
                                          _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, _c128p, i,
-                                         i, i]
+                                         i, i, i]
 
     # ---- space -------------------------------------------------------
     def dim(self, N, M):
@@ -272,8 +274,15 @@ class Oracle:
             raise ValueError(f"singular overlap matrix (column {info - 1})")
         return out.reshape(M, G)
 
+    def linear_half_step(self, der, f, dx, d2coef, d1coef, periodic, dth):
+        f = cvec(f).copy()
+        self.lib.orc_linear_half_step(int(der), len(f), dx, d2coef, _c(d1coef), int(periodic),
+                                      _c(dth), f)
+        return f
+
     def propagate_step(self, st, N, dx, dt, d2coef, d1coef, g, periodic, imagtime, rk_order,
-                       lanczos_m, pot, reg_fac=1e-9, robust=False, der=302, coef_method=20):
+                       lanczos_m, pot, reg_fac=1e-9, robust=False, der=302, coef_method=20,
+                       orb_method=30):
         """One full step; `st` is a dict of numpy arrays updated in place:
         orb (M,G), coef, hob (M,M), hint, rho1 (M,M), rho2, rinv (M,M)."""
         M, G = st["orb"].shape
@@ -284,7 +293,7 @@ class Oracle:
                                     int(imagtime), rk_order, lanczos_m, reg_fac,
                                     np.ascontiguousarray(pot, np.float64),
                                     *[a.reshape(-1) for a in args], int(robust), int(der),
-                                    int(coef_method))
+                                    int(coef_method), int(orb_method))
 
 
 class Reference:
@@ -386,7 +395,7 @@ class Reference:
 
     def make_mctdhb(self, N, M, G, xi, xf, imagtime, rk_order, lanczos_m, dt, omega, g,
                     periodic=True, omega_f=None, pot_period=0.0, g_f=None, g_period=0.0,
-                    der=T.FINITEDIFF, coef=T.LANCZOS):
+                    der=T.FINITEDIFF, coef=T.LANCZOS, orb=T.FULLSTEP_RUNGEKUTTA):
         """A reference MCTDHBDataStruct from its own constructor
         (types_definition.c:247): FULLSTEP_RUNGEKUTTA orbitals, `der`
         derivatives (FINITEDIFF by default), LANCZOS coefficients, harmonic trap
@@ -398,7 +407,7 @@ class Reference:
                                     0.0, 0.0)
         g_args = (C.c_double * 5)(g, g if g_f is None else g_f, g_period, 0.0, 0.0)
         ms = L.get_mctdhb_struct(
-            T.IMAGTIME if imagtime else T.REALTIME, coef, T.FULLSTEP_RUNGEKUTTA,
+            T.IMAGTIME if imagtime else T.REALTIME, coef, orb,
             der, rk_order, lanczos_m, N, M, b"harmonic",
             T.PERIODIC_BOUNDS if periodic else T.ZERO_BOUNDS, xi, xf, G, dt, 1.0, -0.5,
             T.dcomplex(0.0, 0.0), C.cast(pot_args, C.c_void_p), C.cast(g_args, C.c_void_p),

@@ -202,3 +202,64 @@ def test_coef_rk_step_oracle_vs_reference(oracle, reference, imag, rk):
         assert rel_err(st["rho1"], rs["rho1"]) < 1e-10
     finally:
         reference.destroy_mctdhb(ms)
+
+
+@pytest.mark.parametrize("imag,periodic,rk", [(True, True, 5), (False, True, 4),
+                                              (False, False, 5), (True, False, 4)])
+def test_splitstep_oracle_vs_reference(oracle, reference, imag, periodic, rk):
+    """split-step orbitals (orbital_integration.c:352-434): Crank-Nicolson
+    half steps of the linear part around a Runge-Kutta step of
+    orb_full_nonlinear, against the reference's own step"""
+    import mctdhb_types as T
+
+    N, M, G, m, dt, g = 4, 3, 64, 5, 0.005, 0.5
+    xi, xf = -8.0, 8.0
+    ms, keep = reference.make_mctdhb(N, M, G, xi, xf, imag, rk, m, dt, 1.0, g,
+                                     periodic=periodic, orb=T.SPLITSTEP)
+    try:
+        orb, dx = hermite_orbitals(M, G, xi, xf)
+        coef = rand_coef(np.random.default_rng(51 + rk), oracle.dim(N, M))
+        reference.set_state(ms, orb, coef)
+        r0 = reference.get_state(ms)
+        st = oracle_state(r0, coef)
+        for k in range(3):
+            reference.step(ms, k)
+            oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, periodic, imag, rk, m, r0["pot"],
+                                  orb_method=31)
+        rs = reference.get_state(ms)
+        assert rel_err(st["orb"], rs["orb"]) < 1e-10
+        assert rel_err(st["coef"], rs["coef"]) < 1e-10
+        assert rel_err(st["rho1"], rs["rho1"]) < 1e-10
+    finally:
+        reference.destroy_mctdhb(ms)
+
+
+@pytest.mark.parametrize("imag", [False, True])
+def test_linear_half_steps_vs_numpy(oracle, imag):
+    """the split-step linear half steps: the FFT exponential against numpy's
+    FFT; Crank-Nicolson against a dense solve of the same tridiagonal (cyclic
+    on periodic grids) system"""
+    G, dx, a2, a1 = 64, 0.25, -0.5, 0.15j
+    dth = 0.5 * (-1j * 0.01 if imag else 0.01)
+    rng = np.random.default_rng(3)
+    f = rng.normal(size=G) + 1j * rng.normal(size=G)
+    f[-1] = f[0]
+    n = G - 1
+    k = np.arange(n)
+    freq = np.where(k <= (n - 1) // 2, 2 * np.pi * k / (n * dx), 2 * np.pi * (k - n) / (n * dx))
+    want = np.fft.ifft(np.fft.fft(f[:n]) * np.exp(-1j * dth * (1j * a1 * freq - a2 * freq ** 2)))
+    got = oracle.linear_half_step(301, f, dx, a2, a1, True, dth)
+    assert rel_err(got[:n], want) < 1e-12 and got[-1] == got[0]
+    for periodic in (True, False):
+        m = n if periodic else G
+        mid, up = 1j + a2 * dth / dx ** 2, -a2 * dth / dx ** 2 / 2 - a1 * dth / dx / 4
+        lo = -a2 * dth / dx ** 2 / 2 + a1 * dth / dx / 4
+        A = np.diag(np.full(m, mid)) + np.diag(np.full(m - 1, up), 1) + \
+            np.diag(np.full(m - 1, lo), -1)
+        B = np.diag(np.full(m, 1j - a2 * dth / dx ** 2)) + \
+            np.diag(np.full(m - 1, -up), 1) + np.diag(np.full(m - 1, -lo), -1)
+        if periodic:
+            A[0, -1], A[-1, 0], B[0, -1], B[-1, 0] = lo, up, -lo, -up
+        want = np.linalg.solve(A, B @ f[:m])
+        got = oracle.linear_half_step(302, f, dx, a2, a1, periodic, dth)
+        assert rel_err(got[:m], want) < 1e-12, periodic
