@@ -142,9 +142,9 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
         set_error("mctdhb_propagate_step: incomplete MCTDHBDataStruct");
         return;
     }
-    if (mctdhb->orb_integ_method != FULLSTEP_RUNGEKUTTA) {
-        set_error("mctdhb_propagate_step: the GPU path integrates full-step Runge-Kutta orbitals "
-                  "(got method %d)", (int)mctdhb->orb_integ_method);
+    if (mctdhb->orb_integ_method != FULLSTEP_RUNGEKUTTA && mctdhb->orb_integ_method != SPLITSTEP) {
+        set_error("mctdhb_propagate_step: orbital method %d not FULLSTEP_RUNGEKUTTA or SPLITSTEP",
+                  (int)mctdhb->orb_integ_method);
         return;
     }
     const bool sil = mctdhb->coef_integ_method == LANCZOS;
@@ -198,7 +198,8 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
         mctdhb_solver_set_orthogonality(s, mctdhb->orb_workspace->impr_ortho ? 1 : 0))
         return;
     if (mctdhb_solver_set_derivative(s, (int)mctdhb->orb_der_method) ||
-        mctdhb_solver_set_coef_method(s, (int)mctdhb->coef_integ_method))
+        mctdhb_solver_set_coef_method(s, (int)mctdhb->coef_integ_method) ||
+        mctdhb_solver_set_orb_method(s, (int)mctdhb->orb_integ_method))
         return;
     cudaStream_t st = 0;
     if (mctdhb_solver_phase(s, 0, st)) return;

@@ -15,6 +15,11 @@
 //   Runge-Kutta step     propagate_fullstep_orb_rk (orbital_integration.c:284)
 //                        with the named tableaux Heun / classical RK4 /
 //                        Butcher RK5
+//   split step           propagate_splitstep_orb (orbital_integration.c:352):
+//                        Crank-Nicolson or FFT-exponential half steps as one
+//                        precomputed operator product (circulant on periodic
+//                        grids, dense with zero bounds), RK of the full
+//                        nonlinear term (split_nonlinear_orbitals.c:63-160)
 //   Gram-Schmidt         orthonormalize (calculus.c:171-191)
 //   rho1 synchronisation sync_density_matrices (synchronize.c:42-57)
 // Grid functions are row-major M x G complex128; integrals use the composite
@@ -130,6 +135,87 @@ __global__ void __launch_bounds__(256) orb_toeplitz_kernel(OrbView o, const doub
     double2 acc = make_double2(0.0, 0.0);
     for (int j = 0; j < n; j++) acc = cfma(__ldg(t + j), fs[j], acc);
     L[(size_t)k * G + x] = cadd(acc, cscale(fs[xr], o.pot[xr]));
+}
+
+// Linear half step of the split-step integrator: out_k = Op f_k.  Circulant
+// Op on the n = G - 1 periodic points (kernel t, (Op f)_x =
+// sum_j t[j - x + n - 1] f_j, out(n) = out(0)), or dense on all G points
+// (zero bounds; stored column-major, Op[x][j] = D[j G + x]).
+__global__ void __launch_bounds__(256) orb_half_kernel(OrbView o, const double2* __restrict__ op,
+                                                       int dense, const double2* __restrict__ y,
+                                                       double2* __restrict__ out) {
+    extern __shared__ double2 fs[];
+    const int G = o.G, n = dense ? G : G - 1;
+    const int k = blockIdx.y;
+    const double2* f = y + (size_t)k * G;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) fs[j] = f[j];
+    __syncthreads();
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= G) return;
+    double2 acc = make_double2(0.0, 0.0);
+    if (dense) {
+        for (int j = 0; j < n; j++) acc = cfma(__ldg(op + (size_t)j * G + x), fs[j], acc);
+    } else {
+        const double2* t = op + (n - 1 - (x == n ? 0 : x));
+        for (int j = 0; j < n; j++) acc = cfma(__ldg(t + j), fs[j], acc);
+    }
+    out[(size_t)k * G + x] = acc;
+}
+
+// B[k][j] = sum_{a,s,q,l} rinv[k][a] rho2[a + sM + qM^2 + lM^3]
+//           hint[j + sM + lM^2 + qM^3]: the projection of the interacting
+// part through g in orb_full_nonlinear (split_nonlinear_orbitals.c:63-160),
+// summed over all index orders (rho2 and g are symmetric in the pairs)
+__global__ void orb_bmat_kernel(int M, const double2* __restrict__ rinv,
+                                const double2* __restrict__ rho2,
+                                const double2* __restrict__ hint, double2* __restrict__ B) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M * M) return;
+    const int k = e / M, j = e % M, M2 = M * M, M3 = M2 * M;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int a = 0; a < M; a++) {
+        double2 inner = make_double2(0.0, 0.0);
+        for (int s = 0; s < M; s++)
+            for (int q = 0; q < M; q++)
+                for (int l = 0; l < M; l++)
+                    inner = cfma(rho2[a + s * M + q * M2 + l * M3],
+                                 hint[j + s * M + l * M2 + q * M3], inner);
+        acc = cfma(rinv[k * M + a], inner, acc);
+    }
+    B[e] = acc;
+}
+
+// nonlinear right-hand side of the split step (orbital_integration.c:
+// 243-281): -i tf (interacting - sum_j (h[j][k] + B[k][j]) f_j + V f_k)
+__global__ void orb_split_rhs_kernel(OrbView o, const double2* __restrict__ y,
+                                     const double2* __restrict__ Q,
+                                     const double2* __restrict__ hob,
+                                     const double2* __restrict__ B, double2* __restrict__ out) {
+    const int M = o.M, G = o.G;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M * G) return;
+    const int k = t / G, x = t % G;
+    double2 fx[kMaxOrb];
+    for (int a = 0; a < M; a++) fx[a] = y[(size_t)a * G + x];
+    const double2* Qk = Q + (size_t)k * M * M * M;
+    double2 red = make_double2(0.0, 0.0);
+    for (int s = 0; s < M; s++) {
+        double2 ts = make_double2(0.0, 0.0);
+        for (int l = 0; l < M; l++) {
+            double2 tl = make_double2(0.0, 0.0);
+            for (int q = 0; q < M; q++) tl = cfma(Qk[s + q * M + l * M * M], fx[q], tl);
+            ts = cfma(tl, fx[l], ts);
+        }
+        red = cfma(make_double2(fx[s].x, -fx[s].y), ts, red);
+    }
+    for (int j = 0; j < M; j++) {
+        const double2 c = cadd(hob[j * M + k], B[k * M + j]);
+        red.x -= c.x * fx[j].x - c.y * fx[j].y;
+        red.y -= c.x * fx[j].y + c.y * fx[j].x;
+    }
+    red = cadd(red, cscale(fx[k], o.pot[x]));
+    const double2 mi_tf = make_double2(o.tf.y, -o.tf.x);
+    out[t] = cmul(mi_tf, red);
 }
 
 // H phi_k at every grid point: linear part (finite differences, or the
@@ -313,6 +399,8 @@ void orb_release(OrbCtx& c) {
     cudaFree(c.d_fail);
     cudaFree(c.d_lin_t);
     cudaFree(c.d_L);
+    cudaFree(c.d_half);
+    cudaFree(c.d_B);
     c = OrbCtx();
 }
 
@@ -362,10 +450,23 @@ static int combo(const OrbCtx& c, const double2* y, std::initializer_list<std::p
     return 0;
 }
 
-int orb_rk_step(const OrbCtx& c, int order, double dt, const double2* rinv, const double2* rho2,
-                const double2* y, double2* ynext, cudaStream_t st) {
-    const int M = c.M, M4 = M * M * M * M;
-    orb_q_kernel<<<(M4 + 127) / 128, 128, 0, st>>>(M, c.d_g, rinv, rho2, c.d_Q);
+// right-hand side of one RK stage: full step (orb_rhs) or the split step's
+// nonlinear part (Q, c.split_hob and c.d_B prepared)
+static int stage_rhs(const OrbCtx& c, bool split, const double2* y, double2* out,
+                     cudaStream_t st) {
+    if (!split) return orb_rhs(c, y, out, st);
+    const int n = c.M * c.G;
+    orb_split_rhs_kernel<<<(n + 127) / 128, 128, 0, st>>>(c.view, y, c.d_Q, c.split_hob, c.d_B,
+                                                          out);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+static int rk_stages(const OrbCtx& c, bool split, int order, double dt, const double2* y,
+                     double2* ynext, cudaStream_t st) {
+    auto orb_rhs = [&](const OrbCtx& cc, const double2* yy, double2* out, cudaStream_t s2) {
+        return stage_rhs(cc, split, yy, out, s2);
+    };
     double2* const* k = c.d_k;
     double2* w = c.d_k[6];
     int rc = 0;
@@ -404,6 +505,46 @@ int orb_rk_step(const OrbCtx& c, int order, double dt, const double2* rinv, cons
         return -1;
     }
     return rc ? -1 : 0;
+}
+
+int orb_rk_step(const OrbCtx& c, int order, double dt, const double2* rinv, const double2* rho2,
+                const double2* y, double2* ynext, cudaStream_t st) {
+    const int M = c.M, M4 = M * M * M * M;
+    orb_q_kernel<<<(M4 + 127) / 128, 128, 0, st>>>(M, c.d_g, rinv, rho2, c.d_Q);
+    return rk_stages(c, false, order, dt, y, ynext, st);
+}
+
+// apply the half-step operator to every orbital of y (in place, through
+// the spare stage buffer)
+static int half_step(const OrbCtx& c, double2* y, cudaStream_t st) {
+    const int G = c.G;
+    const int nn = c.half_dense ? G : G - 1;
+    const dim3 grid((G + 255) / 256, c.M);
+    orb_half_kernel<<<grid, 256, (size_t)nn * sizeof(double2), st>>>(c.view, c.d_half,
+                                                                      c.half_dense, y, c.d_k[7]);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(y, c.d_k[7], (size_t)c.M * G * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, st));
+    return 0;
+}
+
+int orb_split_step(OrbCtx& c, int order, double dt, const double2* rinv, const double2* rho2,
+                   double2* y, double2* ynext, double2* hob, double2* hint, cudaStream_t st) {
+    if (!c.split || !c.d_half) {
+        set_error("orb_split_step: split-step operator not set up");
+        return -1;
+    }
+    const int M = c.M, M4 = M * M * M * M;
+    if (half_step(c, y, st)) return -1;
+    // h and g of the half-stepped orbitals (the reference's
+    // sync_orbital_matrices inside propagate_splitstep_orb)
+    if (orb_matrices(c, y, hob, hint, st)) return -1;
+    orb_q_kernel<<<(M4 + 127) / 128, 128, 0, st>>>(M, c.d_g, rinv, rho2, c.d_Q);
+    orb_bmat_kernel<<<(M * M + 63) / 64, 64, 0, st>>>(M, rinv, rho2, hint, c.d_B);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    c.split_hob = hob;
+    if (rk_stages(c, true, order, dt, y, ynext, st)) return -1;
+    return half_step(c, ynext, st);
 }
 
 int orb_rhs_eval(const OrbCtx& c, const double2* rinv, const double2* rho2, const double2* y,
@@ -506,6 +647,101 @@ int orb_set_derivative(OrbCtx& c, int der) {
                                          (int)((size_t)(c.G - 1) * sizeof(double2))));
     c.view.lin_t = c.d_lin_t;
     c.der = der;
+    return 0;
+}
+
+// Half-step operator of the split-step integrator for dth = prop_dt / 2
+// (LINEAR_TSTEP_FRAC of split_linear_orbitals.h):
+//   finite differences, Crank-Nicolson (split_linear_orbitals.c:23-56,
+//     289-373): Op = A^{-1} B with A = i + dth (a2 D2 + a1 D1),
+//     B = i - dth (a2 D2 + a1 D1) in the reference's tridiagonal entries;
+//     periodic grids: A and B are circulant on the G - 1 distinct points, so
+//     Op is the circulant with eigenvalues lambda_B / lambda_A; zero bounds:
+//     Op dense, column by column by the Thomas algorithm
+//   DVR / spectral, FFT exponential (:57-82, 375-402): the circulant with
+//     eigenvalues exp(-i dth (i freq a1 - freq^2 a2)) at the FFT frequencies
+int orb_set_split(OrbCtx& c, int split, double dt, int imagtime) {
+    using cd = std::complex<double>;
+    cudaFree(c.d_half);
+    cudaFree(c.d_B);
+    c.d_half = nullptr;
+    c.d_B = nullptr;
+    c.split = 0;
+    if (!split) return 0;
+    const int G = c.G;
+    const bool periodic = c.view.periodic != 0, fd = c.der == kDerFiniteDiff;
+    if (!periodic && !fd) {
+        set_error("split step: the FFT exponential needs periodic boundaries");
+        return -1;
+    }
+    if ((periodic && G - 1 > 8191) || (!periodic && G > 2048)) {
+        set_error("split step: grid of %d points above the operator's limit", G);
+        return -1;
+    }
+    const double dx = c.view.dx, a2 = c.view.a2, pi = 3.14159265358979323846;
+    const cd a1(c.view.a1.x, c.view.a1.y), I(0.0, 1.0);
+    const cd dth = 0.5 * (imagtime ? cd(0.0, -dt) : cd(dt, 0.0));
+    const cd mid = I + a2 * dth / dx / dx, up = -a2 * dth / dx / dx / 2.0 - a1 * dth / dx / 4.0,
+             lo = -a2 * dth / dx / dx / 2.0 + a1 * dth / dx / 4.0;
+    const cd rmid = I - a2 * dth / dx / dx;
+    std::vector<double2> op;
+    if (periodic) {
+        const int n = G - 1;
+        std::vector<cd> ex(n), mu(n), cop(n);
+        for (int m = 0; m < n; m++) ex[m] = std::polar(1.0, 2.0 * pi * m / n);
+        for (int m = 0; m < n; m++) {
+            if (fd) {
+                const cd w = ex[m], wi = std::conj(ex[m]);
+                mu[m] = (rmid - up * w - lo * wi) / (mid + up * w + lo * wi);
+            } else {
+                const double freq = m <= (n - 1) / 2 ? 2.0 * pi * m / (n * dx)
+                                                     : 2.0 * pi * (m - n) / (n * dx);
+                mu[m] = std::exp(-I * dth * (I * a1 * freq - a2 * freq * freq));
+            }
+        }
+        // c_op[d] = (1/n) sum_m mu_m e^{-2 pi i m d / n}
+        for (int d = 0; d < n; d++) {
+            cd z = 0.0;
+            for (int m = 0; m < n; m++) z += mu[m] * std::conj(ex[((long)m * d) % n]);
+            cop[d] = z / (double)n;
+        }
+        op.resize(2 * (size_t)n - 1);
+        for (int d = -(n - 1); d < n; d++) {
+            const cd v = cop[((d % n) + n) % n];
+            op[d + n - 1] = make_double2(v.real(), v.imag());
+        }
+    } else {
+        // zero bounds: columns of A^{-1} B (A, B tridiagonal on all G points)
+        op.resize((size_t)G * G);
+        std::vector<cd> cc(G), dd(G), b(G), x(G);
+        for (int j = 0; j < G; j++) {
+            for (int i = 0; i < G; i++) b[i] = 0.0;
+            b[j] = rmid;
+            if (j > 0) b[j - 1] = -up;  // B[j-1][j]
+            if (j + 1 < G) b[j + 1] = -lo;  // B[j+1][j]
+            cc[0] = up / mid;
+            dd[0] = b[0] / mid;
+            for (int i = 1; i < G; i++) {
+                const cd den = mid - lo * cc[i - 1];
+                cc[i] = up / den;
+                dd[i] = (b[i] - lo * dd[i - 1]) / den;
+            }
+            x[G - 1] = dd[G - 1];
+            for (int i = G - 2; i >= 0; i--) x[i] = dd[i] - cc[i] * x[i + 1];
+            for (int i = 0; i < G; i++)
+                op[(size_t)j * G + i] = make_double2(x[i].real(), x[i].imag());
+        }
+    }
+    MCTDHB_CUDA_TRY(cudaMalloc(&c.d_half, op.size() * sizeof(double2)));
+    MCTDHB_CUDA_TRY(
+        cudaMemcpy(c.d_half, op.data(), op.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    MCTDHB_CUDA_TRY(cudaMalloc(&c.d_B, (size_t)c.M * c.M * sizeof(double2)));
+    const int nn = periodic ? G - 1 : G;
+    MCTDHB_CUDA_TRY(cudaFuncSetAttribute(orb_half_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)((size_t)nn * sizeof(double2))));
+    c.half_dense = periodic ? 0 : 1;
+    c.split = 1;
     return 0;
 }
 

@@ -43,6 +43,12 @@ struct OrbCtx {
     int der = kDerFiniteDiff;      // derivative method of the linear part
     double2* d_lin_t = nullptr;    // Toeplitz kernel of DVR / spectral derivatives
     double2* d_L = nullptr;        // linear part of every orbital (DVR / spectral)
+    // split-step integrator (orbital_integration.c:352-434)
+    int split = 0;
+    int half_dense = 0;            // half-step operator: 0 circulant kernel, 1 dense
+    double2* d_half = nullptr;     // circulant: 2n - 1 kernel; dense: G x G, column-major
+    double2* d_B = nullptr;        // M x M projection through g of the nonlinear part
+    const double2* split_hob = nullptr;  // h of the half-stepped orbitals (caller's buffer)
 };
 
 std::vector<double> simpson_weights(int n, double h);
@@ -59,6 +65,14 @@ int orb_periodic(const OrbCtx& c, double2* orb, cudaStream_t st);
 // derivative method: kDerFiniteDiff, or kDerDVR / kDerSpectral on a
 // periodic grid (the Toeplitz kernel is set up on the host)
 int orb_set_derivative(OrbCtx& c, int der);
+// split-step integrator on or off; builds the linear half-step operator
+// for time step dt (Crank-Nicolson for finite differences, the FFT
+// exponential for DVR / spectral), again whenever the method changes
+int orb_set_split(OrbCtx& c, int split, double dt, int imagtime);
+// one split step of the orbitals: y -> ynext through the half steps, h and
+// g of the half-stepped orbitals into hob / hint, and RK of the nonlinear part
+int orb_split_step(OrbCtx& c, int order, double dt, const double2* rinv, const double2* rho2,
+                   double2* y, double2* ynext, double2* hob, double2* hint, cudaStream_t st);
 // S_sl = <f_s|f_l> (Simpson) into c.d_S
 int orb_overlap_matrix(const OrbCtx& c, const double2* orb, cudaStream_t st);
 int orb_orthonormalize(const OrbCtx& c, double2* orb, cudaStream_t st);

@@ -48,11 +48,19 @@ namespace {
 // phase 0 (orbital_integration.c:284-349): orbitals advanced with the
 // current rho1^{-1} and rho2
 int phase_orbitals(mctdhb_solver_s* s, cudaStream_t st) {
-    const OrbCtx& o = s->orb;
+    OrbCtx& o = s->orb;
     const size_t n = (size_t)s->M * s->G;
     if (o.view.periodic && orb_periodic(o, s->d_orb, st)) return -1;
-    if (orb_rk_step(o, s->rk_order, s->dt, s->d_rinv, s->d_rho2, s->d_orb, s->d_orb_next, st))
+    if (o.split) {
+        // orbital_integration.c:352-434 (h and g of the half-stepped
+        // orbitals are rebuilt in phase 1 from the new orbitals)
+        if (orb_split_step(o, s->rk_order, s->dt, s->d_rinv, s->d_rho2, s->d_orb, s->d_orb_next,
+                           s->d_hob, s->d_hint, st))
+            return -1;
+    } else if (orb_rk_step(o, s->rk_order, s->dt, s->d_rinv, s->d_rho2, s->d_orb,
+                           s->d_orb_next, st)) {
         return -1;
+    }
     MCTDHB_CUDA_TRY(cudaMemcpyAsync(s->d_orb, s->d_orb_next, n * sizeof(double2),
                                     cudaMemcpyDeviceToDevice, st));
     if (s->imagtime && orb_orthonormalize(o, s->d_orb, st)) return -1;
@@ -279,7 +287,26 @@ int mctdhb_solver_set_derivative(mctdhb_solver s, int der_method) {
     if (der_method == s->orb.der) return 0;
     MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
     drop_graphs(s);  // the linear part is part of the captured step
-    return orb_set_derivative(s->orb, der_method);
+    if (orb_set_derivative(s->orb, der_method)) return -1;
+    return s->orb.split ? orb_set_split(s->orb, 1, s->dt, s->imagtime) : 0;
+}
+
+// Orbital integrator (driver.c:165-173): 30 FULLSTEP_RUNGEKUTTA (default),
+// 31 SPLITSTEP (orbital_integration.c:352-434: Crank-Nicolson half steps of
+// the linear part for finite differences, the FFT exponential for DVR and
+// spectral derivatives, around a Runge-Kutta step of the nonlinear part)
+int mctdhb_solver_set_orb_method(mctdhb_solver s, int orb_method) {
+    if (!s || (orb_method != 30 && orb_method != 31)) {
+        set_error("mctdhb_solver_set_orb_method: method not in {30 FULLSTEP_RUNGEKUTTA, "
+                  "31 SPLITSTEP}");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int split = orb_method == 31;
+    if (split == s->orb.split) return 0;
+    MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
+    drop_graphs(s);
+    return orb_set_split(s->orb, split, s->dt, s->imagtime);
 }
 
 // The projector of the orbital equation: 0 the simple one, 1 the robust one

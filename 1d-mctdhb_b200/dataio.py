@@ -365,7 +365,7 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
     <out_dir>/<prefix>_mctdhb_parameters.dat.
 
     `integrator`: the descriptor dict (read_integrator_descriptor); the GPU
-    solver runs FULLSTEP_RUNGEKUTTA orbitals with DVR (the reference's
+    solver runs FULLSTEP_RUNGEKUTTA or SPLITSTEP orbitals with DVR (the reference's
     default), SPECTRAL or FINITEDIFF derivatives and LANCZOS or RUNGEKUTTA
     coefficients.
     `monitor`: the dict of read_monitor_config.  Every
@@ -386,11 +386,12 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
 
     desc = dict(DEFAULT_INTEGRATOR, **(integrator or {}))
     mon = dict(DEFAULT_MONITOR, **(monitor or {}))
-    if desc["orb_method"] != FULLSTEP_RUNGEKUTTA or \
+    if desc["orb_method"] not in (FULLSTEP_RUNGEKUTTA, SPLITSTEP) or \
             desc["coef_method"] not in (LANCZOS, RUNGEKUTTA) or \
             desc["der_method"] not in (DVR, SPECTRAL, FINITEDIFF):
-        raise ValueError("the GPU solver runs FULLSTEP_RUNGEKUTTA orbitals (DVR, SPECTRAL or "
-                         "FINITEDIFF derivatives) and LANCZOS or RUNGEKUTTA coefficients")
+        raise ValueError("the GPU solver runs FULLSTEP_RUNGEKUTTA or SPLITSTEP orbitals (DVR, "
+                         "SPECTRAL or FINITEDIFF derivatives) and LANCZOS or RUNGEKUTTA "
+                         "coefficients")
     imag = desc["integ_type"] == IMAGTIME
     rec_n, mon_n = mon["rec_nsteps"], mon["monitor_nsteps"]
     os.makedirs(out_dir, exist_ok=True)
@@ -410,6 +411,7 @@ def run_jobs(prefix, in_dir, out_dir, integrator=None, monitor=None, stream=None
         try:
             s.set_derivative(desc["der_method"])
             s.set_coef_method(desc["coef_method"])
+            s.set_orb_method(desc["orb_method"])
             if mon["reg_factor"] is not None:
                 s.set_regularization(mon["reg_factor"])
             pot = builtin_potential(job.pot_func, 0.0, x, job.pot_params)

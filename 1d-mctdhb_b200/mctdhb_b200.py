@@ -54,7 +54,7 @@ EXPORTED = [
     "mctdhb_solver_device_coef", "mctdhb_solver_device_orbitals", "mctdhb_solver_time",
     "mctdhb_solver_set_orthogonality", "mctdhb_solver_overlap_residual",
     "mctdhb_solver_eig_residual", "mctdhb_solver_lowest_state", "mctdhb_solver_set_derivative",
-    "mctdhb_solver_set_coef_method",
+    "mctdhb_solver_set_coef_method", "mctdhb_solver_set_orb_method",
 ]
 
 _lib = None
@@ -180,6 +180,8 @@ def load(path=LIB_PATH):
     L.mctdhb_solver_set_derivative.argtypes = [vp, i]
     L.mctdhb_solver_set_coef_method.restype = i
     L.mctdhb_solver_set_coef_method.argtypes = [vp, i]
+    L.mctdhb_solver_set_orb_method.restype = i
+    L.mctdhb_solver_set_orb_method.argtypes = [vp, i]
     L.mctdhb_solver_overlap_residual.restype = i
     L.mctdhb_solver_overlap_residual.argtypes = [vp, C.POINTER(d)]
     L.mctdhb_solver_eig_residual.restype = i
@@ -418,6 +420,11 @@ class Solver:
         """coefficient integrator: 20 short iterative Lanczos, 21 Runge-Kutta"""
         _check(load().mctdhb_solver_set_coef_method(self.h, int(coef_method)),
                "mctdhb_solver_set_coef_method")
+
+    def set_orb_method(self, orb_method):
+        """orbital integrator: 30 full-step Runge-Kutta, 31 split step"""
+        _check(load().mctdhb_solver_set_orb_method(self.h, int(orb_method)),
+               "mctdhb_solver_set_orb_method")
 
     def set_orthogonality(self, robust):
         """projector of the orbital equation: False simple, True robust"""

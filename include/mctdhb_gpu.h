@@ -216,6 +216,10 @@ int  mctdhb_solver_set_derivative(mctdhb_solver s, int der_method);
  * (src/integrator/coefficients_integration.c:29-57, the solver's order;
  * order 2 takes the RK5 tableau as the reference does). */
 int  mctdhb_solver_set_coef_method(mctdhb_solver s, int coef_method);
+/* Orbital integrator, as the reference's orb_integ_method
+ * (src/integrator/driver.c:165-173): 30 FULLSTEP_RUNGEKUTTA (default),
+ * 31 SPLITSTEP (src/integrator/orbital_integration.c:352-434). */
+int  mctdhb_solver_set_orb_method(mctdhb_solver s, int orb_method);
 int  mctdhb_solver_overlap_residual(mctdhb_solver s, double* res);
 int  mctdhb_solver_eig_residual(mctdhb_solver s, double e, double* res);
 int  mctdhb_solver_lowest_state(mctdhb_solver s, int niter, double* e);

@@ -204,6 +204,68 @@ def test_dropin_methods_step_vs_reference(gpu, reference, imag, der, coef):
         reference.destroy_mctdhb(B)
 
 
+@pytest.mark.parametrize("der,imag,periodic,rk", [(302, True, True, 5), (302, False, True, 4),
+                                                  (302, False, False, 5), (302, True, False, 4),
+                                                  (301, False, True, 5), (300, True, True, 4)])
+def test_solver_splitstep_vs_oracle(gpu, oracle, der, imag, periodic, rk):
+    """split-step orbitals (orbital_integration.c:352-434): half steps as one
+    circulant (periodic) or dense (zero bounds) operator product, h and g of
+    the half-stepped orbitals, RK of the full nonlinear term"""
+    N, M, G, m, dt, g, steps = 5, 3, 64, 5, 0.005, 0.5, 4
+    xi, xf = -8.0, 8.0
+    orb, dx = hermite_orbitals(M, G, xi, xf)
+    coef = rand_coef(np.random.default_rng(60 + rk + der), oracle.dim(N, M))
+    pot = harmonic(G, xi, xf)
+    s = gpu.Solver(N, M, G, xi, xf, dt, imag, rk, m, periodic=periodic)
+    s.set_derivative(der)
+    s.set_orb_method(31)
+    s.set_potential(pot)
+    s.set_interaction(g)
+    s.set_state(orb, coef)
+    st = oracle_init(oracle, N, orb, coef, dx, pot, g)
+    for _ in range(steps):
+        oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, periodic, imag, rk, m, pot, der=der,
+                              orb_method=31)
+    s.step(steps)
+    d = s.get()
+    assert rel_err(d["orb"], st["orb"]) < 1e-10
+    assert rel_err(d["coef"], st["coef"]) < 1e-10
+    assert rel_err(d["rho1"], st["rho1"]) < 1e-10
+    s.close()
+
+
+@pytest.mark.parametrize("imag,periodic", [(True, True), (False, True), (False, False)])
+def test_dropin_splitstep_vs_reference(gpu, reference, imag, periodic):
+    """split-step structs (finite differences: Crank-Nicolson) stepped by the
+    reference and by the GPU drop-in"""
+    import mctdhb_types as T
+
+    N, M, G, m, dt, g = 5, 3, 64, 5, 0.005, 0.5
+    xi, xf = -8.0, 8.0
+    orb, _ = hermite_orbitals(M, G, xi, xf)
+    coef = rand_coef(np.random.default_rng(17), reference.lib.space_dimension(N, M))
+    kw = dict(periodic=periodic, orb=T.SPLITSTEP)
+    A, ka = reference.make_mctdhb(N, M, G, xi, xf, imag, 5, m, dt, 1.0, g, **kw)
+    B, kb = reference.make_mctdhb(N, M, G, xi, xf, imag, 5, m, dt, 1.0, g, **kw)
+    try:
+        reference.set_state(A, orb, coef)
+        reference.set_state(B, orb, coef)
+        L = gpu.load()
+        for k in range(3):
+            reference.step(A, k)
+            ow = np.zeros(M * G, np.complex128)
+            cw = np.zeros(len(coef), np.complex128)
+            L.mctdhb_gpu_clear_error()
+            L.mctdhb_propagate_step(B, T.carray(ow), T.carray(cw), k)
+            assert gpu.last_error() == "", gpu.last_error()
+        a, b = reference.get_state(A), reference.get_state(B)
+        for key in ("orb", "coef", "rho1", "rho2"):
+            assert rel_err(b[key], a[key]) < 1e-10, key
+    finally:
+        reference.destroy_mctdhb(A)
+        reference.destroy_mctdhb(B)
+
+
 @pytest.mark.parametrize("side_stream", [False, True])
 def test_solver_energy_follows_steps_on_any_stream(gpu, oracle, side_stream):
     """energy() read right after step() -- no other synchronisation -- is the
