@@ -775,6 +775,21 @@ def run_single(mb, torch, name, steps, warmup):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def combine_ranks(dist, t_ms, inst, device):
+    """whole-job figures of a multi-rank run: the timed region is the max
+    over ranks, instance-steps are summed (each rank runs its own mix with no
+    collective in the data path)"""
+    if dist is None:
+        return t_ms, inst
+    import torch
+
+    t = torch.tensor([t_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    n = torch.tensor([inst], dtype=torch.float64, device=device)
+    dist.all_reduce(n)
+    return float(t.item()), int(n.item())
+
+
 def run_gpu(args):
     import torch
 
@@ -823,15 +838,7 @@ def run_gpu(args):
     t_ms = e0.elapsed_time(e1)
     _, state, s1, energy = b.poll()
     inst = int(np.sum(s1.astype(np.int64) - s0.astype(np.int64)))
-    if dist is not None:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-        n = torch.tensor([inst], device="cuda", dtype=torch.float64)
-        dist.all_reduce(n)
-        inst_all = int(n.item())
-    else:
-        inst_all = inst
+    t_ms, inst_all = combine_ranks(dist, t_ms, inst, "cuda")
     value = inst_all / (t_ms / 1000.0)
     kernels = b.kernels
     line = {
