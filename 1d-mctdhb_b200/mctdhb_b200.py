@@ -644,11 +644,20 @@ class Batch:
             raise MctdhbError(f"mctdhb_batch_poll: {last_error()}")
         return n, st, steps, en
 
-    def fetch(self, slot):
+    def fetch(self, slot, out=None):
+        """the slot's state; `out`: optional dict of destination arrays
+        (orb, coef, rho1, rho2; e.g. views of pinned host memory)"""
         N, M, G = self.jobs[slot]
         dim = int(load().space_dimension(N, M))
-        out = {"orb": np.zeros((M, G), np.complex128), "coef": np.zeros(dim, np.complex128),
-               "rho1": np.zeros((M, M), np.complex128), "rho2": np.zeros(M ** 4, np.complex128)}
+        if out is None:
+            out = {"orb": np.zeros((M, G), np.complex128),
+                   "coef": np.zeros(dim, np.complex128),
+                   "rho1": np.zeros((M, M), np.complex128),
+                   "rho2": np.zeros(M ** 4, np.complex128)}
+        for k, n in (("orb", M * G), ("coef", dim), ("rho1", M * M), ("rho2", M ** 4)):
+            a = out[k]
+            if a.dtype != np.complex128 or a.size != n or not a.flags.c_contiguous:
+                raise ValueError(f"fetch: out[{k!r}] must be {n} contiguous complex128")
         e = C.c_double()
         steps = C.c_uint32()
         conv = C.c_int()
