@@ -87,8 +87,11 @@ def test_realtime_sweep_and_ramp_vs_reference(gpu, reference, tmp_path):
         reference.destroy_mctdhb(ms)
 
 
-@pytest.mark.parametrize("der", [D.FINITEDIFF, D.DVR])
-def test_imagtime_final_diagonalisation_vs_reference(gpu, reference, tmp_path, der):
+@pytest.mark.parametrize("der,orb_m,coef_m", [(D.FINITEDIFF, D.FULLSTEP_RUNGEKUTTA, D.LANCZOS),
+                                              (D.DVR, D.FULLSTEP_RUNGEKUTTA, D.LANCZOS),
+                                              (D.FINITEDIFF, D.SPLITSTEP, D.RUNGEKUTTA)])
+def test_imagtime_final_diagonalisation_vs_reference(gpu, reference, tmp_path, der, orb_m,
+                                                     coef_m):
     N, M, G, dt, tend = 6, 3, 64, 0.01, 0.1
     xi, xf = -8.0, 8.0
     line = f"{N} {M} {G} {xi} {xf} {dt} {tend} -0.5 0.0 linear_ramp 0.5 0.5 0 0 0 " \
@@ -98,10 +101,12 @@ def test_imagtime_final_diagonalisation_vs_reference(gpu, reference, tmp_path, d
     coef = rand_coef(np.random.default_rng(10), dim)
     inp, out = str(tmp_path / "in"), str(tmp_path / "out")
     write_inputs(inp, "it", [line], orb, coef)
-    info = D.run_jobs("it", inp, out, integrator=dict(IT, der_method=der))
+    info = D.run_jobs("it", inp, out,
+                      integrator=dict(IT, der_method=der, orb_method=orb_m, coef_method=coef_m))
     nsteps = steps_for(tend, dt)
     assert info[0]["steps"] == nsteps and not info[0]["converged"]
-    ms, keep = reference.make_mctdhb(N, M, G, xi, xf, True, 5, 5, dt, 1.0, 0.5, der=der)
+    ms, keep = reference.make_mctdhb(N, M, G, xi, xf, True, 5, 5, dt, 1.0, 0.5, der=der,
+                                     orb=orb_m, coef=coef_m)
     try:
         reference.set_state(ms, orb, coef)
         for k in range(nsteps):
