@@ -26,6 +26,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <complex>
 #include <vector>
 
 #include "../../include/mctdhb_gpu.h"
@@ -48,11 +49,22 @@ size_t al256(size_t b) { return (b + 255) / 256 * 256; }
 struct JobLayout {
     uint32_t nc = 0, D1 = 0, D2 = 0;
     int vtiles = 0, ytiles = 0, gs[3] = {0, 0, 0}, gk[3] = {0, 0, 0};
-    size_t o_orb, o_stage, o_H, o_pot, o_w, o_Q, o_hob, o_hint, o_pw, o_rho1, o_rho2, o_rinv,
+    size_t o_orb, o_stage, o_H, o_pot, o_w, o_Q, o_hob, o_hint, o_pw, o_lint, o_rho1, o_rho2,
+        o_rinv,
         o_work, o_T, o_sq, o_g, o_V, o_out, o_part, o_py, o_gpart, total;
 };
 
-int job_layout(int N, int M, int G, int lz, JobLayout& L) {
+// der: 0 / 302 finite differences, 300 DVR, 301 spectral (periodic only)
+int job_layout(int N, int M, int G, int lz, int der, int periodic, JobLayout& L) {
+    if (der != 0 && der != kDerFiniteDiff && der != kDerDVR && der != kDerSpectral) {
+        set_error("batch: derivative method %d not in {302, 300, 301}", der);
+        return -1;
+    }
+    const bool toeplitz = der == kDerDVR || der == kDerSpectral;
+    if (toeplitz && !periodic) {
+        set_error("batch: DVR and spectral derivatives need periodic boundaries");
+        return -1;
+    }
     if (M < kBatchMinOrb || M > kBatchMaxOrb) {
         set_error("batch: %d orbitals outside %d..%d", M, kBatchMinOrb, kBatchMaxOrb);
         return -1;
@@ -100,6 +112,7 @@ int job_layout(int N, int M, int G, int lz, JobLayout& L) {
     L.o_hob = take(M2 * z);
     L.o_hint = take(M4 * z);
     L.o_pw = take((P * P + 1) * z);  // + the real-W flag (pairhc_tmpl.cuh)
+    L.o_lint = take(toeplitz ? (2 * (size_t)(G - 1) - 1) * z : 0);
     L.o_rho1 = take(M2 * z);
     L.o_rho2 = take(M4 * z);
     L.o_rinv = take(M2 * z);
@@ -447,7 +460,9 @@ extern "C" {
 size_t mctdhb_batch_job_bytes(const mctdhb_job* job, int lanczos_iter) {
     if (!job) return 0;
     JobLayout L;
-    if (job_layout(job->npar, job->norb, job->grid_size, lanczos_iter, L)) return 0;
+    if (job_layout(job->npar, job->norb, job->grid_size, lanczos_iter, job->der_method,
+                   job->periodic, L))
+        return 0;
     return L.total;
 }
 
@@ -576,7 +591,9 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     const double reg = job->reg_fac > 0 ? job->reg_fac : 1e-9;
     std::lock_guard<std::mutex> lk(b->mu);
     JobLayout L;
-    if (job_layout(job->npar, job->norb, job->grid_size, b->lz, L)) return -1;
+    if (job_layout(job->npar, job->norb, job->grid_size, b->lz, job->der_method, job->periodic,
+                   L))
+        return -1;
     int s = -1;
     for (int i = 0; i < b->max_slots; i++)
         if (!b->hs[i].used) {
@@ -626,6 +643,8 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     d.ov.tf = d.imag ? make_double2(0.0, -1.0) : make_double2(1.0, 0.0);
     d.ov.w = (const double*)P(L.o_w);
     d.ov.pot = (const double*)P(L.o_pot);
+    const bool toeplitz = job->der_method == kDerDVR || job->der_method == kDerSpectral;
+    d.ov.lin_t = toeplitz ? (const double2*)P(L.o_lint) : nullptr;
     d.sp.N = N;
     d.sp.M = M;
     d.sp.dim = L.nc;
@@ -658,6 +677,11 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     std::vector<double> sq(N + 3);
     for (int x = 0; x < N + 3; x++) sq[x] = std::sqrt((double)x);
     const std::vector<double> w = simpson_weights(G, d.ov.dx);
+    // DVR / spectral: the Toeplitz kernel of the solver's orbital step
+    const std::vector<double2> lint =
+        toeplitz ? derivative_toeplitz(job->der_method, G, d.ov.dx, d.ov.a2,
+                                       std::complex<double>(d.ov.a1.x, d.ov.a1.y))
+                 : std::vector<double2>();
     int fl[BF_TOTAL] = {0};
     fl[BF_STATE] = SLOT_RUNNING;
     cudaStream_t st = b->st;
@@ -673,6 +697,8 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
         cudaMemcpyAsync((void*)d.ov.pot, job->pot, G * sizeof(double), cudaMemcpyHostToDevice,
                         st) ||
         cudaMemcpyAsync((void*)d.ov.w, w.data(), G * sizeof(double), cudaMemcpyHostToDevice, st) ||
+        (toeplitz && cudaMemcpyAsync((void*)d.ov.lin_t, lint.data(), lint.size() * sizeof(double2),
+                                     cudaMemcpyHostToDevice, st)) ||
         cudaMemcpyAsync((void*)d.sp.T, T.data(), T.size() * sizeof(uint32_t),
                         cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync((void*)d.sp.sq, sq.data(), sq.size() * sizeof(double),

@@ -49,7 +49,8 @@ __device__ void bt_rhs(const BatchSlot& S, const double2* __restrict__ y, double
     const double2* Q = S.Q;
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
         const int k = t / G, x = t % G;
-        const double2 lin = linear_at(o, y + (size_t)k * G, x);
+        const double2 lin = o.lin_t ? toeplitz_at(o, y + (size_t)k * G, x)
+                                    : linear_at(o, y + (size_t)k * G, x);
         double2 fx[kBatchMaxOrb];
         for (int a = 0; a < M; a++) fx[a] = y[(size_t)a * G + x];
         const double2* Qk = Q + (size_t)k * M * M * M;

@@ -571,8 +571,8 @@ int orb_periodic(const OrbCtx& c, double2* orb, cudaStream_t st) {
 //     circulant of FFT -> (i freq a1 - freq^2 a2) -> inverse FFT with
 //     1/sqrt(n) both ways: t[d + n - 1] = c[(-d) mod n],
 //     c[e] = sum_m mult_m e^{2 pi i m e / n} / n.
-static std::vector<double2> derivative_toeplitz(int der, int G, double dx, double a2,
-                                                std::complex<double> a1) {
+std::vector<double2> derivative_toeplitz(int der, int G, double dx, double a2,
+                                         std::complex<double> a1) {
     using cd = std::complex<double>;
     const int n = G - 1;
     const double pi = 3.14159265358979323846, len = n * dx;

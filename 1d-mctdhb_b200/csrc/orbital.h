@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <complex>
 #include <vector>
 
 #include "common.cuh"
@@ -25,6 +26,11 @@ struct OrbView {
 
 // derivative methods of the orbital equation (mctdhb_types.h OrbDerivative)
 constexpr int kDerDVR = 300, kDerSpectral = 301, kDerFiniteDiff = 302;
+
+// Toeplitz kernel (2(G-1) - 1 values, a2 and a1 folded in) of the DVR or
+// spectral linear part on the G - 1 periodic points (orbital.cu)
+std::vector<double2> derivative_toeplitz(int der, int G, double dx, double a2,
+                                         std::complex<double> a1);
 
 struct OrbCtx {
     int M = 0, G = 0;

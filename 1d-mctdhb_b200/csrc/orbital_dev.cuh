@@ -83,6 +83,17 @@ __device__ __forceinline__ double2 linear_at(const OrbView& o, const double2* f,
     return lin;
 }
 
+// DVR / spectral linear part at point x of orbital f (orbital_integration.c:
+// 137-176): sum_j lin_t[j - x + n - 1] f_j + V(x) f(x) on the n = G - 1
+// periodic points, the last point repeating the first
+__device__ __forceinline__ double2 toeplitz_at(const OrbView& o, const double2* f, int x) {
+    const int n = o.G - 1, xr = x == n ? 0 : x;
+    const double2* t = o.lin_t + (n - 1 - xr);
+    double2 acc = make_double2(0.0, 0.0);
+    for (int j = 0; j < n; j++) acc = cfma(__ldg(t + j), f[j], acc);
+    return cadd(acc, cscale(f[xr], o.pot[xr]));
+}
+
 // h_kl integrand at x (orbital_matrices.c:22-70):
 //   -a2 conj(f_k') f_l' + a1 conj(f_k) f_l' + V conj(f_k) f_l
 __device__ __forceinline__ double2 hob_integrand(const OrbView& o, const double2* fk,

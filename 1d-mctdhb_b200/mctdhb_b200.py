@@ -72,7 +72,8 @@ class Job(C.Structure):
                 ("imagtime", C.c_int), ("rk_order", C.c_int), ("dt", C.c_double),
                 ("g", C.c_double), ("max_steps", C.c_uint32), ("energy_tol", C.c_double),
                 ("check_every", C.c_int), ("reg_fac", C.c_double),
-                ("pot", C.POINTER(C.c_double)), ("orbitals", C.c_void_p), ("coef", C.c_void_p)]
+                ("pot", C.POINTER(C.c_double)), ("orbitals", C.c_void_p), ("coef", C.c_void_p),
+                ("der_method", C.c_int)]
 
 
 def load(path=LIB_PATH):

@@ -270,6 +270,8 @@ typedef struct {
     const double* pot;          /* grid_size trap values (host) */
     const void*   orbitals;     /* norb x grid_size complex128, row-major (host) */
     const void*   coef;         /* space_dimension(npar, norb) complex128 (host) */
+    int      der_method;        /* linear part: 0 or 302 finite differences, 300 DVR,
+                                 * 301 spectral (periodic grids only) */
 } mctdhb_job;
 
 typedef struct mctdhb_batch_s* mctdhb_batch;

@@ -25,13 +25,13 @@ def harmonic(G, xi, xf, omega=1.0):
     return 0.5 * omega ** 2 * x ** 2
 
 
-def make_job(oracle_dim, N, M, G, imag, rk, dt, g, steps, seed, etol=0.0, check=0):
+def make_job(oracle_dim, N, M, G, imag, rk, dt, g, steps, seed, etol=0.0, check=0, der=302):
     orb, _ = hermite_orbitals(M, G, XI, XF)
     rng = np.random.default_rng(seed)
     return {"npar": N, "norb": M, "grid_size": G, "xi": XI, "xf": XF, "periodic": 1,
             "imagtime": int(imag), "rk_order": rk, "dt": dt, "g": g, "max_steps": steps,
             "energy_tol": etol, "check_every": check, "pot": harmonic(G, XI, XF),
-            "orbitals": orb, "coef": rand_coef(rng, oracle_dim(N, M))}
+            "orbitals": orb, "coef": rand_coef(rng, oracle_dim(N, M)), "der_method": der}
 
 
 def oracle_init(oracle, N, orb, coef, dx, pot, g):
@@ -53,7 +53,12 @@ MIX = [  # N, M, G, imag, rk, dt, g, steps
     (7, 5, 80, True, 5, 0.01, 0.2, 5),
     (6, 7, 96, True, 5, 0.01, 0.3, 3),
     (5, 8, 64, False, 5, 0.005, 0.2, 3),
+    (6, 4, 96, True, 5, 0.005, 0.4, 4),
+    (5, 3, 128, False, 4, 0.005, 0.6, 4),
 ]
+# derivative method of the jobs (the rest: finite differences): DVR and
+# spectral linear parts as the device Toeplitz sum of the orbital step
+DER = {8: 300, 9: 301}
 
 
 def test_batch_mix_vs_oracle(gpu, oracle):
@@ -63,7 +68,7 @@ def test_batch_mix_vs_oracle(gpu, oracle):
     b = gpu.Batch(16, 256 << 20, m)
     jobs, slots = [], []
     for i, (N, M, G, imag, rk, dt, g, steps) in enumerate(MIX):
-        job = make_job(oracle.dim, N, M, G, imag, rk, dt, g, steps, 900 + i)
+        job = make_job(oracle.dim, N, M, G, imag, rk, dt, g, steps, 900 + i, der=DER.get(i, 302))
         jobs.append(job)
         slots.append(b.admit(job))
     assert None not in slots
@@ -75,7 +80,8 @@ def test_batch_mix_vs_oracle(gpu, oracle):
         dx = (XF - XI) / (G - 1)
         st = oracle_init(oracle, N, job["orbitals"], job["coef"], dx, job["pot"], g)
         for _ in range(nst):
-            oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, imag, rk, m, job["pot"])
+            oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, True, imag, rk, m, job["pot"],
+                                  der=job["der_method"])
         d = b.fetch(s)
         assert rel_err(d["orb"], st["orb"]) < 1e-10, (N, M)
         assert rel_err(d["coef"], st["coef"]) < 1e-10, (N, M)
@@ -100,7 +106,7 @@ def test_batch_same_bits_alone_and_in_a_changing_mix(gpu, oracle):
     target = make_job(oracle.dim, 10, 4, 128, True, 5, 0.01, 0.5, 12, 31)
     alone = run_alone(gpu, target, 12)
     b = gpu.Batch(12, 512 << 20, 5)
-    others = [make_job(oracle.dim, N, M, G, imag, rk, dt, g, n, 50 + i)
+    others = [make_job(oracle.dim, N, M, G, imag, rk, dt, g, n, 50 + i, der=DER.get(i, 302))
               for i, (N, M, G, imag, rk, dt, g, n) in enumerate(MIX)]
     # two jobs ahead of the target, so it lands in a different slot
     early = [b.admit(others[0]), b.admit(others[4])]
@@ -113,6 +119,7 @@ def test_batch_same_bits_alone_and_in_a_changing_mix(gpu, oracle):
     b.release(early[0])  # a stopped job leaves
     b.step(4)
     late.append(b.admit(others[5]))
+    late.append(b.admit(others[8]))  # a DVR job joins
     b.step(10)
     d = b.fetch(s)
     assert d["steps"] == 12

@@ -123,3 +123,25 @@ def test_batch_job_bytes_host():
         B.Batch.job_bytes(job(10, 9, 128), 5)  # the engine runs 2..8 orbitals
     with pytest.raises(B.MctdhbError):
         B.Batch.job_bytes(job(1, 4, 128), 5)  # and at least two bosons
+
+
+def test_batch_job_derivative_method_host():
+    """DVR / spectral jobs hold a Toeplitz kernel of 2(G-1)-1 complex values
+    in the arena; zero bounds and unknown methods are rejected"""
+    import mctdhb_b200 as B
+
+    def job(der, periodic=1, G=256):
+        return {"npar": 10, "norb": 3, "grid_size": G, "xi": -8.0, "xf": 8.0,
+                "periodic": periodic, "imagtime": 1, "rk_order": 5, "dt": 0.01, "g": 0.5,
+                "max_steps": 10, "pot": np.zeros(G), "orbitals": np.zeros((3, G), np.complex128),
+                "coef": np.zeros(1, np.complex128), "der_method": der}
+
+    fd = B.Batch.job_bytes(job(302), 5)
+    assert B.Batch.job_bytes(job(0), 5) == fd  # 0: finite differences
+    for der in (300, 301):
+        extra = B.Batch.job_bytes(job(der), 5) - fd
+        assert 16 * (2 * 255 - 1) <= extra < 16 * (2 * 255 - 1) + 256
+    with pytest.raises(B.MctdhbError):
+        B.Batch.job_bytes(job(300, periodic=0), 5)
+    with pytest.raises(B.MctdhbError):
+        B.Batch.job_bytes(job(303), 5)
