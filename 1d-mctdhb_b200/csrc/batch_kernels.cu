@@ -304,13 +304,18 @@ __global__ void __launch_bounds__(kBatchVecThreads)
 #pragma unroll
     for (int k = 0; k <= I; k++) acc[k] = make_double2(0.0, 0.0);
     BT_ROWS(r) {
+        // every Krylov value is loaded before the store to out (which may
+        // alias V as far as the compiler knows), V[I] once
+        double2 v[I + 1];
+#pragma unroll
+        for (int k = 0; k <= I; k++) v[k] = S.V[(size_t)k * nc + r];
         double2 o = S.out[r];
-        const double2 av = cmul(alpha, S.V[(size_t)I * nc + r]);
+        const double2 av = cmul(alpha, v[I]);
         o.x -= av.x;
         o.y -= av.y;
         S.out[r] = o;
 #pragma unroll
-        for (int k = 0; k <= I; k++) acc[k] = cfma_conj(S.V[(size_t)k * nc + r], o, acc[k]);
+        for (int k = 0; k <= I; k++) acc[k] = cfma_conj(v[k], o, acc[k]);
     }
 #pragma unroll
     for (int k = 0; k <= I; k++) {
