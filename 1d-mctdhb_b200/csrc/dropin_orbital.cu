@@ -179,7 +179,7 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
         c->key = key;
     }
     mctdhb_solver s = c->s;
-    const size_t n = (size_t)M * G, M2 = (size_t)M * M, M4 = M2 * M2;
+    const size_t n = (size_t)M * G, M2 = (size_t)M * M;
     const size_t nc = psi->space_dim;
     c->stage.resize(std::max(n, M2));
     // state in: orbitals, coefficients, rho2, rho1^{-1}; trap, g, factor
@@ -217,11 +217,16 @@ void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coe
     if (mctdhb_solver_get(s, orbh.data(), psi->coef, hob.data(), psi->hint, rho1.data(),
                           psi->tb_denmat, rinv.data()))
         return;
+    // std::complex<double> is laid out as two doubles, like double2
     for (int k = 0; k < M; k++) {
-        std::memcpy(psi->orbitals[k], orbh.data() + (size_t)k * G, G * sizeof(double2));
-        std::memcpy(psi->hob[k], hob.data() + (size_t)k * M, M * sizeof(double2));
-        std::memcpy(psi->ob_denmat[k], rho1.data() + (size_t)k * M, M * sizeof(double2));
-        std::memcpy(psi->inv_ob_denmat[k], rinv.data() + (size_t)k * M, M * sizeof(double2));
+        std::memcpy(static_cast<void*>(psi->orbitals[k]), orbh.data() + (size_t)k * G,
+                    G * sizeof(double2));
+        std::memcpy(static_cast<void*>(psi->hob[k]), hob.data() + (size_t)k * M,
+                    M * sizeof(double2));
+        std::memcpy(static_cast<void*>(psi->ob_denmat[k]), rho1.data() + (size_t)k * M,
+                    M * sizeof(double2));
+        std::memcpy(static_cast<void*>(psi->inv_ob_denmat[k]), rinv.data() + (size_t)k * M,
+                    M * sizeof(double2));
     }
     if (orb_works &&
         cudaMemcpy(orb_works, mctdhb_solver_orb_next(s), n * sizeof(double2),
