@@ -488,3 +488,33 @@ def test_relaxation_n10_m4_grid256(gpu, oracle):
     that envelope."""
     e, e_ref, d, st = relax(gpu, oracle, 256)
     assert abs(e - e_ref) < 5e-8 * abs(e_ref), (e, e_ref)
+
+
+@pytest.mark.parametrize("orb_method", [30, 31])
+def test_large_grid_dvr_equals_spectral(gpu, orb_method):
+    """4097 points: the Toeplitz (full step) and half-step (split step)
+    kernels stage 64 KB of orbital in shared memory.  With d1coef = 0 the DVR
+    matrix and the spectral derivative are one operator, so the two runs
+    agree to rounding"""
+    # explicit RK on the full step needs dt * (pi / dx)^2 / 2 below ~2 (dt
+    # 5e-6 here); the split step's linear part is exact
+    N, M, G, g, steps = 4, 3, 4097, 0.5, 3
+    dt = 5e-6 if orb_method == 30 else 5e-4
+    xi, xf = -10.0, 10.0
+    orb, _ = hermite_orbitals(M, G, xi, xf)
+    coef = rand_coef(np.random.default_rng(5), gpu.load().space_dimension(N, M))
+    pot = harmonic(G, xi, xf)
+    out = []
+    for der in (300, 301):
+        s = gpu.Solver(N, M, G, xi, xf, dt, False, 4, 5)
+        s.set_derivative(der)
+        s.set_orb_method(orb_method)
+        s.set_potential(pot)
+        s.set_interaction(g)
+        s.set_state(orb, coef)
+        s.step(steps)
+        out.append(s.get())
+        s.close()
+    assert np.isfinite(out[0]["orb"]).all()
+    assert rel_err(out[0]["orb"], out[1]["orb"]) < 1e-10
+    assert rel_err(out[0]["coef"], out[1]["coef"]) < 1e-10
