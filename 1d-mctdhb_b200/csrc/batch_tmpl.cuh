@@ -186,19 +186,19 @@ constexpr size_t batch_y_smem() {
 
 template <int M>
 int batch_prepare() {
-    static bool done = false;
-    if (done) return 0;
-    MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bhcp_y_kernel<M>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)batch_y_smem<M>()));
-    MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 2>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         gram_smem(M, 2)));
-    MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 1>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         gram_smem(M, 1)));
-    done = true;
-    return 0;
+    static std::atomic<uint64_t> done{0};
+    return set_attributes_once(done, []() -> int {
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bhcp_y_kernel<M>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)batch_y_smem<M>()));
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 2>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             gram_smem(M, 2)));
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 1>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             gram_smem(M, 1)));
+        return 0;
+    });
 }
 
 template <int M>

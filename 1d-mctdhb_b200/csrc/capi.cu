@@ -39,6 +39,11 @@ void set_error(const char* fmt, ...) {
 const char* last_error() { return g_err.c_str(); }
 void clear_error() { g_err.clear(); }
 
+std::mutex& attr_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+
 }  // namespace mctdhb
 
 using namespace mctdhb;

@@ -17,7 +17,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 namespace mctdhb {
@@ -164,6 +166,25 @@ __device__ __forceinline__ double2 cscale(double2 a, double r) {
 }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) {
     return make_double2(a.x + b.x, a.y + b.y);
+}
+
+// Function attributes such as the dynamic shared-memory limit above 48 KB
+// belong to one device: a set-once guard keeps one bit per device (the
+// device current at the call) and takes a process-wide lock, so the first
+// call on every device sets them and host threads calling at once do not
+// race on the flag.  `set` returns 0 on success.
+std::mutex& attr_mutex();
+template <class F>
+int set_attributes_once(std::atomic<uint64_t>& done, F&& set) {
+    int dev = 0;
+    MCTDHB_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(attr_mutex());
+    if (dev < 0 || dev >= 64) return set();  // no bit for it: set on every call
+    const uint64_t bit = 1ull << dev;
+    if (done.load(std::memory_order_acquire) & bit) return 0;
+    if (set()) return -1;
+    done.fetch_or(bit, std::memory_order_release);
+    return 0;
 }
 
 inline int num_sms() {

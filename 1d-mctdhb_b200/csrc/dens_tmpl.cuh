@@ -178,13 +178,14 @@ int dens_launch_variant(const SpaceView& sp, const double2* C, double2* partial,
                         cudaStream_t st) {
     constexpr int EP = (dens_nelem(M) + 7) / 8 * 8;
     const size_t smem = (size_t)(DENS_BLOCK / 32) * EP * sizeof(double2);
-    static bool attr = false;
-    if (!attr) {
-        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(dens_kernel<M, SYNC, MINB>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem));
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr{0};
+    if (set_attributes_once(attr, [&]() -> int {
+            MCTDHB_CUDA_TRY(cudaFuncSetAttribute(dens_kernel<M, SYNC, MINB>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem));
+            return 0;
+        }))
+        return -1;
     if (grid == 0) return 0;  // attributes only (before graph capture)
     dens_kernel<M, SYNC, MINB><<<grid, DENS_BLOCK, smem, st>>>(sp, C, partial);
     MCTDHB_CUDA_TRY(cudaGetLastError());

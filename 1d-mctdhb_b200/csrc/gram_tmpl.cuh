@@ -322,17 +322,16 @@ int gram_launch(const SpaceView& sp, uint32_t Dp, const double2* C, double2* par
 // launch attributes (dynamic shared memory beyond 48 KB), before any capture
 template <int M>
 int gram_prepare_tmpl() {
-    static bool done = false;
-    if (!done) {
+    static std::atomic<uint64_t> done{0};
+    return set_attributes_once(done, []() -> int {
         MCTDHB_CUDA_TRY(cudaFuncSetAttribute(gram_kernel<M, 2>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              gram_smem(M, 2)));
         MCTDHB_CUDA_TRY(cudaFuncSetAttribute(gram_kernel<M, 1>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              gram_smem(M, 1)));
-        done = true;
-    }
-    return 0;
+        return 0;
+    });
 }
 
 template <int M>

@@ -94,6 +94,61 @@ __host__ __device__ void for_each_density_element(int M, Fn&& f) {
 }
 
 
+// The same enumeration split into independent tasks, so many threads can
+// write the element list at once: task t < M writes rho1[t][t] and
+// rho2[tttt]; the next M(M-1)/2 tasks, one per pair k<l, write rho2[klkl]
+// and the M+1 single-move elements of (k,l); the last M(M+1)/2 tasks, one
+// per source pair k<=s, write that pair's doubles.  Every element lands at
+// its index in for_each_density_element's order (offsets in closed form).
+__host__ __device__ constexpr int dens_ntasks(int M) { return M + M * (M - 1) / 2 + M * (M + 1) / 2; }
+
+template <class Fn>
+__host__ __device__ void density_element_task(int M, int t, Fn&& f) {
+    const int npair = M * (M - 1) / 2;
+    if (t < M) {
+        f(t, D_R1_DIAG, t, t, t, t);
+        f(M + t, D_R2_KKKK, t, t, t, t);
+        return;
+    }
+    t -= M;
+    if (t < npair) {
+        int k = 0, r = t;  // t-th pair k<l in lexicographic order
+        while (r >= M - 1 - k) r -= M - 1 - k, k++;
+        const int l = k + 1 + r;
+        f(2 * M + t, D_R2_KSKS, k, l, k, l);
+        int e = 2 * M + npair + t * (M + 1);
+        f(e++, D_R1_OFF, k, l, k, l);
+        f(e++, D_R2_KKKL, k, k, k, l);
+        f(e++, D_R2_KLLL, k, l, l, l);
+        for (int s = 0; s < M; s++)
+            if (s != k && s != l) f(e++, D_R2_KSSL, k, s, s, l);
+        return;
+    }
+    t -= npair;
+    // t-th source pair k<=s; doubles of the pairs before it
+    int e = 2 * M + npair + npair * (M + 1);
+    int k = 0, s = 0;
+    for (int u = 0;; u++) {
+        if (u == t) break;
+        e += (k == s) ? (M - 1 - k) + (M - 1) * (M - 2) / 2 : (M - 2) * (M - 3) / 2;
+        if (++s == M) s = ++k;
+    }
+    for (int q = 0; q < M; q++)
+        for (int l = q; l < M; l++) {
+            if (k == s) {
+                if (q == k || l == k) continue;
+                if (q == l) {
+                    if (q > k) f(e++, D_R2_KKQQ, k, k, q, q);
+                } else {
+                    f(e++, D_R2_KKQL, k, k, q, l);
+                }
+            } else {
+                if (q == l || q == k || q == s || l == k || l == s) continue;
+                f(e++, D_R2_KSQL, k, s, q, l);
+            }
+        }
+}
+
 // Packed H.C coefficient table (layout above) from h (M x M row-major) and
 // g (hint[k + sM + qM^2 + lM^3]); the caller runs it on one thread.
 __device__ inline void hc_pack_table(int M, const double2* __restrict__ hob,

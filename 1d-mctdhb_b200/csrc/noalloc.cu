@@ -100,15 +100,16 @@ __global__ void noalloc_tables_kernel(int N, int M, uint32_t* __restrict__ T,
             sq[i - nT] = sqrt((double)(i - nT));
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int e = 0;
-        for_each_density_element(M, [&](int kind, int k, int s, int q, int l) {
+    // element descriptors: independent tasks (one per orbital, per pair
+    // k<l and per source pair k<=s), so the list is written in parallel
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < dens_ntasks(M);
+         t += gridDim.x * blockDim.x) {
+        density_element_task(M, t, [&](int e, int kind, int k, int s, int q, int l) {
             desc[5 * e] = kind;
             desc[5 * e + 1] = k;
             desc[5 * e + 2] = s;
             desc[5 * e + 3] = q;
             desc[5 * e + 4] = l;
-            e++;
         });
     }
 }
@@ -171,7 +172,7 @@ extern "C" int mctdhb_dev_density_matrices_noalloc(uint16_t npar, uint16_t norb,
     sp.sq = sq;
     cudaStream_t st = (cudaStream_t)stream;
 
-    const int ntab = rows * (N + 1) + N + 3;
+    const int ntab = std::max(rows * (N + 1) + N + 3, dens_ntasks(M));
     noalloc_tables_kernel<<<std::max(1, std::min(64, (ntab + 255) / 256)), 256, 0, st>>>(
         N, M, T, sq, desc);
     MCTDHB_CUDA_TRY(cudaGetLastError());

@@ -397,14 +397,13 @@ __global__ void __launch_bounds__(256)
 
 template <int M>
 int hcp_prepare_tmpl() {
-    static bool done = false;
-    if (!done) {
+    static std::atomic<uint64_t> done{0};
+    return set_attributes_once(done, []() -> int {
         MCTDHB_CUDA_TRY(cudaFuncSetAttribute(hcp_y_kernel<M>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)PairHcShape<M>::SMEM));
-        done = true;
-    }
-    return 0;
+        return 0;
+    });
 }
 
 template <int M>

@@ -105,12 +105,21 @@ void set_orbital_hint(OrbitalEquation eq_desc, uint16_t norb, Cmatrix orb, Carra
 /* include/integrator/synchronize.h:45 (synchronize.c:35) */
 void sync_orbital_matrices(OrbitalEquation eq_desc, ManyBodyState psi);
 /* include/integrator/driver.h:67 (driver.c:159): one full step on the GPU.
- * Supported integrator settings: FULLSTEP_RUNGEKUTTA orbitals with
- * FINITEDIFF derivatives (RK2 / RK4 / RK5 as the named tableaux Heun,
- * classical RK4 and Butcher RK5), LANCZOS coefficients, the simple
- * projector.  Other settings are reported as errors.  orb_works receives
- * the orbitals after the Runge-Kutta step, coef_works the Lanczos
- * combination before the imaginary-time renormalisation. */
+ * Supported integrator settings (every method of the reference):
+ *   orbitals      FULLSTEP_RUNGEKUTTA (RK2 / RK4 / RK5 as the named tableaux
+ *                 Heun, classical RK4 and Butcher RK5) or SPLITSTEP
+ *                 (orbital_integration.c:352-434: Crank-Nicolson or FFT
+ *                 exponential half steps around a Runge-Kutta step of the
+ *                 nonlinear part);
+ *   derivatives   DVR (the reference's default), SPECTRAL or FINITEDIFF;
+ *   coefficients  LANCZOS (needs coef_workspace->lan_work) or RUNGEKUTTA
+ *                 (coefficients_integration.c:29-57; order 2 runs the RK5
+ *                 tableau, as the reference's switch does);
+ *   projector     the simple one, or the robust one when
+ *                 orb_workspace->impr_ortho is set.
+ * Any other orbital or coefficient method is reported as an error.
+ * orb_works receives the orbitals after the orbital step, coef_works the
+ * coefficient combination before the imaginary-time renormalisation. */
 void mctdhb_propagate_step(MCTDHBDataStruct mctdhb, Carray orb_works, Carray coef_works,
                            uint32_t curr_step);
 
@@ -245,8 +254,8 @@ int mctdhb_dev_double_jump_map(mctdhb_space sp, int diff, void* d_strides, void*
 /* The reference integrates one system per process (driver.c:205-330; its
  * globals driver.c:15-19 make it single-instance).  These calls have no
  * counterpart there: each admitted job is one such integration (the step of
- * mctdhb_propagate_step, driver.c:159-201, FULLSTEP_RUNGEKUTTA + FINITEDIFF
- * + LANCZOS), and all running jobs advance together, one CUDA graph launch
+ * mctdhb_propagate_step, driver.c:159-201, with FULLSTEP_RUNGEKUTTA orbitals,
+ * FINITEDIFF, DVR or SPECTRAL derivatives and LANCZOS coefficients), and all running jobs advance together, one CUDA graph launch
  * per step of the whole batch.  A job stops on the device after max_steps
  * steps or, in imaginary time, by the reference's energy rule checked every
  * check_every steps (driver.c:47-67 without the eigen-residual test):

@@ -3,7 +3,10 @@ m = hbar = 1) as a fixture: the harmonic-trap block (V = x^2 / 2) and the
 harmonic + Gaussian barrier block (V = x^2 / 2 + b^2 exp(-x^2 / 2c^2),
 b = 3, c = 0.5).  The ring block is left out (its ring length is not given).
 
-    python tests/golden/make_benchmark_fixture.py /root/reference/benchmark.dat
+    python tests/golden/make_benchmark_fixture.py [path/to/benchmark.dat]
+
+The default path is benchmark.dat of the reference tree named by
+$MCTDHB_REFERENCE, else of the `reference` folder beside this repository.
 """
 import json
 import os
@@ -29,7 +32,9 @@ def parse(path):
 
 
 if __name__ == "__main__":
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/benchmark.dat"
+    repo = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    ref = os.environ.get("MCTDHB_REFERENCE") or os.path.join(os.path.dirname(repo), "reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ref, "benchmark.dat")
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "benchmark_known_answers.json")
     with open(out, "w") as f:
         json.dump({"source": "benchmark.dat of the reference", **parse(src)}, f, indent=1)

@@ -6,8 +6,9 @@ library, shared by every call.
 
 The entry point is called through the C ABI and checked against
 mctdhb_dev_density_matrices (which owns its scratch through an mctdhb_space)
-on two calls in a row, with a different coefficient vector each time, so
-the second call sees the array as the first one left it.  This file is named
+and against the oracle, on two calls in a row, with a different coefficient
+vector each time, so the second call sees the array as the first one left
+it.  This file is named
 to be collected last: the array then holds whatever earlier tests' calls
 left in it, and the test also passes alone in a fresh process."""
 import ctypes as C
@@ -72,6 +73,28 @@ def test_noalloc_matches_density_matrices(gpu, N, M):
             assert rel_err(got2, want2) < TOL, f"rho2, call {call}"
     finally:
         L.mctdhb_space_destroy(h)
+
+
+# against the oracle directly: the capped grid of the register-resident
+# kernel (30, 6), and the generic kernel whose grid is set by what fits in
+# the array (3 particles in 20 orbitals; 2 in 25, the largest norb that fits)
+ORACLE_SIZES = [(10, 4), (30, 6), (3, 20), (2, 25)]
+
+
+@pytest.mark.parametrize("N,M", ORACLE_SIZES)
+def test_noalloc_matches_oracle(gpu, oracle, N, M):
+    import torch
+
+    L = gpu.load()
+    dim = oracle.dim(N, M)
+    rng = np.random.default_rng(4300 + 31 * N + M)
+    for call in range(2):
+        c = rand_coef(rng, dim)
+        got1, got2 = _densities(L, (N, torch.from_numpy(c).cuda()), M, noalloc=True)
+        want1 = oracle.onebody_dm(N, M, c).reshape(-1)
+        want2 = oracle.twobody_dm(N, M, c)
+        assert rel_err(got1, want1) < TOL, f"rho1, call {call}"
+        assert rel_err(got2, want2) < TOL, f"rho2, call {call}"
 
 
 def test_noalloc_rejects_oversize_and_null(gpu):
