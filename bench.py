@@ -287,8 +287,102 @@ def workload_config(args, jobs):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle's C restatement on a sample of the jobs
+# CPU baseline: the compiled reference's own step on a sample of the jobs
 # ---------------------------------------------------------------------------
+REF_SAMPLE = 24     # jobs of the mix stepped by the reference arm
+CPU_SAMPLE = 12     # jobs of the mix stepped for the GPU arm's cpu_baseline
+
+
+def step_bytes(j, m=LZ):
+    """algorithmic bytes of one full step of a job: m H.C launches
+    (32 nc + 16 G each) and the densities (16 nc + 16 G)"""
+    nc, G = dim(j["npar"], j["norb"]), distinct_couplings(j["npar"], j["norb"])
+    return m * (32.0 * nc + 16.0 * G) + 16.0 * nc + 16.0 * G
+
+
+def systematic_sample(jobs, n):
+    """n jobs at evenly spaced ranks of the mix sorted by step cost
+    (algorithmic bytes), largest first: the heavy-tailed mix (its 25 largest
+    jobs carry ~85% of the bytes) is represented in proportion, from the
+    largest jobs to the smallest"""
+    order = sorted(range(len(jobs)), key=lambda i: -step_bytes(jobs[i]))
+    return [order[int((k + 0.5) * len(jobs) / n)] for k in range(n)]
+
+
+def sample_cost_ratio(jobs, idx):
+    """mean step bytes of the sampled jobs over the mean of the whole mix:
+    the sample's throughput estimates the mix's within about this factor"""
+    return (sum(step_bytes(jobs[i]) for i in idx) / len(idx)) / \
+        (sum(step_bytes(j) for j in jobs) / len(jobs))
+
+
+class RefTimer:
+    """The compiled reference (oracle/_ref: the reference's own C sources,
+    OpenMP) stepping jobs of the mix one at a time, each by the reference's
+    own mctdhb_propagate_step (driver.c:159-201).  A job's struct comes from
+    oracle/ref_setup.c (the reference's sub-constructors, maps from the
+    oracle's OpenMP builders) and its initial synchronisation from the
+    reference (sync_orbital_matrices, sync_density_matrices); set-up is
+    timed apart, only the step is the measured work."""
+
+    def __init__(self):
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        from oracle import Reference
+
+        self.R = Reference()
+        self.setup_s = 0.0
+
+    def threads(self, n=None):
+        if n is not None:
+            self.R.lib.omp_set_num_threads(int(n))
+        return int(self.R.lib.omp_get_max_threads())
+
+    def step_job(self, j):
+        import ctypes
+
+        import mctdhb_types as T
+
+        R = self.R
+        t0 = time.perf_counter()
+        ms = R.make_job_struct(j, LZ)
+        if ms is None:
+            raise RuntimeError(f"reference cannot map N={j['npar']} M={j['norb']}")
+        try:
+            R.set_state(ms, j["orbitals"], j["coef"])
+            ow = np.zeros(j["norb"] * j["grid_size"], np.complex128)
+            cw = np.zeros(dim(j["npar"], j["norb"]), np.complex128)
+            self.setup_s += time.perf_counter() - t0
+            t1 = time.perf_counter()
+            R.lib.mctdhb_propagate_step(ms, T.carray(ow), T.carray(cw), ctypes.c_uint32(0))
+            return time.perf_counter() - t1
+        finally:
+            R.destroy_job_struct(ms)
+
+    def map_build(self, j):
+        """seconds of the reference's own serial map build
+        (get_multiconf_struct, types_definition.c:111-142) and of the
+        oracle's parallel one used for set-up, on one job"""
+        R = self.R
+        out = {}
+        for name, fn in (("reference_serial_s", R.lib.get_multiconf_struct),
+                         ("setup_parallel_s", R.lib.refset_multiconf)):
+            t0 = time.perf_counter()
+            mc = fn(j["npar"], j["norb"])
+            out[name] = time.perf_counter() - t0
+            R.lib.destroy_multiconf_struct(mc)
+        out["job"] = f"N={j['npar']} M={j['norb']} (nc={dim(j['npar'], j['norb'])})"
+        return out
+
+
+def port_step(O, j):
+    """seconds of one full step of the oracle's C restatement on a job"""
+    st, dx = oracle_state(O, j)
+    t0 = time.perf_counter()
+    O.propagate_step(st, j["npar"], dx, j["dt"], -0.5, 0.0, j["g"], True, bool(j["imagtime"]),
+                     j["rk_order"], LZ, j["pot"])
+    return time.perf_counter() - t0
+
+
 def oracle_state(O, j):
     orb = np.ascontiguousarray(j["orbitals"].copy())
     G = j["grid_size"]
@@ -301,121 +395,105 @@ def oracle_state(O, j):
             "rinv": np.ascontiguousarray(ri)}, dx
 
 
-def step_bytes(j, m=LZ):
-    """algorithmic bytes of one full step of a job: m H.C launches
-    (32 nc + 16 G each) and the densities (16 nc + 16 G)"""
-    nc, G = dim(j["npar"], j["norb"]), distinct_couplings(j["npar"], j["norb"])
-    return m * (32.0 * nc + 16.0 * G) + 16.0 * nc + 16.0 * G
+def ref_sample_desc(jobs, idx, threads, what):
+    return (f"{what}: one full step (RK5 orbitals, h, g, SIL({LZ}), rho1, rho2) of each of "
+            f"{len(idx)} jobs of the {len(jobs)}-job mix at evenly spaced ranks of step cost, "
+            f"by the compiled reference's own mctdhb_propagate_step (OpenMP, {threads} host "
+            f"threads); set-up (maps, initial densities) not timed; sample mean step bytes "
+            f"{sample_cost_ratio(jobs, idx):.3f} x the mix mean")
 
 
-class CpuEstimate:
-    """CPU time of one full step of the whole mix, estimated from full oracle
-    steps of a stratified sample of its jobs.
-
-    The cost of a job's step is heavy-tailed in its size (at N ~ U{10..60},
-    M in {3..6} the 25 largest of 256 jobs hold ~85% of the algorithmic
-    bytes), so the jobs are split into the TOP largest by step_bytes and the
-    rest; each stratum's CPU seconds per algorithmic byte is measured on the
-    jobs sampled from it (ratio estimator) and applied to the stratum's total
-    bytes.  Each sampled job runs one complete oracle step (orbitals, h, g,
-    SIL, rho1, rho2); its set-up (initial densities) is not timed."""
-    TOP = 25
-
-    def __init__(self, jobs, seed):
-        sys.path.insert(0, os.path.join(REPO, "oracle"))
-        from oracle import Oracle
-
-        self.O = Oracle()
-        self.jobs = jobs
-        self.rng = np.random.default_rng(seed)
-        order = sorted(range(len(jobs)), key=lambda i: -step_bytes(jobs[i]))
-        self.strata = {"large": order[:self.TOP], "rest": order[self.TOP:]}
-        self.total = {h: sum(step_bytes(jobs[i]) for i in ix) for h, ix in self.strata.items()}
-        self.t = {h: 0.0 for h in self.strata}
-        self.b = {h: 0.0 for h in self.strata}
-        self.n = {h: 0 for h in self.strata}
-        self.queue = {h: [] for h in self.strata}
-
-    def _draw(self, h):
-        if not self.queue[h]:
-            self.queue[h] = self.rng.permutation(self.strata[h]).tolist()
-        return self.queue[h].pop()
-
-    def _run(self, h, i):
-        j = self.jobs[i]
-        st, dx = oracle_state(self.O, j)
-        t0 = time.perf_counter()
-        self.O.propagate_step(st, j["npar"], dx, j["dt"], -0.5, 0.0, j["g"], True,
-                              bool(j["imagtime"]), j["rk_order"], LZ, j["pot"])
-        dt = time.perf_counter() - t0
-        self.t[h] += dt
-        self.b[h] += step_bytes(j)
-        self.n[h] += 1
-        return dt
-
-    def sample(self, n_large=1, rest_budget_s=3.0):
-        """one bounded round: n_large jobs of the large stratum, then jobs of
-        the rest until rest_budget_s seconds of their steps"""
-        for _ in range(n_large):
-            self._run("large", self._draw("large"))
-        spent = 0.0
-        while spent < rest_budget_s:
-            spent += self._run("rest", self._draw("rest"))
-
-    def seconds_per_mix_step(self):
-        return sum(self.t[h] / self.b[h] * self.total[h] for h in self.strata if self.b[h] > 0)
-
-    def value(self):
-        return len(self.jobs) / self.seconds_per_mix_step()
-
-    def describe(self):
-        return {h: {"jobs_in_stratum": len(self.strata[h]), "jobs_timed": self.n[h],
-                    "seconds": self.t[h], "s_per_gb": self.t[h] / self.b[h] * 1e9}
-                for h in self.strata if self.n[h]}
-
-
-def cpu_sample(jobs, seed=5):
-    """the oracle's C restatement (OpenMP, all host threads) on a bounded
-    stratified sample of the mix, scaled to instance-steps/s"""
-    est = CpuEstimate(jobs, seed)
-    est.sample(n_large=1, rest_budget_s=4.0)
-    cores = os.cpu_count()
-    return {"value": est.value(), "unit": "instance-steps/s", "cores": cores, "kind": "port",
-            "seconds": sum(est.t.values()), "strata": est.describe(),
-            "sample": f"full oracle steps (RK5 orbitals, h, g, SIL({LZ}), rho1, rho2; C "
-                      f"restatement, OpenMP on {cores} host threads) of 1 job drawn from the "
-                      f"{CpuEstimate.TOP} largest and of jobs from the rest for ~4 s; each "
-                      f"stratum's seconds per algorithmic byte scaled to its total bytes"}
+def cpu_sample(jobs):
+    """the GPU arm's cpu_baseline: the compiled reference on a bounded
+    systematic sample of the mix, all host threads"""
+    rt = RefTimer()
+    idx = systematic_sample(jobs, CPU_SAMPLE)
+    t = sum(rt.step_job(jobs[i]) for i in idx)
+    threads = rt.threads()
+    return {"value": len(idx) / t, "unit": "instance-steps/s", "cores": threads,
+            "kind": "reference", "seconds": t, "setup_seconds": rt.setup_s,
+            "sample": ref_sample_desc(jobs, idx, threads, "measured")}
 
 
 def run_reference(args):
-    """the reference arm: the oracle port on the host cores, same metric"""
+    """the reference arm: the compiled reference's own step on the host
+    cores, same metric (instance-steps/s of the batched mix).  The K timed
+    steps share a systematic sample of REF_SAMPLE jobs (step s takes the
+    sample's jobs s, s+K, ...); value = job-steps done / seconds of the
+    reference's steps.  Rank 0 only."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     jobs = mix_jobs()
-    warm = CpuEstimate(jobs, seed=100)
+    rt = RefTimer()
+    cores = rt.threads()
+    idx = systematic_sample(jobs, max(REF_SAMPLE, args.steps))
+    small = min(idx, key=lambda i: step_bytes(jobs[i]))
     for _ in range(args.warmup):
-        warm.sample(n_large=0, rest_budget_s=0.5)
-    est = CpuEstimate(jobs, seed=5)
-    for _ in range(args.steps):
-        est.sample(n_large=1, rest_budget_s=2.0)
-    v = est.value()
-    cores = os.cpu_count()
-    base = {"value": v, "unit": "instance-steps/s", "cores": cores, "kind": "port",
-            "seconds": sum(est.t.values()), "strata": est.describe(),
-            "sample": f"per timed step: a full oracle step (C restatement, OpenMP on {cores} "
-                      f"host threads) of 1 job drawn from the {CpuEstimate.TOP} largest of the "
-                      f"mix and of jobs from the rest for ~2 s; pooled over {args.steps} steps, "
-                      f"each stratum's seconds per algorithmic byte scaled to its total bytes"}
+        rt.step_job(jobs[small])
+    per_step = [0.0] * args.steps
+    done = 0
+    for s in range(args.steps):
+        for i in idx[s::args.steps]:
+            per_step[s] += rt.step_job(jobs[i])
+            done += 1
+    total = sum(per_step)
+    v = done / total
+    base = {"value": v, "unit": "instance-steps/s", "cores": cores, "kind": "reference",
+            "seconds": total, "setup_seconds": rt.setup_s,
+            "sample": ref_sample_desc(jobs, idx, cores, f"per timed step, 1/{args.steps} of")}
+    # the reference application's default of half the host threads
+    # (apps/mctdhb_main.c:138), on every fourth job of the sample
+    half = max(1, cores // 2)
+    rt.threads(half)
+    sub = idx[::4]
+    th = sum(rt.step_job(jobs[i]) for i in sub)
+    rt.threads(cores)
+    th_all = sum(rt.step_job(jobs[i]) for i in sub)
+    maps = rt.map_build(jobs[idx[len(idx) // 2]])
+    # the oracle's C restatement against the reference, same jobs
+    from oracle import Oracle
+
+    O = Oracle()
+    calib = []
+    for i in (idx[2], idx[len(idx) // 2], idx[-2]):
+        j = jobs[i]
+        tr, tp = rt.step_job(j), port_step(O, j)
+        calib.append({"job": f"N={j['npar']} M={j['norb']} G={j['grid_size']}",
+                      "reference_s": tr, "port_s": tp, "reference_over_port": tr / tp})
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "instance-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * MIX_N / v, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": workload_config(args, jobs), "cpu_baseline": base,
+        "half_threads": {"threads": half, "value": len(sub) / th, "jobs": len(sub),
+                         "unit": "instance-steps/s",
+                         "what": "the reference application's default thread count "
+                                 "(apps/mctdhb_main.c:138), every fourth sampled job",
+                         "all_threads_value_same_jobs": len(sub) / th_all},
+        "map_build": maps, "port_vs_reference": calib,
         "e2e": {"value": v, "unit": "instance-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def run_reference_full_mix(args):
+    """one complete step of all 256 jobs of the mix by the compiled
+    reference (long: minutes), with the systematic samples' estimates
+    beside it"""
+    jobs = mix_jobs()
+    rt = RefTimer()
+    t = [rt.step_job(j) for j in jobs]
+    full = len(jobs) / sum(t)
+    out = {"impl": "reference", "what": "one complete step of the whole mix, compiled reference",
+           "value": full, "unit": "instance-steps/s", "seconds": sum(t),
+           "setup_seconds": rt.setup_s, "cores": rt.threads()}
+    for n in (CPU_SAMPLE, REF_SAMPLE):
+        ix = systematic_sample(jobs, n)
+        est = n / sum(t[i] for i in ix)
+        out[f"sample_{n}"] = {"value": est, "rel_error": est / full - 1.0,
+                              "cost_ratio": sample_cost_ratio(jobs, ix)}
+    print(json.dumps(out), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -998,6 +1076,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--ref-full-mix", action="store_true",
+                    help="with --impl reference: one complete step of the whole mix by the "
+                         "compiled reference, against its sampled estimates")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="timed steps per job on the plain one-at-a-time path")
@@ -1017,6 +1098,8 @@ def main():
         run_profile()
     elif args.profile_kernels:
         run_profile_kernels(args.profile_kernels)
+    elif args.impl == "reference" and args.ref_full_mix:
+        run_reference_full_mix(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -338,6 +338,14 @@ class Reference:
         L.Csimps.restype = T.dcomplex
         L.Csimps.argtypes = [C.c_uint32, C.c_double, T.Carray]
         L.dxFD.argtypes = [C.c_uint32, C.c_double, T.Carray, T.Carray]
+        # ref_setup.c: reference structs with maps from the oracle's builders
+        L.refset_multiconf.restype = T.MultiConfiguration
+        L.refset_multiconf.argtypes = [C.c_uint16, C.c_uint16]
+        L.refset_mctdhb_struct.restype = T.MCTDHBDataStruct
+        L.refset_mctdhb_struct.argtypes = [C.c_int] * 6 + [
+            C.c_uint16, C.c_uint16, C.c_int, C.c_double, C.c_double, C.c_uint16, C.c_double,
+            C.c_double, C.c_double, C.c_double, _f64p, C.c_double]
+        L.refset_destroy.argtypes = [T.MCTDHBDataStruct]
 
     def multiconf(self, N, M):
         return self.lib.get_multiconf_struct(N, M)
@@ -450,6 +458,25 @@ class Reference:
 
     def destroy_mctdhb(self, ms):
         self.lib.destroy_mctdhb_struct(ms)
+
+    def make_job_struct(self, job, lanczos_m, der=T.FINITEDIFF, coef=T.LANCZOS,
+                        orb=T.FULLSTEP_RUNGEKUTTA):
+        """A reference MCTDHBDataStruct for a job dict (the batched engine's
+        fields: npar, norb, grid_size, xi, xf, periodic, imagtime, rk_order,
+        dt, g, pot), built by ref_setup.c: the reference's own
+        sub-constructors with maps from the oracle's OpenMP builders, no DVR
+        matrix unless der is DVR.  None where the reference's 32-bit map
+        layout would overflow.  Free with destroy_job_struct."""
+        d1 = complex(job.get("d1coef", 0j))
+        ms = self.lib.refset_mctdhb_struct(
+            int(job["imagtime"]), coef, orb, der, int(job["rk_order"]), lanczos_m,
+            int(job["npar"]), int(job["norb"]), int(job.get("periodic", 1)), job["xi"], job["xf"],
+            int(job["grid_size"]), job["dt"], job.get("d2coef", -0.5), d1.real, d1.imag,
+            np.ascontiguousarray(job["pot"], np.float64), job["g"])
+        return ms if ms else None
+
+    def destroy_job_struct(self, ms):
+        self.lib.refset_destroy(ms)
 
 
 def hermite_orbitals(M, G, xi, xf):
