@@ -185,7 +185,7 @@ struct mctdhb_batch_s {
 namespace {
 
 int* cnt_vec(int* c) { return c; }
-constexpr int kCntInts = kBatchCntInts;
+constexpr int kCntInts = kBatchCntAll;  // with the monitor flags
 
 void drop_graph(mctdhb_batch_s* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -363,7 +363,9 @@ int enqueue_step(mctdhb_batch_s* b, unsigned mask) {
     const int* nV = cnt_vec(b->d_cnt);
     const int vgrid = num_sms() * 8, sgrid = b->max_slots;
     const int lz = b->lz;
-    bt_orbital_kernel<<<sgrid, kBatchOrbThreads, kBatchMaxGrid * sizeof(double), st>>>(S, sl, nL, 0);
+    int* mon = batch_mon(b->d_cnt);
+    bt_orbital_kernel<<<sgrid, kBatchOrbThreads, kBatchMaxGrid * sizeof(double), st>>>(S, sl, nL, 0,
+                                                                                       mon);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     auto hc = [&](int iter) {
         return per_group(b, mask, [&](int M, cudaStream_t s) {
@@ -398,7 +400,14 @@ int enqueue_step(mctdhb_batch_s* b, unsigned mask) {
                               s);
         }))
         return -1;
-    bt_tail_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 0);
+    bt_tail_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 0, mon);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    // the monitor: the eigen residual of the slots whose energy rule passed
+    // in this step with eig_tol set (driver.c:47-67); every launch returns at
+    // once when no slot of its orbital count needs it
+    if (hc(kBatchMonIter)) return -1;
+    bt_resid_kernel<<<vgrid, kBatchVecThreads, 0, st>>>(S, V, nV);
+    bt_monitor_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -588,6 +597,10 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
         set_error("mctdhb_batch_admit: need dt > 0 and at least one step");
         return -1;
     }
+    if (job->eig_tol < 0 || job->ortho_tol < 0 || job->ortho_tol > kOverlapAbort) {
+        set_error("mctdhb_batch_admit: need eig_tol >= 0 and 0 <= ortho_tol <= %g", kOverlapAbort);
+        return -1;
+    }
     const double reg = job->reg_fac > 0 ? job->reg_fac : 1e-9;
     std::lock_guard<std::mutex> lk(b->mu);
     JobLayout L;
@@ -633,6 +646,8 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     d.dt = job->dt;
     d.etol = job->energy_tol;
     d.reg_fac = reg;
+    d.eig_tol = job->eig_tol > 0 ? job->eig_tol : 0.0;
+    d.ortho_tol = job->ortho_tol > 0 ? job->ortho_tol : kOrthoSwitch;
     d.pdt = d.imag ? make_double2(0.0, -job->dt) : make_double2(job->dt, 0.0);
     d.ov.M = M;
     d.ov.G = G;
@@ -684,6 +699,7 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
                  : std::vector<double2>();
     int fl[BF_TOTAL] = {0};
     fl[BF_STATE] = SLOT_RUNNING;
+    fl[BF_ROBUST] = job->impr_ortho ? 1 : 0;
     cudaStream_t st = b->st;
     auto undo = [&]() {
         arena_give(b, h.off, h.bytes);
@@ -732,12 +748,12 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
         return undo();
     }
     bt_orbital_kernel<<<1, kBatchOrbThreads, kBatchMaxGrid * sizeof(double), st>>>(
-        b->d_slots, pl + 1, pl, 1);
+        b->d_slots, pl + 1, pl, 1, nullptr);
     if (prepare_group(M) ||
         dens_group(M, b->d_slots, b->d_pro_g, b->d_pro_g + kBatchMaxSlices, dpc, pl + 1, pl, 1,
                    st))
         return undo();
-    bt_tail_kernel<<<1, kBatchVecThreads, 0, st>>>(b->d_slots, pl + 1, pl, 1);
+    bt_tail_kernel<<<1, kBatchVecThreads, 0, st>>>(b->d_slots, pl + 1, pl, 1, nullptr);
     const cudaError_t e = cudaGetLastError();
     const cudaError_t e2 = cudaStreamSynchronize(st);
     if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -849,6 +865,77 @@ int mctdhb_batch_release(mctdhb_batch b, int slot) {
     arena_give(b, h.off, h.bytes);
     h = HostSlot();
     b->lists_dirty = true;
+    return 0;
+}
+
+int mctdhb_batch_monitor(mctdhb_batch b, int slot, double* overlap_res, double* eig_res,
+                         int* robust) {
+    if (!b || slot < 0 || slot >= b->max_slots || !b->hs[slot].used) {
+        set_error("mctdhb_batch_monitor: no job in slot %d", slot);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    const BatchSlot& d = b->hs[slot].d;
+    int fl[BF_TOTAL];
+    double2 sc[BS_TOTAL];
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(fl, d.flags, sizeof(fl), cudaMemcpyDeviceToHost, b->st));
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(sc, d.scal, sizeof(sc), cudaMemcpyDeviceToHost, b->st));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(b->st));
+    if (overlap_res) *overlap_res = sc[BS_MISC + 5].x;
+    if (eig_res) *eig_res = sc[BS_MISC + 6].x;
+    if (robust) *robust = fl[BF_ROBUST] | (fl[BF_ROBFAIL] << 1);
+    return 0;
+}
+
+int mctdhb_batch_lowest_state(mctdhb_batch b, int slot, int niter, double* energy) {
+    if (!b || slot < 0 || slot >= b->max_slots || !b->hs[slot].used || niter < 0 ||
+        niter > 64) {
+        set_error("mctdhb_batch_lowest_state: no job in slot %d or niter %d outside 0..64", slot,
+                  niter);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    HostSlot& h = b->hs[slot];
+    const BatchSlot& d = h.d;
+    int fl[BF_TOTAL];
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(fl, d.flags, sizeof(fl), cudaMemcpyDeviceToHost, b->st));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(b->st));
+    if (fl[BF_STATE] == SLOT_RUNNING) {
+        set_error("mctdhb_batch_lowest_state: the job in slot %d is still running", slot);
+        return -1;
+    }
+    // driver.c:41-46: min(nc / 2, 50) iterations, none below 4 configurations
+    int it = niter;
+    if (it == 0) it = d.nc < 4 ? 0 : (int)std::min<uint32_t>(d.nc / 2, 50u);
+    double e = 0.0;
+    if (it > 0) {
+        SpaceCtx sc;
+        sc.N = d.N;
+        sc.M = d.M;
+        sc.dim = d.nc;
+        sc.view = d.sp;
+        LanczosWork w;
+        double* d_e = nullptr;
+        int rc = hcp_prepare(d.M) || lanczos_alloc(w, sc, it);
+        if (!rc && cudaMalloc(&d_e, sizeof(double)) != cudaSuccess) {
+            set_error("mctdhb_batch_lowest_state: cudaMalloc failed");
+            rc = -1;
+        }
+        if (!rc) rc = lowest_state(sc, w, d.V, it, d_e, b->st);
+        if (!rc && (cudaMemcpyAsync(&e, d_e, sizeof(double), cudaMemcpyDeviceToHost, b->st) ||
+                    cudaStreamSynchronize(b->st))) {
+            set_error("mctdhb_batch_lowest_state: %s", cudaGetErrorString(cudaGetLastError()));
+            rc = -1;
+        }
+        lanczos_free(w);
+        if (d_e) cudaFree(d_e);
+        if (rc) return -1;
+    } else {
+        double2 sc[BS_TOTAL];
+        MCTDHB_CUDA_TRY(cudaMemcpy(sc, d.scal, sizeof(sc), cudaMemcpyDeviceToHost));
+        e = sc[BS_MISC + 3].x;
+    }
+    if (energy) *energy = e;
     return 0;
 }
 

@@ -25,6 +25,7 @@ constexpr int kBatchMaxSlices = 1024;  // Gram slices per slot and annihilation 
 constexpr int kBatchMaxLz = 16;        // Lanczos vectors per step
 constexpr int kBatchMinOrb = 2, kBatchMaxOrb = 8;
 constexpr int kBatchMaxGrid = 4096;
+constexpr int kBatchMonIter = -1;  // H.C launch of the monitor (eigen residual)
 constexpr int kBatchOrbThreads = 512;
 
 // per-slot device scalars (double2 units)
@@ -32,7 +33,9 @@ constexpr int BS_DIAG = 0;
 constexpr int BS_OFFD = kBatchMaxLz;
 constexpr int BS_ORTHO = 2 * kBatchMaxLz;
 constexpr int BS_Y = 3 * kBatchMaxLz;
-// [0] max beta, [1] 1/beta, [2] |C|^2, [3] energy, [4] previous E/N (stop rule)
+// [0] max beta, [1] 1/beta, [2] |C|^2, [3] energy, [4] previous E/N (stop rule),
+// [5] overlap residual of the orbitals (real time), [6] eigen residual
+// max_i |E C_i - (H C)_i| / N at its last evaluation (imaginary time)
 constexpr int BS_MISC = 4 * kBatchMaxLz;
 constexpr int BS_Z = BS_MISC + 8;  // kBatchMaxLz^2 doubles of eigenvectors
 constexpr int BS_TOTAL = BS_Z + kBatchMaxLz * kBatchMaxLz / 2;
@@ -45,9 +48,17 @@ constexpr int BF_STATE = 3;  // SLOT_*
 constexpr int BF_STEPS = 4;  // steps done
 constexpr int BF_CONV = 5;   // 1: stopped by the energy rule
 constexpr int BF_INFO = 6;   // rho1 inverse status
-constexpr int BF_TOTAL = 8;
+constexpr int BF_ROBUST = 7; // robust projector of the orbital equation on
+constexpr int BF_MON = 8;    // eigen residual due in this step (monitor H.C)
+constexpr int BF_ROBFAIL = 9;  // singular overlap matrix met by the robust projector
+constexpr int BF_TOTAL = 10;
 
-constexpr int SLOT_EMPTY = 0, SLOT_RUNNING = 1, SLOT_DONE = 2;
+// SLOT_ABORTED: real time, overlap residual above the reference's critical
+// value (REALTIME_OVERLAP_RESIDUE_TOL, driver.c:89-95, where the reference
+// exits; the engine stops that job alone)
+constexpr int SLOT_EMPTY = 0, SLOT_RUNNING = 1, SLOT_DONE = 2, SLOT_ABORTED = 3;
+constexpr double kOverlapAbort = 1e-3;     // REALTIME_OVERLAP_RESIDUE_TOL (driver.h:7)
+constexpr double kOrthoSwitch = 1e-8;      // threshold_impr_ortho (driver.c:19)
 
 struct BatchSlot {
     int N, M, G, imag, rk, check_every, lz, pad0;
@@ -59,6 +70,8 @@ struct BatchSlot {
     uint32_t D1;  // D(N-1, M); D(N-2, M) is sp.dim2
     int pad1;
     double dt, etol, reg_fac;
+    double eig_tol;    // eigen-residual half of the imaginary-time stop rule (0: off)
+    double ortho_tol;  // real time: overlap residual that switches the robust projector on
     double2 pdt;  // SIL time step: dt (real time) or -i dt (imaginary time)
     OrbView ov;   // grid, equation coefficients, Simpson weights, trap
     SpaceView sp; // with the pair matrix sp.pair_w and its scratch sp.pair_y
@@ -89,6 +102,12 @@ constexpr int LIST_G2 = 2;  // rho2 Gram: idx = slice
 constexpr int LIST_G1 = 3;  // rho1 Gram: idx = slice
 constexpr int kBatchLists = 4;
 constexpr int kBatchCntInts = 1 + 2 * kBatchLists * kBatchNumM;
+// after the count block: one flag per orbital count, set in a step when a
+// slot of that count needs the monitor H.C (eigen residual), cleared at the
+// start of every step
+constexpr int kBatchCntAll = kBatchCntInts + kBatchNumM;
+__host__ __device__ inline int* batch_mon(int* c) { return c + kBatchCntInts; }
+__host__ __device__ inline const int* batch_mon(const int* c) { return c + kBatchCntInts; }
 __host__ __device__ inline int* batch_offs(int* c, int list) { return c + 1 + 2 * list * kBatchNumM; }
 __host__ __device__ inline int* batch_cnts(int* c, int list) {
     return c + 1 + (2 * list + 1) * kBatchNumM;
@@ -108,7 +127,8 @@ __host__ __device__ constexpr int batch_pair_rows(int M) {
 // batch_m*.cu: per-M kernels over the tile lists.
 //   hcp_batch_launch   out = H V[iter] (- beta V[iter-1]) of every running
 //                      slot of orbital count M: pair contraction (parts & 1),
-//                      gather-back (parts & 2)
+//                      gather-back (parts & 2); iter = kBatchMonIter: out =
+//                      H V[0] of the slots whose eigen residual is due
 //   gram_batch_launch  rho1 / rho2 of V[0] of the slots of orbital count M
 //                      (`list` / `nlist`: the slots, one finalize block each)
 //   batch_prepare      launch attributes (call before any stream capture)

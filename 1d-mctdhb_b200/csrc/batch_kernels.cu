@@ -38,6 +38,67 @@ __device__ __forceinline__ bool slot_running(const BatchSlot& S) {
 // orbital side, one block per slot
 // ---------------------------------------------------------------------------
 
+// <y_s|y_l> (Simpson) for every s, l into out[s * M + l], one warp per entry
+__device__ void bt_overlaps(const BatchSlot& S, const double2* __restrict__ y, double2* out) {
+    const OrbView& o = S.ov;
+    const int M = o.M, G = o.G;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int p = warp; p < M * M; p += nw) {
+        const int a = p / M, b = p % M;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int x = lane; x < G; x += 32) {
+            const double2 t = cfma_conj(y[(size_t)a * G + x], y[(size_t)b * G + x],
+                                        make_double2(0.0, 0.0));
+            acc.x += o.w[x] * t.x;
+            acc.y += o.w[x] * t.y;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) out[p] = acc;
+    }
+    __syncthreads();
+}
+
+// robust projector (orbital_integration.c:22-92): P <- S^{-1} P with the
+// full overlap matrix S_sl = <y_s|y_l> of the stage orbitals, as the
+// single-system solver does; a singular S keeps the simple projector's P
+// and flags the slot (BF_ROBFAIL)
+__device__ void bt_robust(const BatchSlot& S, const double2* __restrict__ y, double2* sP) {
+    __shared__ double2 sS[kBatchMaxOrb * kBatchMaxOrb], sI[kBatchMaxOrb * kBatchMaxOrb];
+    const int M = S.ov.M;
+    bt_overlaps(S, y, sS);
+    if (threadIdx.x == 0) {
+        if (herm_inverse(M, sS, sI)) {
+            S.flags[BF_ROBFAIL] = 1;
+        } else {
+            double2 t[kBatchMaxOrb * kBatchMaxOrb];
+            for (int a = 0; a < M; a++)
+                for (int k = 0; k < M; k++) {
+                    double2 z = make_double2(0.0, 0.0);
+                    for (int l = 0; l < M; l++) z = cfma(sI[a * M + l], sP[l * M + k], z);
+                    t[a * M + k] = z;
+                }
+            for (int i = 0; i < M * M; i++) sP[i] = t[i];
+        }
+    }
+    __syncthreads();
+}
+
+// overlap residual sum_{k<l} |<f_k|f_l>| / M of the slot's orbitals
+// (integrator_monitor.c:31-42) into scal[BS_MISC + 5], summed in the
+// reference's (k, l) order
+__device__ void bt_overlap_residual(const BatchSlot& S) {
+    __shared__ double2 sS[kBatchMaxOrb * kBatchMaxOrb];
+    const int M = S.ov.M;
+    bt_overlaps(S, S.orb, sS);
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int k = 0; k < M; k++)
+            for (int l = k + 1; l < M; l++) sum += hypot(sS[k * M + l].x, sS[k * M + l].y);
+        S.scal[BS_MISC + 5] = make_double2(sum / M, 0.0);
+    }
+    __syncthreads();
+}
+
 // dy/dt of the orbital equation (orbital_integration.c:179-240) for all
 // orbitals y (M x G): H = linear part + interacting part, overlaps
 // P[s][k] = <y_s|H_k> (simple projector, :95-131), out = -i tf (H - sum_s y_s P[s][k]).
@@ -81,6 +142,7 @@ __device__ void bt_rhs(const BatchSlot& S, const double2* __restrict__ y, double
         if (lane == 0) sP[p] = acc;
     }
     __syncthreads();
+    if (S.flags[BF_ROBUST]) bt_robust(S, y, sP);
     const double2 mi_tf = make_double2(o.tf.y, -o.tf.x);
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
         const int k = t / G, x = t % G;
@@ -213,7 +275,9 @@ __device__ void bt_matrices(const BatchSlot& S) {
 // mode 1: the matrices of the orbitals as given (set-up of a new slot)
 __global__ void __launch_bounds__(kBatchOrbThreads)
     bt_orbital_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
-                      const int* __restrict__ nlist, int mode) {
+                      const int* __restrict__ nlist, int mode, int* __restrict__ mon) {
+    // a new step: no monitor H.C due yet in any orbital count
+    if (mon != nullptr && blockIdx.x == 0 && threadIdx.x < kBatchNumM) mon[threadIdx.x] = 0;
     if ((int)blockIdx.x >= *nlist) return;
     const BatchSlot& S = slots[list[blockIdx.x]];
     if (!slot_running(S)) return;
@@ -238,6 +302,9 @@ __global__ void __launch_bounds__(kBatchOrbThreads)
             __syncthreads();
         }
         bt_periodic(S);
+        // real time: the orbitals' drift from orthonormality, for the
+        // monitor of the tail kernel (driver.c:69-96)
+        if (!S.imag) bt_overlap_residual(S);
     }
     bt_matrices(S);
     __syncthreads();
@@ -526,7 +593,7 @@ __global__ void bt_small_kernel(const BatchSlot* __restrict__ slots, const int* 
 // imaginary-time stop rule as driver.c:229 does).
 __global__ void __launch_bounds__(kBatchVecThreads)
     bt_tail_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
-                   const int* __restrict__ nlist, int prologue) {
+                   const int* __restrict__ nlist, int prologue, int* __restrict__ mon) {
     BT_SLOT
     const int M = S.M;
     if (threadIdx.x == 0) {
@@ -539,22 +606,98 @@ __global__ void __launch_bounds__(kBatchVecThreads)
     S.scal[BS_MISC + 3] = E;
     if (prologue) {
         S.scal[BS_MISC + 4] = make_double2(E.x / S.N, 0.0);
+        S.scal[BS_MISC + 6] = make_double2(-1.0, 0.0);  // no eigen residual yet
         return;
     }
     const int steps = S.flags[BF_STEPS] + 1;
     S.flags[BF_STEPS] = steps;
     int state = SLOT_RUNNING;
-    if (S.imag && S.check_every > 0 && steps % S.check_every == 0) {
-        // driver.c:47-67: |E/N - prev| < tol * prev
+    const bool check = S.check_every > 0 && steps % S.check_every == 0;
+    if (S.imag && check) {
+        // driver.c:47-67: |E/N - prev| < tol * prev, and with eig_tol set the
+        // eigen residual below it: that half is decided by bt_monitor_kernel
+        // after the monitor's H.C of this step
         const double curr = E.x / S.N, prev = S.scal[BS_MISC + 4].x;
         if (fabs(curr - prev) < S.etol * prev) {
-            state = SLOT_DONE;
-            S.flags[BF_CONV] = 1;
+            if (S.eig_tol > 0.0) {
+                S.flags[BF_MON] = 1;
+                mon[S.M] = 1;
+            } else {
+                state = SLOT_DONE;
+                S.flags[BF_CONV] = 1;
+            }
         }
         S.scal[BS_MISC + 4] = make_double2(curr, 0.0);
     }
-    if ((uint32_t)steps >= S.max_steps) state = SLOT_DONE;
+    if (!S.imag && check) {
+        // driver.c:69-96: switch the robust projector on above the
+        // threshold; above the critical residual the reference exits, the
+        // engine stops this job
+        const double o = S.scal[BS_MISC + 5].x;
+        if (o > S.ortho_tol && !S.flags[BF_ROBUST]) S.flags[BF_ROBUST] = 1;
+        if (o > kOverlapAbort) state = SLOT_ABORTED;
+    }
+    if ((uint32_t)steps >= S.max_steps && state == SLOT_RUNNING) state = SLOT_DONE;
     S.flags[BF_STATE] = state;
+}
+
+// max_i |E C_i - (H C)_i| over a vector tile of the slots whose eigen
+// residual is due (integrator_monitor.c:9-28), into part[tile].x
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_resid_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                    const int* __restrict__ ntiles) {
+    __shared__ double sh[kBatchVecThreads];
+    const int nt = *ntiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const BatchTile tl = tiles[t];
+        const BatchSlot& S = slots[tl.slot];
+        if (!S.flags[BF_MON]) continue;  // block-uniform
+        const uint32_t nc = S.nc;
+        const uint32_t r0 = tl.idx * (uint32_t)kBatchVecRows;
+        const double e = S.scal[BS_MISC + 3].x;
+        double m = 0.0;
+        for (uint32_t r = r0 + threadIdx.x; r < nc && r < r0 + kBatchVecRows;
+             r += kBatchVecThreads) {
+            const double2 c = S.V[r], h = S.out[r];
+            m = fmax(m, hypot(e * c.x - h.x, e * c.y - h.y));
+        }
+        sh[threadIdx.x] = m;
+        __syncthreads();
+        for (int o = kBatchVecThreads / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) S.part[tl.idx] = make_double2(sh[0], 0.0);
+        __syncthreads();
+    }
+}
+
+// the eigen-residual half of the imaginary-time stop rule (driver.c:47-67):
+// res = max over the tiles / N; the slot stops (converged) when res is
+// below eig_tol
+__global__ void __launch_bounds__(kBatchVecThreads)
+    bt_monitor_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                      const int* __restrict__ nlist) {
+    __shared__ double sh[kBatchVecThreads];
+    if ((int)blockIdx.x >= *nlist) return;
+    const BatchSlot& S = slots[list[blockIdx.x]];
+    if (!S.flags[BF_MON]) return;
+    double m = 0.0;
+    for (int t = threadIdx.x; t < S.vtiles; t += blockDim.x) m = fmax(m, S.part[t].x);
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    const double res = sh[0] / S.N;
+    S.scal[BS_MISC + 6] = make_double2(res, 0.0);
+    if (res < S.eig_tol) {
+        S.flags[BF_STATE] = SLOT_DONE;
+        S.flags[BF_CONV] = 1;
+    }
+    S.flags[BF_MON] = 0;
 }
 
 #undef BT_SLOT

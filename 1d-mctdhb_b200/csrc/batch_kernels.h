@@ -6,8 +6,10 @@
 
 namespace mctdhb {
 
+// mon: the count block's monitor flags, cleared at the start of a step
+// (mode 0); nullptr for the admission set-up (mode 1)
 __global__ void bt_orbital_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
-                                  const int* __restrict__ nlist, int mode);
+                                  const int* __restrict__ nlist, int mode, int* __restrict__ mon);
 __global__ void bt_dot_kernel(const BatchSlot* __restrict__ slots,
                               const BatchTile* __restrict__ tiles, const int* __restrict__ ntiles,
                               int i);
@@ -36,6 +38,12 @@ __global__ void bt_norm_kernel(const BatchSlot* __restrict__ slots, const int* _
 __global__ void bt_small_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
                                 const int* __restrict__ nlist);
 __global__ void bt_tail_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
-                               const int* __restrict__ nlist, int prologue);
+                               const int* __restrict__ nlist, int prologue, int* __restrict__ mon);
+// the monitor's eigen residual: per-tile maxima, then the per-slot decision
+__global__ void bt_resid_kernel(const BatchSlot* __restrict__ slots,
+                                const BatchTile* __restrict__ tiles,
+                                const int* __restrict__ ntiles);
+__global__ void bt_monitor_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
+                                  const int* __restrict__ nlist);
 
 }  // namespace mctdhb

@@ -16,8 +16,10 @@
 
 namespace mctdhb {
 
-// H.C of this step's Lanczos iteration runs for the slot
-__device__ __forceinline__ bool bt_hc_active(const BatchSlot& S) {
+// H.C of this step's Lanczos iteration runs for the slot; the monitor's
+// H.C (iter == kBatchMonIter) for the slots whose eigen residual is due
+__device__ __forceinline__ bool bt_hc_active(const BatchSlot& S, int iter) {
+    if (iter == kBatchMonIter) return S.flags[BF_MON] != 0;
     return S.flags[BF_STATE] == SLOT_RUNNING && !S.flags[BF_BREAK];
 }
 
@@ -46,15 +48,17 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
     constexpr int WS = PS_::WS;
     double2* Wb = smem;               // two buffers of P x WS
     double2* Ab = smem + 2 * P * WS;  // two buffers of ROWS x PS
+    if (iter == kBatchMonIter && batch_mon(cnt)[M] == 0) return;  // no residual due
     const int nt = batch_cnt(cnt, LIST_HY, M);
     const BatchTile* list = tiles + batch_off(cnt, LIST_HY, M);
+    const int vin = iter < 0 ? 0 : iter;  // input vector V[vin]
     const int t = threadIdx.x;
     const bool producer = t >= PS_::CONSUMERS;
     const int pt = t - PS_::CONSUMERS;
     int wslot[2] = {-1, -1};  // slot whose W each buffer holds (same in every producer)
     auto fill = [&](const BatchTile tl, int buf) {
         const BatchSlot& S = slots[tl.slot];
-        const bool active = bt_hc_active(S);
+        const bool active = bt_hc_active(S, iter);
         if (pt == 0)
             meta[buf] = PairTileMeta{S.sp.pair_y, tl.idx * (uint32_t)ROWS, S.sp.dim2, active,
                                      active && S.sp.pair_w[P * P].x != 0.0};
@@ -63,7 +67,7 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
             pair_stage_w<M>(S.sp.pair_w, Wb + buf * P * WS, pt, PS_::PRODUCERS);
             wslot[buf] = tl.slot;
         }
-        pair_gather<M>(S.sp, S.V + (size_t)iter * S.nc, tl.idx, Ab + (size_t)buf * ROWS * PS, pt,
+        pair_gather<M>(S.sp, S.V + (size_t)vin * S.nc, tl.idx, Ab + (size_t)buf * ROWS * PS, pt,
                        PS_::PRODUCERS);
     };
     BatchTile next{};
@@ -92,19 +96,21 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
 
 // Lanczos H.C of step iteration `iter`, gathered back from Y:
 //   out = H V[iter] - beta_{iter-1} V[iter-1]   (iter > 0)
-//   out = H V[0]                                (iter == 0)
+//   out = H V[0]                                (iter == 0, kBatchMonIter)
 // Slots that stopped, or whose Lanczos recurrence broke down in this step,
-// are skipped (multiconfig_lanczos.c:70-71).
+// are skipped (multiconfig_lanczos.c:70-71); the monitor's launch
+// (kBatchMonIter) takes only the slots whose eigen residual is due.
 template <int M>
 __global__ void __launch_bounds__(kBatchHcRows)
     bhcp_g_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
                   const int* __restrict__ cnt, int iter) {
+    if (iter == kBatchMonIter && batch_mon(cnt)[M] == 0) return;
     const int nt = batch_cnt(cnt, LIST_HG, M);
     const BatchTile* list = tiles + batch_off(cnt, LIST_HG, M);
     for (int k = blockIdx.x; k < nt; k += gridDim.x) {
         const BatchTile tl = list[k];
         const BatchSlot& S = slots[tl.slot];
-        if (!bt_hc_active(S)) continue;
+        if (!bt_hc_active(S, iter)) continue;
         const uint32_t nc = S.nc;
         const uint32_t row = tl.idx + threadIdx.x;
         if (row >= nc) continue;

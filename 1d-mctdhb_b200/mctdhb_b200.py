@@ -40,6 +40,7 @@ EXPORTED = [
     "mctdhb_batch_create", "mctdhb_batch_destroy", "mctdhb_batch_job_bytes",
     "mctdhb_batch_free_bytes", "mctdhb_batch_admit", "mctdhb_batch_step", "mctdhb_batch_sync",
     "mctdhb_batch_poll", "mctdhb_batch_fetch", "mctdhb_batch_release",
+    "mctdhb_batch_monitor", "mctdhb_batch_lowest_state",
     "mctdhb_batch_kernel_count", "mctdhb_batch_stream", "mctdhb_batch_launch_hc",
     "mctdhb_fp64_mma_probe",
     "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
@@ -73,7 +74,8 @@ class Job(C.Structure):
                 ("g", C.c_double), ("max_steps", C.c_uint32), ("energy_tol", C.c_double),
                 ("check_every", C.c_int), ("reg_fac", C.c_double),
                 ("pot", C.POINTER(C.c_double)), ("orbitals", C.c_void_p), ("coef", C.c_void_p),
-                ("der_method", C.c_int)]
+                ("der_method", C.c_int), ("eig_tol", C.c_double), ("ortho_tol", C.c_double),
+                ("impr_ortho", C.c_int)]
 
 
 def load(path=LIB_PATH):
@@ -215,6 +217,10 @@ def load(path=LIB_PATH):
                                      C.POINTER(i)]
     L.mctdhb_batch_release.restype = i
     L.mctdhb_batch_release.argtypes = [vp, i]
+    L.mctdhb_batch_monitor.restype = i
+    L.mctdhb_batch_monitor.argtypes = [vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
+    L.mctdhb_batch_lowest_state.restype = i
+    L.mctdhb_batch_lowest_state.argtypes = [vp, i, i, C.POINTER(d)]
     L.mctdhb_batch_kernel_count.restype = i
     L.mctdhb_batch_kernel_count.argtypes = [vp]
     L.mctdhb_batch_stream.restype = vp
@@ -672,6 +678,22 @@ class Batch:
     def release(self, slot):
         _check(load().mctdhb_batch_release(self.h, slot), "mctdhb_batch_release")
         self.jobs.pop(slot, None)
+
+    def monitor(self, slot):
+        """{'overlap_residual', 'eig_residual', 'robust', 'robust_failed'} of a job"""
+        o, e, r = C.c_double(), C.c_double(), C.c_int()
+        _check(load().mctdhb_batch_monitor(self.h, slot, C.byref(o), C.byref(e), C.byref(r)),
+               "mctdhb_batch_monitor")
+        return {"overlap_residual": o.value, "eig_residual": e.value,
+                "robust": bool(r.value & 1), "robust_failed": bool(r.value & 2)}
+
+    def lowest_state(self, slot, niter=0):
+        """final diagonalisation of a stopped job (0: the reference's
+        iteration count); returns the Lanczos energy"""
+        e = C.c_double()
+        _check(load().mctdhb_batch_lowest_state(self.h, slot, niter, C.byref(e)),
+               "mctdhb_batch_lowest_state")
+        return e.value
 
     @property
     def kernels(self):

@@ -281,6 +281,19 @@ typedef struct {
     const void*   coef;         /* space_dimension(npar, norb) complex128 (host) */
     int      der_method;        /* linear part: 0 or 302 finite differences, 300 DVR,
                                  * 301 spectral (periodic grids only) */
+    /* the reference driver's monitor (driver.c:47-96), every check_every
+     * steps: */
+    double   eig_tol;           /* imaginary time: the energy rule also needs the
+                                 * eigen residual max_i |E C_i - (H C)_i| / N
+                                 * below eig_tol (driver.c:47-67; the reference's
+                                 * default 1e-6); 0: the energy rule alone */
+    double   ortho_tol;         /* real time: overlap residual (integrator_monitor.c:31)
+                                 * above which the robust projector is switched on
+                                 * (driver.c:69-96); 0: the reference's 1e-8.  Above
+                                 * 1e-3 (REALTIME_OVERLAP_RESIDUE_TOL) the job stops
+                                 * with state 3 (the reference exits) */
+    int      impr_ortho;        /* 1: the robust projector from the first step
+                                 * (orbital_integration.c:22-92) */
 } mctdhb_job;
 
 typedef struct mctdhb_batch_s* mctdhb_batch;
@@ -300,8 +313,9 @@ int    mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot);
 int    mctdhb_batch_step(mctdhb_batch b, int nsteps);
 int    mctdhb_batch_sync(mctdhb_batch b);
 /* per slot (arrays of max_slots, each may be NULL): state 0 empty,
- * 1 running, 2 stopped; steps done; current energy.  Returns the number of
- * running jobs (synchronises). */
+ * 1 running, 2 stopped, 3 aborted (real time: overlap residual above 1e-3);
+ * steps done; current energy.  Returns the number of running jobs
+ * (synchronises). */
 int    mctdhb_batch_poll(mctdhb_batch b, int* state, uint32_t* steps, double* energy);
 /* a job's orbitals, coefficients, rho1, rho2 (host, each may be NULL),
  * energy, steps and whether the energy rule stopped it */
@@ -309,6 +323,20 @@ int    mctdhb_batch_fetch(mctdhb_batch b, int slot, void* orbitals, void* coef, 
                           void* rho2, double* energy, uint32_t* steps, int* converged);
 /* frees the slot and its arena range */
 int    mctdhb_batch_release(mctdhb_batch b, int slot);
+/* the monitor of a job (driver.c:47-96): the orbitals' overlap residual at
+ * its last step (real time), the eigen residual at its last evaluation
+ * (imaginary time with eig_tol set; -1 before the first), and in *robust
+ * bit 0 the robust projector on, bit 1 a singular overlap matrix met by it */
+int    mctdhb_batch_monitor(mctdhb_batch b, int slot, double* overlap_res, double* eig_res,
+                            int* robust);
+/* the final diagonalisation of driver.c:295-316 for a stopped job: its
+ * coefficients become the lowest eigenvector of H in its orbitals after
+ * niter Lanczos iterations (0: min(nc / 2, 50), none below 4
+ * configurations, as the reference's get_appropriate_lanczos_iterations);
+ * *energy is the Lanczos energy.  The densities are kept, as there.  The
+ * reference runs it when an imaginary-time run ends at its final time
+ * without converging. */
+int    mctdhb_batch_lowest_state(mctdhb_batch b, int slot, int niter, double* energy);
 int    mctdhb_batch_kernel_count(mctdhb_batch b); /* kernels per step graph */
 /* one launch of the batched H.C of the running jobs with norb orbitals
  * (out = H C of each job, on the engine's stream): parts = 1 the pair
