@@ -150,7 +150,10 @@ def coefficients(nc, rng):
     return c / np.linalg.norm(c)
 
 
-def make_job(rng, N, M, G, imag, steps, xi=BXI, xf=BXF, big=False):
+def make_job(rng, N, M, G, imag, steps, xi=BXI, xf=BXF, big=False, coef_rng=None):
+    """one job: trap (harmonic or double well by a coin), g ~ U(0.01, 1),
+    Hermite-Gaussian orbitals, seeded normalised random coefficients (from
+    coef_rng when given, else from rng after the job's other draws)"""
     dw = bool(rng.random() < 0.5)
     pot = trap(dw, G, xi, xf)
     g = float(rng.uniform(0.01, 1.0))
@@ -159,20 +162,73 @@ def make_job(rng, N, M, G, imag, steps, xi=BXI, xf=BXF, big=False):
             "dt": stable_dt(0.01 if imag else 0.005, G, pot, xi, xf), "g": g,
             "max_steps": int(steps), "energy_tol": 1e-10 if imag else 0.0,
             "check_every": 1 if imag else 0, "pot": pot,
-            "orbitals": hermite_orbitals(M, G, xi, xf), "coef": coefficients(dim(N, M), rng),
+            "orbitals": hermite_orbitals(M, G, xi, xf),
+            "coef": coefficients(dim(N, M), rng if coef_rng is None else coef_rng),
             "big": big}
 
 
-def mix_jobs(n=MIX_N, seed=MIX_SEED, max_steps=5000):
-    """the batched workload: n imaginary-time relaxations of uneven size"""
+def mix_sizes(n=MIX_N, seed=MIX_SEED):
+    """(N, M, grid) of the batched workload's jobs: one seeded stream of
+    sizes, traps and interactions; job i's coefficients come from its own
+    stream (seed, i), so any subset of jobs can be built alone"""
     rng = np.random.default_rng(seed)
-    jobs = []
+    out = []
     for _ in range(n):
         N = int(rng.integers(10, 61))
         M = int(rng.choice([3, 4, 5, 6]))
         G = int(rng.choice(GRIDS))
-        jobs.append(make_job(rng, N, M, G, True, max_steps))
+        rng.random()      # trap coin
+        rng.uniform()     # interaction
+        out.append((N, M, G))
+    return out
+
+
+def mix_jobs(n=MIX_N, seed=MIX_SEED, max_steps=5000, keep=None):
+    """the batched workload: n imaginary-time relaxations of uneven size
+    (only the indices in `keep`, when given, in index order)"""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(n):
+        N = int(rng.integers(10, 61))
+        M = int(rng.choice([3, 4, 5, 6]))
+        G = int(rng.choice(GRIDS))
+        if keep is not None and i not in keep:
+            rng.random()
+            rng.uniform()
+            continue
+        jobs.append(make_job(rng, N, M, G, True, max_steps,
+                             coef_rng=np.random.default_rng([seed, i])))
     return jobs
+
+
+def footprint(N, M, G):
+    """arena bytes of a mix job (mctdhb_batch_job_bytes; finite differences,
+    periodic, Lanczos LZ)"""
+    import mctdhb_b200 as mb
+
+    one = np.zeros(1)
+    return mb.Batch.job_bytes({"npar": N, "norb": M, "grid_size": G, "xi": BXI, "xf": BXF,
+                               "periodic": 1, "imagtime": 1, "rk_order": 5, "dt": 0.01,
+                               "g": 0.5, "max_steps": 1, "pot": one, "orbitals": one,
+                               "coef": one, "der_method": 302}, LZ)
+
+
+def rank_jobs(rank, world):
+    """this rank's jobs: the whole job is MIX_N jobs per rank drawn from one
+    seeded stream (its first MIX_N are the one-GPU mix), assigned to ranks by
+    HBM footprint (partition.by_footprint); every rank computes the same
+    assignment and builds only its own jobs -- no collective"""
+    if world == 1:
+        return mix_jobs(), None
+    import partition
+
+    sizes = mix_sizes(MIX_N * world)
+    fp = [footprint(*x) for x in sizes]
+    share = partition.by_footprint(fp, world)
+    loads = partition.loads(fp, share)
+    info = {"jobs": len(sizes), "rule": "longest-processing-time by mctdhb_batch_job_bytes",
+            "bytes_per_rank_max_over_mean": max(loads) / (sum(loads) / world)}
+    return mix_jobs(n=MIX_N * world, keep=set(share[rank])), info
 
 
 def served_jobs(njobs, seed=77, imag_steps=5000, real_steps=500, big_frac=0.05, nmax=60):
@@ -281,7 +337,9 @@ def workload_config(args, jobs):
                         "1e-10 every step, 5000-step limit, dt=min(0.01, 1.5/lambda_max)",
             "mix": mix_summary(jobs), "seed": MIX_SEED, "lanczos_iter": LZ,
             "step": "one full MCTDHB step of every running system: one CUDA graph launch",
-            "parallelism": f"replicas{args.gpus}: each GPU its own mix, no collective",
+            "parallelism": (f"dp{args.gpus}: {args.gpus} x {MIX_N} jobs of one seeded stream "
+                            "assigned to GPUs by HBM footprint, no collective"
+                            if args.gpus > 1 else "one GPU"),
             "l2": "inputs larger than L2 (the mix holds ~12 GB of coefficient and Krylov "
                   "vectors)"}
 
@@ -914,7 +972,7 @@ def run_gpu(args):
         if dist is not None:
             dist.barrier()
 
-    jobs = mix_jobs(seed=MIX_SEED + rank)
+    jobs, part = rank_jobs(rank, world)
     b = mb.Batch(len(jobs), arena_bytes(mb, jobs), LZ)
     slots = [b.admit(j) for j in jobs]
     assert None not in slots, "the arena is sized for every job"
@@ -951,6 +1009,8 @@ def run_gpu(args):
         "instance_steps": inst_all, "clocks": clk, "gpu_launches": kernels * args.steps,
         "kernels_per_step": kernels,
     }
+    if part is not None:
+        line["partition"] = part
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:

@@ -141,20 +141,11 @@ def test_n100_m6_one_step(gpu, oracle):
 
 def mix_sample(picks):
     """jobs of the batched workload (bench.mix_jobs: seed 2024, 256 jobs) at
-    the given positions, drawn from the same seeded stream (the coefficient
-    vectors of the other jobs are drawn and dropped)"""
+    the given positions, built alone (each job's coefficients have their own
+    seeded stream)"""
     import bench
 
-    rng = np.random.default_rng(bench.MIX_SEED)
-    out = {}
-    for i in range(max(picks) + 1):
-        N = int(rng.integers(10, 61))
-        M = int(rng.choice([3, 4, 5, 6]))
-        G = int(rng.choice(bench.GRIDS))
-        job = bench.make_job(rng, N, M, G, True, 5000)
-        if i in picks:
-            out[i] = job
-    return [out[i] for i in picks]
+    return bench.mix_jobs(n=max(picks) + 1, keep=set(picks))
 
 
 def test_batch_mix_largest_jobs_vs_oracle(gpu, oracle):

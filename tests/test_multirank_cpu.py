@@ -1,9 +1,11 @@
-"""The multi-rank host logic of bench.py, as two gloo ranks on the CPU.
+"""The multi-rank host logic, as two gloo ranks on the CPU.
 
-`bench.py --gpus N` runs one batched mix per rank with no collective in the
-data path (independent systems shard; weak scaling).  What is shared is the
-result: the timed region is the max over ranks, the instance-steps are
-summed, and only rank 0 prints.  The reference arm runs on rank 0 alone.
+`bench.py --gpus N` draws N x 256 jobs from one seeded stream and assigns
+them to ranks by HBM footprint (1d-mctdhb_b200/partition.py), every rank
+computing the same assignment with no collective in the data path
+(independent systems shard; weak scaling).  What is shared is the result:
+the timed region is the max over ranks, the instance-steps are summed, and
+only rank 0 prints.  The reference arm runs on rank 0 alone.
 """
 import os
 import socket
@@ -18,6 +20,79 @@ def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         return s.getsockname()[1]
+
+
+def _partition_worker(rank, world, port, q):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "1d-mctdhb_b200"))
+    import bench
+    import partition
+
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        sizes = bench.mix_sizes(bench.MIX_N * world)
+        # footprint proxy without the library: coefficient and Krylov bytes
+        fp = [(bench.LZ + 1) * 16 * bench.dim(N, M) + 16 * 7 * M * G for N, M, G in sizes]
+        mine = partition.by_footprint(fp, world)[rank]
+        # the assignment every rank computed alone, gathered only to check it
+        allv = [None] * world
+        dist.all_gather_object(allv, (mine, sum(fp[i] for i in mine)))
+        q.put((rank, allv, fp))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_footprint_partition_over_two_gloo_ranks():
+    """every job of the 2 x 256-job stream lands on exactly one rank, and
+    each rank's footprint is within mean + largest job"""
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_partition_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+            pytest.fail("a rank did not finish")
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(2))
+    (r0, allv, fp), (r1, allv1, _) = res
+    assert allv == allv1  # both ranks saw the same assignment
+    idx = sorted(i for share, _ in allv for i in share)
+    assert idx == list(range(len(fp)))  # each job exactly once
+    mean = sum(fp) / 2
+    for _, load in allv:
+        assert load <= mean + max(fp)
+    assert max(load for _, load in allv) / mean < 1.05  # LPT on a 512-job stream
+
+
+def test_partition_rules_on_the_cpu():
+    sys.path.insert(0, os.path.join(REPO, "1d-mctdhb_b200"))
+    import partition
+
+    sizes = [5, 9, 1, 7, 3, 3, 8, 2]
+    share = partition.by_footprint(sizes, 3)
+    assert sorted(i for s in share for i in s) == list(range(len(sizes)))
+    loads = partition.loads(sizes, share)
+    assert max(loads) <= sum(sizes) / 3 + max(sizes)
+    assert partition.by_footprint(sizes, 1) == [list(range(len(sizes)))]
+    ranks = partition.stream_by_footprint(sizes, 2)
+    assert ranks[:3] == [0, 1, 0]  # each to the rank with the least footprint so far
+    with pytest.raises(ValueError):
+        partition.by_footprint(sizes, 0)
 
 
 def _worker(rank, world, port, q):
