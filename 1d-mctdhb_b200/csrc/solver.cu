@@ -38,12 +38,54 @@ struct mctdhb_solver_s {
     // phase 0: orbital step; phase 1: matrices, SIL, densities
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    // mctdhb_solver_relax: the step inside a conditional WHILE node
+    cudaGraph_t relax_graph = nullptr;
+    cudaGraphExec_t relax_exec = nullptr;
+    struct RelaxCtl* d_ctl = nullptr;
+    struct RelaxCtl* h_ctl = nullptr;  // pinned
+    bool relax_pending = false;
     int kernels = 0;
     bool has_state = false;
     std::mutex mu;
 };
 
+// device state of mctdhb_solver_relax: the parameters of a run (written
+// before each launch) and its counters
+struct RelaxCtl {
+    uint32_t max_steps, steps;
+    int check_every, conv;
+    double tol, prev;
+};
+
 namespace {
+
+constexpr uint32_t kRelaxHardCap = 100000000u;  // no run passes this many steps
+
+// E of the state before the first step seeds the energy rule (driver.c:229)
+__global__ void relax_init_kernel(RelaxCtl* __restrict__ c, const double2* __restrict__ E,
+                                  int N) {
+    c->steps = 0;
+    c->conv = 0;
+    c->prev = E->x / N;
+}
+
+// after every step: the imaginary-time energy rule of driver.c:47-67 (every
+// check_every steps) and the step limit; the WHILE node repeats the step
+// while this sets 1
+__global__ void relax_rule_kernel(RelaxCtl* __restrict__ c, const double2* __restrict__ E,
+                                  int N, int imag, cudaGraphConditionalHandle h) {
+    const uint32_t steps = ++c->steps;
+    bool stop = steps >= c->max_steps || steps >= kRelaxHardCap;
+    if (imag && c->check_every > 0 && steps % (uint32_t)c->check_every == 0) {
+        const double curr = E->x / N;
+        if (fabs(curr - c->prev) < c->tol * c->prev) {
+            c->conv = 1;
+            stop = true;
+        }
+        c->prev = curr;
+    }
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
 
 // phase 0 (orbital_integration.c:284-349): orbitals advanced with the
 // current rho1^{-1} and rho2
@@ -130,6 +172,86 @@ void drop_graphs(mctdhb_solver_s* s) {
         s->exec[p] = nullptr;
         s->graph[p] = nullptr;
     }
+    if (s->relax_exec) cudaGraphExecDestroy(s->relax_exec);
+    if (s->relax_graph) cudaGraphDestroy(s->relax_graph);
+    s->relax_exec = nullptr;
+    s->relax_graph = nullptr;
+}
+
+// The relaxation graph: the energy of the current state and the rule's
+// initial state, then a conditional WHILE node whose body is one step
+// (both phases), the energy of the new state and the rule kernel.
+int build_relax_graph(mctdhb_solver_s* s) {
+    if (s->relax_exec) return 0;
+    cudaStream_t st = s->cs;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        set_error("solver relax: capture: %s", cudaGetErrorString(e));
+        return -1;
+    }
+    cudaGraph_t g = nullptr;
+    cudaGraphConditionalHandle h = 0;
+    cudaGraphNode_t cnode = nullptr;
+    cudaGraph_t body = nullptr;
+    int rc = orb_energy(s->M, s->d_rho1, s->d_rho2, s->d_hob, s->d_hint, s->d_E, st);
+    if (!rc) {
+        relax_init_kernel<<<1, 1, 0, st>>>(s->d_ctl, s->d_E, s->N);
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaStreamCaptureStatus cs;
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
+            if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
+        }
+        if (e == cudaSuccess)
+            e = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
+        if (e != cudaSuccess) {
+            set_error("solver relax: conditional node: %s", cudaGetErrorString(e));
+            rc = -1;
+        }
+    }
+    e = cudaStreamEndCapture(st, &s->relax_graph);
+    if (rc || e != cudaSuccess) {
+        if (!rc) set_error("solver relax: capture: %s", cudaGetErrorString(e));
+        drop_graphs(s);
+        return -1;
+    }
+    // the body: one step, the energy, the rule
+    e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        set_error("solver relax: body capture: %s", cudaGetErrorString(e));
+        drop_graphs(s);
+        return -1;
+    }
+    rc = phase_orbitals(s, st) || phase_coefficients(s, st) ||
+         orb_energy(s->M, s->d_rho1, s->d_rho2, s->d_hob, s->d_hint, s->d_E, st);
+    if (!rc) {
+        relax_rule_kernel<<<1, 1, 0, st>>>(s->d_ctl, s->d_E, s->N, s->imagtime, h);
+        if (cudaGetLastError() != cudaSuccess) rc = -1;
+    }
+    cudaGraph_t out = nullptr;
+    e = cudaStreamEndCapture(st, &out);
+    if (rc || e != cudaSuccess) {
+        if (!rc) set_error("solver relax: body capture: %s", cudaGetErrorString(e));
+        drop_graphs(s);
+        return -1;
+    }
+    e = cudaGraphInstantiate(&s->relax_exec, s->relax_graph, 0);
+    if (e != cudaSuccess) {
+        set_error("solver relax: instantiate: %s", cudaGetErrorString(e));
+        drop_graphs(s);
+        return -1;
+    }
+    return 0;
 }
 
 }  // namespace
@@ -219,6 +341,8 @@ void mctdhb_solver_destroy(mctdhb_solver s) {
     cudaFree(s->d_rinv);
     cudaFree(s->d_E);
     cudaFree(s->d_info);
+    cudaFree(s->d_ctl);
+    if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->cs) cudaStreamDestroy(s->cs);
     if (s->ev_step) cudaEventDestroy(s->ev_step);
     orb_release(s->orb);
@@ -370,6 +494,59 @@ int mctdhb_solver_step(mctdhb_solver s, int nsteps, void* stream) {
         s->t += s->dt;
     }
     MCTDHB_CUDA_TRY(cudaEventRecord(s->ev_step, (cudaStream_t)stream));
+    return 0;
+}
+
+// Steps on the device until the imaginary-time energy rule or max_steps,
+// with no host round trip: one launch of the relaxation graph.
+int mctdhb_solver_relax(mctdhb_solver s, uint32_t max_steps, double energy_tol, int check_every,
+                        void* stream) {
+    if (!s || !s->has_state || max_steps < 1 || max_steps > kRelaxHardCap || check_every < 0 ||
+        !(energy_tol >= 0.0)) {
+        set_error("mctdhb_solver_relax: invalid argument or solver without state");
+        return -1;
+    }
+    if (s->M == 1) {
+        set_error("mctdhb_solver_relax: one orbital (no coefficients to relax); use step");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->d_ctl) {
+        if (cudaMalloc(&s->d_ctl, sizeof(RelaxCtl)) != cudaSuccess ||
+            cudaMallocHost(&s->h_ctl, sizeof(RelaxCtl)) != cudaSuccess) {
+            set_error("mctdhb_solver_relax: allocation failed");
+            return -1;
+        }
+    }
+    if (build_relax_graph(s)) return -1;
+    cudaStream_t st = (cudaStream_t)stream;
+    // the previous run's counters may still be read: order after it
+    MCTDHB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_step, 0));
+    MCTDHB_CUDA_TRY(cudaStreamSynchronize(st));
+    *s->h_ctl = RelaxCtl{max_steps, 0u, check_every, 0, energy_tol, 0.0};
+    MCTDHB_CUDA_TRY(cudaMemcpyAsync(s->d_ctl, s->h_ctl, sizeof(RelaxCtl), cudaMemcpyHostToDevice,
+                                    st));
+    MCTDHB_CUDA_TRY(cudaGraphLaunch(s->relax_exec, st));
+    MCTDHB_CUDA_TRY(cudaEventRecord(s->ev_step, st));
+    s->relax_pending = true;
+    return 0;
+}
+
+int mctdhb_solver_relax_result(mctdhb_solver s, uint32_t* steps, int* converged) {
+    if (!s || !s->d_ctl) {
+        set_error("mctdhb_solver_relax_result: no relaxation run");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    MCTDHB_CUDA_TRY(cudaEventSynchronize(s->ev_step));
+    RelaxCtl c;
+    MCTDHB_CUDA_TRY(cudaMemcpy(&c, s->d_ctl, sizeof(c), cudaMemcpyDeviceToHost));
+    if (s->relax_pending) {
+        s->t += c.steps * s->dt;
+        s->relax_pending = false;
+    }
+    if (steps) *steps = c.steps;
+    if (converged) *converged = c.conv;
     return 0;
 }
 

@@ -56,6 +56,7 @@ EXPORTED = [
     "mctdhb_solver_set_orthogonality", "mctdhb_solver_overlap_residual",
     "mctdhb_solver_eig_residual", "mctdhb_solver_lowest_state", "mctdhb_solver_set_derivative",
     "mctdhb_solver_set_coef_method", "mctdhb_solver_set_orb_method",
+    "mctdhb_solver_relax", "mctdhb_solver_relax_result",
 ]
 
 _lib = None
@@ -229,6 +230,10 @@ def load(path=LIB_PATH):
     L.mctdhb_batch_launch_hc.argtypes = [vp, i, i]
     L.mctdhb_solver_step_phase.restype = i
     L.mctdhb_solver_step_phase.argtypes = [vp, i, vp]
+    L.mctdhb_solver_relax.restype = i
+    L.mctdhb_solver_relax.argtypes = [vp, u32, d, i, vp]
+    L.mctdhb_solver_relax_result.restype = i
+    L.mctdhb_solver_relax_result.argtypes = [vp, C.POINTER(u32), C.POINTER(i)]
     L.mctdhb_fp64_mma_probe.restype = i
     L.mctdhb_fp64_mma_probe.argtypes = [i, i, vp, vp]
     _lib = L
@@ -455,6 +460,19 @@ class Solver:
         _check(load().mctdhb_solver_lowest_state(self.h, niter, C.byref(e)),
                "mctdhb_solver_lowest_state")
         return e.value
+
+    def relax(self, max_steps, energy_tol=0.0, check_every=0, stream=None):
+        """steps on the device until the energy rule or max_steps (one graph
+        launch, asynchronous); relax_result() gives (steps, converged)"""
+        _check(load().mctdhb_solver_relax(self.h, int(max_steps), float(energy_tol),
+                                          int(check_every), _stream_ptr(stream)),
+               "mctdhb_solver_relax")
+
+    def relax_result(self):
+        n, c = C.c_uint32(), C.c_int()
+        _check(load().mctdhb_solver_relax_result(self.h, C.byref(n), C.byref(c)),
+               "mctdhb_solver_relax_result")
+        return n.value, bool(c.value)
 
 
 class DropIn:

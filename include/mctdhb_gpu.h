@@ -232,6 +232,19 @@ int  mctdhb_solver_set_orb_method(mctdhb_solver s, int orb_method);
 int  mctdhb_solver_overlap_residual(mctdhb_solver s, double* res);
 int  mctdhb_solver_eig_residual(mctdhb_solver s, double e, double* res);
 int  mctdhb_solver_lowest_state(mctdhb_solver s, int niter, double* e);
+/* Steps on the device until the imaginary-time energy rule of the
+ * reference's driver (driver.c:47-67: |E/N - E_prev/N| < energy_tol *
+ * E_prev/N, checked every check_every steps; check_every 0 or real time: no
+ * rule) or max_steps steps: one launch of a CUDA graph whose conditional
+ * WHILE node repeats the step and a kernel evaluates the rule, so no step
+ * waits for the host (the reference's loop, driver.c:248-285, checks on the
+ * host).  Asynchronous on `stream`; needs norb >= 2.  No counterpart in
+ * the reference as one call. */
+int  mctdhb_solver_relax(mctdhb_solver s, uint32_t max_steps, double energy_tol,
+                         int check_every, void* stream);
+/* steps done by the last mctdhb_solver_relax and whether the energy rule
+ * stopped it (synchronises with it) */
+int  mctdhb_solver_relax_result(mctdhb_solver s, uint32_t* steps, int* converged);
 void*  mctdhb_solver_device_coef(mctdhb_solver s);
 void*  mctdhb_solver_device_orbitals(mctdhb_solver s);
 double mctdhb_solver_time(mctdhb_solver s);
