@@ -524,16 +524,23 @@ int mctdhb_batch_create(int max_slots, size_t arena_bytes, int lanczos_iter, mct
     for (int li = 0; li < kBatchLists && !bad; li++)
         bad = cudaMalloc(&b->d_tl[li], b->cap[li] * sizeof(BatchTile)) ||
               cudaMallocHost(&b->h_tl[li], b->cap[li] * sizeof(BatchTile));
+    // the engine's stream (and with it every launch of its step graph) takes
+    // the device's highest priority: a batch of many small jobs shares the
+    // GPU with work on other streams (a serving loop's one-at-a-time lane for
+    // jobs that fill the GPU alone) and its short kernels go first whenever
+    // SMs free up
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     if (bad ||
         cudaMallocHost(&b->h_flags, (size_t)max_slots * BF_TOTAL * sizeof(int)) ||
         cudaMallocHost(&b->h_scal, (size_t)max_slots * BS_TOTAL * sizeof(double2)) ||
-        cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) ||
+        cudaStreamCreateWithPriority(&b->st, cudaStreamNonBlocking, prio_hi) ||
         cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) {
         set_error("mctdhb_batch_create: device allocation of %zu bytes failed", b->arena_bytes);
         return fail();
     }
     for (int M = 0; M < kNumM; M++)
-        if (cudaStreamCreateWithFlags(&b->side[M], cudaStreamNonBlocking) ||
+        if (cudaStreamCreateWithPriority(&b->side[M], cudaStreamNonBlocking, prio_hi) ||
             cudaEventCreateWithFlags(&b->ev_join[M], cudaEventDisableTiming)) {
             set_error("mctdhb_batch_create: stream creation failed");
             return fail();

@@ -39,7 +39,11 @@ struct PairHcShape {
     // Rows of A per tile, one producer thread per row (unrank and gather).
     // Up to 6 orbitals a row carries little contraction, so a tile must
     // keep 256 rows of gathers in flight for the tensor cores; at 7 and 8
-    // orbitals 128 rows do.
+    // orbitals 128 rows do.  Measured alternatives at six orbitals (mix
+    // contraction 14.3 ms): 128-row tiles 16.9-18.7 ms; two rows per
+    // producer thread with half the producers (freeing registers for one
+    // output pass and W in registers) 16.8 ms; one output pass at 128
+    // registers (spills) 14.7 ms.  The gathers want threads.
     static constexpr bool WIDE = P <= 21;
     // W fragments held in registers by the consumers (up to 5 orbitals; at 6
     // they would spill under the 128-register budget of a 512-thread block)

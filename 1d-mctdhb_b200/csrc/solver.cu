@@ -532,6 +532,17 @@ int mctdhb_solver_relax(mctdhb_solver s, uint32_t max_steps, double energy_tol, 
     return 0;
 }
 
+int mctdhb_solver_query(mctdhb_solver s) {
+    if (!s) {
+        set_error("mctdhb_solver_query: null solver");
+        return -1;
+    }
+    const cudaError_t e = cudaEventQuery(s->ev_step);
+    if (e == cudaErrorNotReady) return 0;
+    MCTDHB_CUDA_TRY(e);
+    return 1;
+}
+
 int mctdhb_solver_relax_result(mctdhb_solver s, uint32_t* steps, int* converged) {
     if (!s || !s->d_ctl) {
         set_error("mctdhb_solver_relax_result: no relaxation run");

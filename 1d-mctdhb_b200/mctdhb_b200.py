@@ -56,7 +56,7 @@ EXPORTED = [
     "mctdhb_solver_set_orthogonality", "mctdhb_solver_overlap_residual",
     "mctdhb_solver_eig_residual", "mctdhb_solver_lowest_state", "mctdhb_solver_set_derivative",
     "mctdhb_solver_set_coef_method", "mctdhb_solver_set_orb_method",
-    "mctdhb_solver_relax", "mctdhb_solver_relax_result",
+    "mctdhb_solver_relax", "mctdhb_solver_relax_result", "mctdhb_solver_query",
 ]
 
 _lib = None
@@ -232,6 +232,8 @@ def load(path=LIB_PATH):
     L.mctdhb_solver_step_phase.argtypes = [vp, i, vp]
     L.mctdhb_solver_relax.restype = i
     L.mctdhb_solver_relax.argtypes = [vp, u32, d, i, vp]
+    L.mctdhb_solver_query.restype = i
+    L.mctdhb_solver_query.argtypes = [vp]
     L.mctdhb_solver_relax_result.restype = i
     L.mctdhb_solver_relax_result.argtypes = [vp, C.POINTER(u32), C.POINTER(i)]
     L.mctdhb_fp64_mma_probe.restype = i
@@ -467,6 +469,13 @@ class Solver:
         _check(load().mctdhb_solver_relax(self.h, int(max_steps), float(energy_tol),
                                           int(check_every), _stream_ptr(stream)),
                "mctdhb_solver_relax")
+
+    def done(self):
+        """True once the last launch has finished on the device (no wait)"""
+        r = load().mctdhb_solver_query(self.h)
+        if r < 0:
+            raise MctdhbError(f"mctdhb_solver_query: {last_error()}")
+        return r == 1
 
     def relax_result(self):
         n, c = C.c_uint32(), C.c_int()

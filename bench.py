@@ -704,85 +704,63 @@ def e2e_batch(mb, torch, jobs, steps):
 # ---------------------------------------------------------------------------
 # serving: continuous batching against one-at-a-time
 # ---------------------------------------------------------------------------
-def serve_batched(mb, arrivals, arena, max_slots=512, steps_per_poll=2):
-    """continuous batching in real time: jobs are admitted (first come first
-    served) once arrived and once they fit in the arena, advanced together
-    by the batch step, retired when they stop.  Returns latencies, the
-    makespan and the jobs' final energies."""
-    b = mb.Batch(max_slots, arena, LZ)
-    pending = list(enumerate(arrivals))
-    waiting, running, lat, energy = [], {}, {}, {}
-    t_start = time.perf_counter()
-    while pending or waiting or running:
-        now = time.perf_counter() - t_start
-        while pending and pending[0][1][0] <= now:
-            waiting.append(pending.pop(0))
-        while waiting:
-            s = b.admit(waiting[0][1][1])
-            if s is None:
-                break
-            running[s] = waiting.pop(0)
-        if not running:
-            if pending:
-                time.sleep(max(0.0, min(0.002, pending[0][1][0] - now)))
-            continue
-        b.step(steps_per_poll)
-        _, state, _, en = b.poll()
-        now = time.perf_counter() - t_start
-        for s in [s for s in running if state[s] == 2]:
-            i, (ta, _) = running.pop(s)
-            lat[i] = now - ta
-            energy[i] = float(en[s])
-            b.release(s)
-    total = time.perf_counter() - t_start
-    b.close()
-    n = len(arrivals)
-    return [lat[i] for i in range(n)], total, [energy[i] for i in range(n)]
+# jobs with at least this many configurations fill the GPU alone (N=30 M=8:
+# 10.3 M); the server runs them in its solver lane beside the batch
+HEAVY_NC = 9_000_000
 
 
-def plain_service(mb, torch, jobs):
-    """each job alone through the plain solver, back to back, to its own stop
-    (step limit, or the imaginary-time energy rule of the reference's driver
-    checked on the host every check_every steps); service time = wall clock
-    from solver creation to the stop, set-up included"""
-    stream = torch.cuda.current_stream()
-    svc, energy = [], []
-    for j in jobs:
-        t0 = time.perf_counter()
-        s = mb.Solver(j["npar"], j["norb"], j["grid_size"], j["xi"], j["xf"], j["dt"],
-                      bool(j["imagtime"]), j["rk_order"], LZ, periodic=bool(j["periodic"]))
+def serve_batched(mb, arrivals, arena, max_slots=512, steps_per_tick=2):
+    """continuous batching in real time through the package's request loop
+    (serving.Server): jobs admitted first come first served once arrived and
+    once they fit in the arena, advanced together, retired when they stop;
+    jobs of HEAVY_NC configurations or more in the server's solver lane.
+    Returns latencies, the makespan and the jobs' final energies."""
+    from serving import Server
+
+    srv = Server(arena, max_slots=max_slots, lanczos_iter=LZ, steps_per_tick=steps_per_tick,
+                 heavy_nc=HEAVY_NC)
+    try:
+        ids = [srv.submit(j, at=t) for t, j in arrivals]
+        srv.run()
+        st = srv.stats()
+        return ([srv.latency(i) for i in ids], st["makespan_s"],
+                [srv.result(i)["energy"] for i in ids], st)
+    finally:
+        srv.close()
+
+
+def plain_job(mb, torch, j):
+    """one job alone through the plain solver to its own stop: the
+    imaginary-time energy rule or the step limit, evaluated on the device
+    (mctdhb_solver_relax: one graph launch, no host round trip per step)"""
+    s = mb.Solver(j["npar"], j["norb"], j["grid_size"], j["xi"], j["xf"], j["dt"],
+                  bool(j["imagtime"]), j["rk_order"], LZ, periodic=bool(j["periodic"]))
+    try:
         s.set_potential(j["pot"])
         s.set_interaction(j["g"])
         s.set_state(j["orbitals"], j["coef"])
-        prev = s.energy().real / j["npar"]
-        e = prev
-        k = 0
-        while k < j["max_steps"]:
-            n = j["check_every"] if (j["imagtime"] and j["check_every"]) else j["max_steps"]
-            n = min(n, j["max_steps"] - k)
-            s.step(n, stream)
-            k += n
-            if j["imagtime"] and j["check_every"]:
-                e = s.energy().real / j["npar"]
-                if abs(e - prev) < j["energy_tol"] * prev:
-                    break
-                prev = e
-        e = s.energy().real
-        torch.cuda.synchronize()
+        check = j["check_every"] if j["imagtime"] else 0
+        s.relax(j["max_steps"], j["energy_tol"], check, torch.cuda.current_stream())
+        steps, _ = s.relax_result()
+        return s.energy().real, steps
+    finally:
         s.close()
-        svc.append(time.perf_counter() - t0)
+
+
+def serve_plain(mb, torch, arrivals):
+    """one-at-a-time serving in real time: the jobs in arrival order, each
+    started when it has arrived and the previous one has finished, run alone
+    by plain_job; latency = finish - arrival"""
+    t0 = time.perf_counter()
+    lat, energy = [], []
+    for ta, j in arrivals:
+        now = time.perf_counter() - t0
+        if now < ta:
+            time.sleep(ta - now)
+        e, _ = plain_job(mb, torch, j)
         energy.append(e)
-    return svc, energy
-
-
-def fcfs(arr, svc):
-    """latencies and makespan of one first-come-first-served server: job i
-    starts at max(its arrival, the previous job's finish)"""
-    fin, lat = 0.0, []
-    for a, s in zip(arr, svc):
-        fin = max(fin, a) + s
-        lat.append(fin - a)
-    return lat, fin
+        lat.append(time.perf_counter() - t0 - ta)
+    return lat, time.perf_counter() - t0 - arrivals[0][0], energy
 
 
 def percentiles(lat):
@@ -792,29 +770,38 @@ def percentiles(lat):
 
 
 def run_serving(mb, torch, rates, njobs, imag_steps, real_steps, big_frac, nmax):
+    """the served workload: a Poisson stream of 70% imaginary-time
+    ground-state jobs (energy rule 1e-10 or imag_steps steps) and 30%
+    real-time quenches (real_steps steps, dt 0.005 capped for RK5
+    stability), sizes as the batched mix plus big_frac N=30 M=8 jobs; at each
+    arrival rate both servers run the same stream in real time"""
     seq = served_jobs(njobs, imag_steps=imag_steps, real_steps=real_steps, big_frac=big_frac,
                       nmax=nmax)
     jobs = [j for _, j in seq]
     unit = [t for t, _ in seq]
-    arena = min(arena_bytes(mb, jobs), 96 << 30)
-    svc, e_plain = plain_service(mb, torch, jobs)
+    arena = min(arena_bytes(mb, [j for j in jobs if dim(j["npar"], j["norb"]) < HEAVY_NC] or
+                            jobs[:1]), 96 << 30)
     out = {"jobs": len(jobs), "imag_steps": imag_steps, "real_steps": real_steps,
-           "big_frac": big_frac, "nmax": nmax, "arena_bytes": arena,
-           "plain_service_s": {"sum": float(sum(svc)), "mean": float(np.mean(svc)),
-                               "max": float(max(svc))},
-           "plain_method": "each job's service time measured alone through mctdhb_solver, "
-                           "back to back; latencies from the first-come-first-served "
-                           "recurrence over the arrivals (what one-at-a-time serving gives)",
+           "big_frac": big_frac, "big_jobs": sum(1 for j in jobs if j["big"]), "nmax": nmax,
+           "arena_bytes": arena,
+           "batched_method": "serving.Server: FCFS admission by footprint into the running "
+                             "batch, 2 batch steps per tick, retirement as jobs stop; jobs of "
+                             f"{HEAVY_NC} configurations or more one at a time in the server's "
+                             "solver lane beside the batch",
+           "plain_method": "one at a time in arrival order, each alone through mctdhb_solver "
+                           "with the same stop rules on the device (mctdhb_solver_relax), "
+                           "run in real time at every rate",
            "rates": []}
     worst = 0.0
     for r in rates:
         arr = [u / r for u in unit]
-        lat_b, t_b, e_b = serve_batched(mb, list(zip(arr, jobs)), arena)
-        lat_p, t_p = fcfs(arr, svc)
-        worst = max(worst, max(abs(x - y) / abs(y) for x, y in zip(e_b, e_plain)))
+        lat_b, t_b, e_b, st_b = serve_batched(mb, list(zip(arr, jobs)), arena)
+        lat_p, t_p, e_p = serve_plain(mb, torch, list(zip(arr, jobs)))
+        worst = max(worst, max(abs(x - y) / abs(y) for x, y in zip(e_b, e_p)))
         out["rates"].append({
             "rate_jobs_per_s": r,
-            "batched": dict(percentiles(lat_b), jobs_per_s=len(jobs) / t_b, makespan_s=t_b),
+            "batched": dict(percentiles(lat_b), jobs_per_s=len(jobs) / t_b, makespan_s=t_b,
+                            peak_running=st_b["peak_running"]),
             "plain": dict(percentiles(lat_p), jobs_per_s=len(jobs) / t_p, makespan_s=t_p),
             "p99_speedup": float(np.percentile(lat_p, 99) / np.percentile(lat_b, 99)),
             "throughput_speedup": t_p / t_b})
@@ -1143,18 +1130,33 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="timed steps per job on the plain one-at-a-time path")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serve-rates", default="10,50,500", help="arrival rates swept, jobs/s")
-    ap.add_argument("--serve-jobs", type=int, default=96, help="jobs served per rate")
-    ap.add_argument("--serve-imag-steps", type=int, default=300)
-    ap.add_argument("--serve-real-steps", type=int, default=100)
-    ap.add_argument("--serve-big-frac", type=float, default=0.0)
-    ap.add_argument("--serve-nmax", type=int, default=30)
+    ap.add_argument("--serving-only", action="store_true",
+                    help="only the serving block (its own JSON line)")
+    # the served workload as configured (sizes as the batched mix plus 5% N=30
+    # M=8 jobs, relaxations to 1e-10 or 5000 steps, 500-step quenches); the
+    # job count per rate is the one cap, so the block ends in minutes
+    ap.add_argument("--serve-rates", default="50,500", help="arrival rates swept, jobs/s")
+    ap.add_argument("--serve-jobs", type=int, default=16, help="jobs served per rate")
+    ap.add_argument("--serve-imag-steps", type=int, default=5000)
+    ap.add_argument("--serve-real-steps", type=int, default=500)
+    ap.add_argument("--serve-big-frac", type=float, default=0.05)
+    ap.add_argument("--serve-nmax", type=int, default=60)
     ap.add_argument("--profile", action="store_true",
                     help="one profiled batch step of a small mix (for ncu captures)")
     ap.add_argument("--profile-kernels", metavar="N,M", nargs="?", const="30,8",
                     help="one profiled H.C and density launch of one system (for ncu captures)")
     args = ap.parse_args()
-    if args.profile:
+    if args.serving_only:
+        import torch
+
+        import mctdhb_b200 as mb
+
+        torch.cuda.set_device(0)
+        print(json.dumps({"serving": run_serving(
+            mb, torch, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs,
+            args.serve_imag_steps, args.serve_real_steps, args.serve_big_frac,
+            args.serve_nmax)}), flush=True)
+    elif args.profile:
         run_profile()
     elif args.profile_kernels:
         run_profile_kernels(args.profile_kernels)

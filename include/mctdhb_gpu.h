@@ -245,6 +245,9 @@ int  mctdhb_solver_relax(mctdhb_solver s, uint32_t max_steps, double energy_tol,
 /* steps done by the last mctdhb_solver_relax and whether the energy rule
  * stopped it (synchronises with it) */
 int  mctdhb_solver_relax_result(mctdhb_solver s, uint32_t* steps, int* converged);
+/* 1 when the solver's last step, phase or relaxation launch has finished
+ * on the device, 0 while it runs, -1 on error (does not block) */
+int  mctdhb_solver_query(mctdhb_solver s);
 void*  mctdhb_solver_device_coef(mctdhb_solver s);
 void*  mctdhb_solver_device_orbitals(mctdhb_solver s);
 double mctdhb_solver_time(mctdhb_solver s);

@@ -68,3 +68,39 @@ def test_full_arena_back_pressures(gpu, oracle):
     for i, r in enumerate(res):
         assert r["state"] == 2 and r["steps"] <= 20 + 5 * i
         assert np.isfinite(r["energy"])
+
+
+def test_heavy_lane_beside_the_batch(gpu, oracle):
+    """with heavy_nc, the large job runs in the solver lane beside the batch:
+    its result is the plain solver's relaxation alone, bit for bit, and the
+    light jobs' results are their batched results alone"""
+    import mctdhb_b200 as mb
+    from serving import Server
+
+    heavy = job(oracle.dim, 14, 5, 128, True, 0.01, 0.4, 40, 21)  # 3060 configurations
+    light = [job(oracle.dim, 8, 3, 96, True, 0.01, 0.5, 30, 22),
+             job(oracle.dim, 6, 4, 64, False, 0.005, 0.3, 25, 23)]
+    arena = sum(mb.Batch.job_bytes(j, 5) for j in light) + (32 << 20)
+    srv = Server(arena, max_slots=8, heavy_nc=3000)
+    try:
+        ids = [srv.submit(j, at=0.0) for j in [heavy] + light]
+        srv.run()
+        res = [srv.result(i) for i in ids]
+    finally:
+        srv.close()
+    assert res[0]["lane"] == "solver"
+    s = mb.Solver(14, 5, 128, XI, XF, 0.01, True, 5, 5)
+    s.set_potential(heavy["pot"])
+    s.set_interaction(heavy["g"])
+    s.set_state(heavy["orbitals"], heavy["coef"])
+    s.relax(40, heavy["energy_tol"], heavy["check_every"])
+    steps, conv = s.relax_result()
+    d = s.get()
+    s.close()
+    assert res[0]["steps"] == steps and res[0]["converged"] == conv
+    for k in ("orb", "coef", "rho1", "rho2"):
+        assert np.array_equal(res[0][k], d[k]), k
+    for j, r in zip(light, res[1:]):
+        (alone,), _ = serve(gpu, [j], [0.0], mb.Batch.job_bytes(j, 5) + (16 << 20))
+        for k in ("orb", "coef", "rho1", "rho2"):
+            assert np.array_equal(alone[k], r[k]), k

@@ -162,3 +162,85 @@ def test_final_diagonalisation_only_for_unconverged_relaxations():
     assert fb.diag == ["limit"]
     assert srv.result(0)["energy_lowest_state"] == -1.0
     assert srv.result(3)["state"] == ABORTED and srv.stats()["aborted"] == 1
+
+
+class FakeLane:
+    """the SolverLane methods: a job needs job['lane_steps'] steps, a chunk
+    of k steps is done at the next poll"""
+
+    def __init__(self):
+        self.cur = None
+        self.started = []
+        self.chunks = []
+
+    def busy(self):
+        return self.cur is not None
+
+    def idle(self):
+        return self.cur is not None and not self.cur["launched"]
+
+    def start(self, job):
+        self.cur = {"job": job, "steps": 0, "launched": 0}
+        self.started.append(job["name"])
+
+    def advance(self, k):
+        self.cur["launched"] = min(k, self.cur["job"]["lane_steps"] - self.cur["steps"])
+        self.chunks.append(self.cur["job"]["name"])
+
+    def poll(self):
+        if self.cur is None or not self.cur["launched"]:
+            return None
+        self.cur["steps"] += self.cur["launched"]
+        self.cur["launched"] = 0
+        if self.cur["steps"] < self.cur["job"]["lane_steps"]:
+            return None
+        job = self.cur["job"]
+        self.cur = None
+        return {"energy": job["name"], "steps": job["lane_steps"], "converged": False,
+                "state": DONE, "monitor": {}, "lane": "solver"}
+
+    def close(self):
+        pass
+
+
+def test_heavy_jobs_take_their_own_lane_light_jobs_first():
+    """jobs of at least heavy_nc configurations run one at a time in the
+    solver lane, FCFS among themselves; the lane advances only while the
+    batch has no job running (light jobs first); a heavy job needs no arena
+    room"""
+    clock = Clock()
+    fb = FakeBatch(8, 30)
+    lane = FakeLane()
+    srv = Server(30, engine=fb, lane=lane, heavy_nc=1000, heavy_chunk=4, clock=clock,
+                 steps_per_tick=1)
+    heavy = lambda name, n: dict(job(name, 10 ** 9, n), npar=30, norb=8, lane_steps=n)
+    srv.submit(heavy("H1", 10), at=0.0)
+    srv.submit(job("a", 20, 3, npar=4, norb=3), at=0.0)
+    srv.submit(heavy("H2", 4), at=0.0)
+    srv.submit(job("b", 20, 2, npar=4, norb=3), at=0.0)  # waits for a's arena room
+    srv.tick()
+    assert lane.started == ["H1"] and lane.chunks == []  # light jobs running: lane waits
+    assert [r.job["name"] for r in srv.running.values()] == ["a"]
+    order = []
+    while srv.busy():
+        clock.t += 0.1
+        order += [srv.reqs[i].job["name"] for i in srv.tick()]
+    assert order == ["a", "b", "H1", "H2"]
+    assert lane.started == ["H1", "H2"] and lane.chunks == ["H1"] * 3 + ["H2"]
+    assert srv.result(0)["lane"] == "solver" and srv.result(0)["steps"] == 10
+    assert srv.stats()["jobs"] == 4
+
+
+def test_starved_heavy_job_gets_chunks_beside_the_batch():
+    clock = Clock()
+    fb = FakeBatch(8, 30)
+    lane = FakeLane()
+    srv = Server(30, engine=fb, lane=lane, heavy_nc=1000, heavy_chunk=1, heavy_max_wait=0.25,
+                 clock=clock, steps_per_tick=1)
+    srv.submit(dict(job("H", 10 ** 9, 3), npar=30, norb=8, lane_steps=3), at=0.0)
+    srv.submit(job("long", 20, 40, npar=4, norb=3), at=0.0)
+    order = []
+    while srv.busy():
+        clock.t += 0.1
+        order += [srv.reqs[i].job["name"] for i in srv.tick()]
+    assert order == ["H", "long"]  # every 0.3 s a chunk despite the running batch
