@@ -51,11 +51,12 @@ struct JobLayout {
     int vtiles = 0, ytiles = 0, gs[3] = {0, 0, 0}, gk[3] = {0, 0, 0};
     size_t o_orb, o_stage, o_H, o_pot, o_w, o_Q, o_hob, o_hint, o_pw, o_lint, o_rho1, o_rho2,
         o_rinv,
-        o_work, o_T, o_sq, o_g, o_V, o_out, o_part, o_py, o_gpart, total;
+        o_work, o_T, o_sq, o_g, o_V, o_out, o_part, o_py, o_gpart, o_half, o_B, total;
 };
 
-// der: 0 / 302 finite differences, 300 DVR, 301 spectral (periodic only)
-int job_layout(int N, int M, int G, int lz, int der, int periodic, JobLayout& L) {
+// der: 0 / 302 finite differences, 300 DVR, 301 spectral (periodic only);
+// split: the split step's half-step operator and B in the arena
+int job_layout(int N, int M, int G, int lz, int der, int periodic, int split, JobLayout& L) {
     if (der != 0 && der != kDerFiniteDiff && der != kDerDVR && der != kDerSpectral) {
         set_error("batch: derivative method %d not in {302, 300, 301}", der);
         return -1;
@@ -126,6 +127,16 @@ int job_layout(int N, int M, int G, int lz, int der, int periodic, JobLayout& L)
     L.o_py = take((size_t)L.D2 * P * z);
     L.o_gpart = take(((size_t)L.gs[2] * gram_entries(M, 2) + (size_t)L.gs[1] * gram_entries(M, 1)) *
                      z);
+    if (split && !periodic && der != 0 && der != kDerFiniteDiff) {
+        set_error("batch: the split step's FFT exponential needs periodic boundaries");
+        return -1;
+    }
+    if (split && !periodic && G > 2048) {
+        set_error("batch: split step on zero bounds limited to 2048 points");
+        return -1;
+    }
+    L.o_half = take(split ? (periodic ? 2 * (size_t)(G - 1) - 1 : (size_t)G * G) * z : 0);
+    L.o_B = take(split ? M2 * z : 0);
     L.total = o;
     return 0;
 }
@@ -179,6 +190,10 @@ struct mctdhb_batch_s {
     cudaGraphExec_t exec = nullptr;
     unsigned graph_mask = 0;
     int kernels = 0;
+    // the pair contraction's launch variant per orbital count, chosen by the
+    // autotuner when the step graph is captured (or set by the caller)
+    int pair_v[kNumM] = {};
+    bool pair_v_forced[kNumM] = {};
     std::mutex mu;
 };
 
@@ -286,18 +301,21 @@ int rebuild_lists(mctdhb_batch_s* b) {
 
 // H.C of Lanczos iteration `iter` of the slots of orbital count M
 int hc_group(int M, const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
-             const int* cnt, int iter, cudaStream_t st, int parts = 3) {
+             const int* cnt, int iter, cudaStream_t st, int parts = 3, int v = 0) {
     switch (M) {
-        case 2: return hcp_batch_launch<2>(slots, hy, hg, cnt, iter, parts, st);
-        case 3: return hcp_batch_launch<3>(slots, hy, hg, cnt, iter, parts, st);
-        case 4: return hcp_batch_launch<4>(slots, hy, hg, cnt, iter, parts, st);
-        case 5: return hcp_batch_launch<5>(slots, hy, hg, cnt, iter, parts, st);
-        case 6: return hcp_batch_launch<6>(slots, hy, hg, cnt, iter, parts, st);
-        case 7: return hcp_batch_launch<7>(slots, hy, hg, cnt, iter, parts, st);
-        case 8: return hcp_batch_launch<8>(slots, hy, hg, cnt, iter, parts, st);
+        case 2: return hcp_batch_launch<2>(slots, hy, hg, cnt, iter, parts, v, st);
+        case 3: return hcp_batch_launch<3>(slots, hy, hg, cnt, iter, parts, v, st);
+        case 4: return hcp_batch_launch<4>(slots, hy, hg, cnt, iter, parts, v, st);
+        case 5: return hcp_batch_launch<5>(slots, hy, hg, cnt, iter, parts, v, st);
+        case 6: return hcp_batch_launch<6>(slots, hy, hg, cnt, iter, parts, v, st);
+        case 7: return hcp_batch_launch<7>(slots, hy, hg, cnt, iter, parts, v, st);
+        case 8: return hcp_batch_launch<8>(slots, hy, hg, cnt, iter, parts, v, st);
     }
     return 0;
 }
+
+// the batched contraction variants (0 and 2, pairhc_tmpl.cuh)
+bool batch_v_ok(int M, int v) { return (v == 0 || v == 2) && pair_variant_ok(M, v); }
 
 // rho1 / rho2 of the slots of orbital count M (the slot list gives the
 // finalize blocks)
@@ -369,7 +387,8 @@ int enqueue_step(mctdhb_batch_s* b, unsigned mask) {
     MCTDHB_CUDA_TRY(cudaGetLastError());
     auto hc = [&](int iter) {
         return per_group(b, mask, [&](int M, cudaStream_t s) {
-            return hc_group(M, S, b->d_tl[LIST_HY], b->d_tl[LIST_HG], b->d_cnt, iter, s);
+            return hc_group(M, S, b->d_tl[LIST_HY], b->d_tl[LIST_HG], b->d_cnt, iter, s, 3,
+                            b->pair_v[M]);
         });
     };
     // Lanczos (multiconfig_lanczos.c:12-90)
@@ -426,12 +445,39 @@ int count_graph_kernels(cudaGraph_t g) {
     return k;
 }
 
+// the autotuner's choice of the contraction variant of orbital count M for
+// the current jobs (key: M and the group's (N-2)-space rows, to a factor of
+// 2), timed on the jobs' own coefficients before the capture
+struct BatchTuneCtx {
+    mctdhb_batch_s* b;
+    int M;
+};
+int batch_tune_launch(void* p, int v, cudaStream_t st) {
+    auto* c = (BatchTuneCtx*)p;
+    if (!batch_v_ok(c->M, v)) return 1;
+    return hc_group(c->M, c->b->d_slots, c->b->d_tl[LIST_HY], c->b->d_tl[LIST_HG], c->b->d_cnt,
+                    0, st, 1, v);
+}
+
+int tune_group(mctdhb_batch_s* b, int M) {
+    if (b->pair_v_forced[M]) return 0;
+    uint64_t rows = 0;
+    for (const HostSlot& h : b->hs)
+        if (h.used && h.running && h.d.M == M) rows += h.L.D2;
+    int bucket = 0;
+    while ((1ull << bucket) < rows) bucket++;
+    BatchTuneCtx ctx{b, M};
+    const int v = tune_pick("bhcp_y", bucket, M, kPairVariants, b->st, batch_tune_launch, &ctx);
+    b->pair_v[M] = batch_v_ok(M, v) ? v : 0;
+    return 0;
+}
+
 int ensure_graph(mctdhb_batch_s* b) {
     if (b->exec && b->graph_mask == b->present_mask) return 0;
     drop_graph(b);
     for (int M = kBatchMinOrb; M <= kBatchMaxOrb; M++)
         if (b->present_mask >> M & 1)
-            if (prepare_group(M)) return -1;
+            if (prepare_group(M) || tune_group(b, M)) return -1;
     cudaError_t e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) {
         set_error("batch: capture: %s", cudaGetErrorString(e));
@@ -470,7 +516,7 @@ size_t mctdhb_batch_job_bytes(const mctdhb_job* job, int lanczos_iter) {
     if (!job) return 0;
     JobLayout L;
     if (job_layout(job->npar, job->norb, job->grid_size, lanczos_iter, job->der_method,
-                   job->periodic, L))
+                   job->periodic, job->orb_method == 31, L))
         return 0;
     return L.total;
 }
@@ -611,8 +657,14 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     const double reg = job->reg_fac > 0 ? job->reg_fac : 1e-9;
     std::lock_guard<std::mutex> lk(b->mu);
     JobLayout L;
+    const int split = job->orb_method == 31;
+    if (job->orb_method != 0 && job->orb_method != 30 && !split) {
+        set_error("mctdhb_batch_admit: orbital method %d not in {30 FULLSTEP_RUNGEKUTTA, "
+                  "31 SPLITSTEP}", job->orb_method);
+        return -1;
+    }
     if (job_layout(job->npar, job->norb, job->grid_size, b->lz, job->der_method, job->periodic,
-                   L))
+                   split, L))
         return -1;
     int s = -1;
     for (int i = 0; i < b->max_slots; i++)
@@ -704,6 +756,19 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
         toeplitz ? derivative_toeplitz(job->der_method, G, d.ov.dx, d.ov.a2,
                                        std::complex<double>(d.ov.a1.x, d.ov.a1.y))
                  : std::vector<double2>();
+    // the split step's half-step operator (the single-system solver's own)
+    std::vector<double2> half;
+    d.split = split;
+    d.half_dense = 0;
+    d.half = split ? (const double2*)P(L.o_half) : nullptr;
+    d.B = split ? (double2*)P(L.o_B) : nullptr;
+    if (split && split_half_operator(G, d.ov.dx, d.ov.a2, d.ov.a1, d.ov.periodic,
+                                     job->der_method == 0 ? kDerFiniteDiff : job->der_method,
+                                     job->dt, d.imag, half, &d.half_dense)) {
+        arena_give(b, h.off, h.bytes);
+        h = HostSlot();
+        return -1;
+    }
     int fl[BF_TOTAL] = {0};
     fl[BF_STATE] = SLOT_RUNNING;
     fl[BF_ROBUST] = job->impr_ortho ? 1 : 0;
@@ -722,6 +787,8 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
         cudaMemcpyAsync((void*)d.ov.w, w.data(), G * sizeof(double), cudaMemcpyHostToDevice, st) ||
         (toeplitz && cudaMemcpyAsync((void*)d.ov.lin_t, lint.data(), lint.size() * sizeof(double2),
                                      cudaMemcpyHostToDevice, st)) ||
+        (split && cudaMemcpyAsync((void*)d.half, half.data(), half.size() * sizeof(double2),
+                                  cudaMemcpyHostToDevice, st)) ||
         cudaMemcpyAsync((void*)d.sp.T, T.data(), T.size() * sizeof(uint32_t),
                         cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync((void*)d.sp.sq, sq.data(), sq.size() * sizeof(double),
@@ -965,7 +1032,30 @@ int mctdhb_batch_launch_hc(mctdhb_batch b, int norb, int parts) {
     if (b->lists_dirty && rebuild_lists(b)) return -1;
     if (prepare_group(norb)) return -1;
     return hc_group(norb, b->d_slots, b->d_tl[LIST_HY], b->d_tl[LIST_HG], b->d_cnt, 0, b->st,
-                    parts);
+                    parts, b->pair_v[norb]);
+}
+
+int mctdhb_batch_variant(mctdhb_batch b, int norb) {
+    if (!b || norb < kBatchMinOrb || norb > kBatchMaxOrb) {
+        set_error("mctdhb_batch_variant: invalid argument");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    return b->pair_v[norb];
+}
+
+int mctdhb_batch_set_variant(mctdhb_batch b, int norb, int variant) {
+    if (!b || norb < kBatchMinOrb || norb > kBatchMaxOrb ||
+        (variant >= 0 && !batch_v_ok(norb, variant))) {
+        set_error("mctdhb_batch_set_variant: no variant %d of the batched contraction for %d "
+                  "orbitals", variant, norb);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->pair_v_forced[norb] = variant >= 0;
+    b->pair_v[norb] = variant >= 0 ? variant : 0;
+    drop_graph(b);  // captured with the old variant
+    return 0;
 }
 
 void* mctdhb_batch_stream(mctdhb_batch b) { return b ? (void*)b->st : nullptr; }

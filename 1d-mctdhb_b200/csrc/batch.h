@@ -78,6 +78,12 @@ struct BatchSlot {
     const double* g;     // contact interaction (device scalar)
     double2 *orb, *stage, *H, *Q, *hob, *hint, *rho1, *rho2, *rinv, *work;
     double2 *V;          // lz x nc Krylov vectors; V[0] holds the coefficients
+    // split step (split: 1): the half-step operator (orbital.h,
+    // split_half_operator; dense: column-major G x G, else the circulant
+    // kernel of the G - 1 periodic points) and the M x M projection B
+    int split, half_dense;
+    const double2* half;
+    double2* B;
     double2 *out, *part;
     double2* gpart;      // Gram partials: gs[2] slices of rho2's, then gs[1] of rho1's
     double2* scal;       // BS_TOTAL
@@ -128,13 +134,15 @@ __host__ __device__ constexpr int batch_pair_rows(int M) {
 //   hcp_batch_launch   out = H V[iter] (- beta V[iter-1]) of every running
 //                      slot of orbital count M: pair contraction (parts & 1),
 //                      gather-back (parts & 2); iter = kBatchMonIter: out =
-//                      H V[0] of the slots whose eigen residual is due
+//                      H V[0] of the slots whose eigen residual is due;
+//                      variant: the contraction's launch variant (0 or 2,
+//                      pairhc_tmpl.cuh)
 //   gram_batch_launch  rho1 / rho2 of V[0] of the slots of orbital count M
 //                      (`list` / `nlist`: the slots, one finalize block each)
 //   batch_prepare      launch attributes (call before any stream capture)
 template <int M>
 int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
-                     const int* cnt, int iter, int parts, cudaStream_t st);
+                     const int* cnt, int iter, int parts, int variant, cudaStream_t st);
 template <int M>
 int gram_batch_launch(const BatchSlot* slots, const BatchTile* g2, const BatchTile* g1,
                       const int* cnt, const int* list, const int* nlist, int nblocks,

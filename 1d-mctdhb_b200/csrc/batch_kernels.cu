@@ -154,6 +154,85 @@ __device__ void bt_rhs(const BatchSlot& S, const double2* __restrict__ y, double
     __syncthreads();
 }
 
+// the split step's nonlinear right-hand side (orbital_integration.c:
+// 243-281), as orb_split_rhs_kernel: -i tf (interacting - sum_j (h[j][k] +
+// B[k][j]) f_j + V f_k), h of the half-stepped orbitals
+__device__ void bt_split_rhs(const BatchSlot& S, const double2* __restrict__ y,
+                             double2* __restrict__ out) {
+    const OrbView& o = S.ov;
+    const int M = o.M, G = o.G, n = M * G;
+    const double2* Q = S.Q;
+    const double2 mi_tf = make_double2(o.tf.y, -o.tf.x);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int k = t / G, x = t % G;
+        double2 fx[kBatchMaxOrb];
+        for (int a = 0; a < M; a++) fx[a] = y[(size_t)a * G + x];
+        const double2* Qk = Q + (size_t)k * M * M * M;
+        double2 red = make_double2(0.0, 0.0);
+        for (int s = 0; s < M; s++) {
+            double2 ts = make_double2(0.0, 0.0);
+            for (int l = 0; l < M; l++) {
+                double2 tl = make_double2(0.0, 0.0);
+                for (int q = 0; q < M; q++) tl = cfma(Qk[s + q * M + l * M * M], fx[q], tl);
+                ts = cfma(tl, fx[l], ts);
+            }
+            red = cfma(make_double2(fx[s].x, -fx[s].y), ts, red);
+        }
+        for (int j = 0; j < M; j++) {
+            const double2 c = cadd(S.hob[j * M + k], S.B[k * M + j]);
+            red.x -= c.x * fx[j].x - c.y * fx[j].y;
+            red.y -= c.x * fx[j].y + c.y * fx[j].x;
+        }
+        red = cadd(red, cscale(fx[k], o.pot[x]));
+        out[t] = cmul(mi_tf, red);
+    }
+    __syncthreads();
+}
+
+// linear half step of the split step, y <- Op y for every orbital, through
+// the spare stage buffer (orb_half_kernel: the same sums in the same order)
+__device__ void bt_half_step(const BatchSlot& S, double2* y) {
+    const int M = S.ov.M, G = S.ov.G, n = M * G;
+    const int dense = S.half_dense, nn = dense ? G : G - 1;
+    double2* w = S.stage + (size_t)7 * n - n;  // stage[6], the stage input of RK
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int k = t / G, x = t % G;
+        const double2* f = y + (size_t)k * G;
+        double2 acc = make_double2(0.0, 0.0);
+        if (dense) {
+            for (int j = 0; j < nn; j++) acc = cfma(S.half[(size_t)j * G + x], f[j], acc);
+        } else {
+            const double2* tk = S.half + (nn - 1 - (x == nn ? 0 : x));
+            for (int j = 0; j < nn; j++) acc = cfma(tk[j], f[j], acc);
+        }
+        w[t] = acc;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) y[t] = w[t];
+    __syncthreads();
+}
+
+// B[k][j] = sum_a rinv[k][a] sum_{s,q,l} rho2[a + sM + qM^2 + lM^3]
+//           hint[j + sM + lM^2 + qM^3] (orb_bmat_kernel, same order)
+__device__ void bt_bmat(const BatchSlot& S) {
+    const int M = S.M, M2 = M * M, M3 = M2 * M;
+    for (int e = threadIdx.x; e < M2; e += blockDim.x) {
+        const int k = e / M, j = e % M;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int a = 0; a < M; a++) {
+            double2 inner = make_double2(0.0, 0.0);
+            for (int s = 0; s < M; s++)
+                for (int q = 0; q < M; q++)
+                    for (int l = 0; l < M; l++)
+                        inner = cfma(S.rho2[a + s * M + q * M2 + l * M3],
+                                     S.hint[j + s * M + l * M2 + q * M3], inner);
+            acc = cfma(S.rinv[k * M + a], inner, acc);
+        }
+        S.B[e] = acc;
+    }
+    __syncthreads();
+}
+
 // out = y + dt sum_j c_j k_j
 struct Combo {
     int n;
@@ -178,45 +257,53 @@ __device__ void bt_combo(const BatchSlot& S, const double2* y, const Combo& cb, 
 }
 
 // Runge-Kutta step of the orbitals in place (orbital_integration.c:284-349)
-// with the named tableaux Heun (2), classical RK4 (4) and Butcher RK5 (5).
-// Stage j lives in stage[j], the stage input in stage[6].
-__device__ void bt_rk_step(const BatchSlot& S, double2* sP) {
+// with the named tableaux Heun (2), classical RK4 (4) and Butcher RK5 (5);
+// split: the split step's nonlinear right-hand side (orbital_integration.c:
+// 387-415) in place of the full one.  Stage j lives in stage[j], the stage
+// input in stage[6].
+__device__ void bt_rk_step(const BatchSlot& S, double2* sP, bool split) {
     const int n = S.ov.M * S.ov.G;
     double2* y = S.orb;
     double2* w = S.stage + (size_t)6 * n;
     auto k = [&](int j) { return S.stage + (size_t)j * n; };
+    auto rhs = [&](const double2* in, double2* out) {
+        if (split)
+            bt_split_rhs(S, in, out);
+        else
+            bt_rhs(S, in, out, sP);
+    };
     auto C1 = [](int a, double ca) { Combo c{1, {a}, {ca}}; return c; };
     switch (S.rk) {
         case 2:
-            bt_rhs(S, y, k(0), sP);
+            rhs(y, k(0));
             bt_combo(S, y, C1(0, 1.0), w);
-            bt_rhs(S, w, k(1), sP);
+            rhs(w, k(1));
             bt_combo(S, y, Combo{2, {0, 1}, {0.5, 0.5}}, y);
             break;
         case 4:
-            bt_rhs(S, y, k(0), sP);
+            rhs(y, k(0));
             bt_combo(S, y, C1(0, 0.5), w);
-            bt_rhs(S, w, k(1), sP);
+            rhs(w, k(1));
             bt_combo(S, y, C1(1, 0.5), w);
-            bt_rhs(S, w, k(2), sP);
+            rhs(w, k(2));
             bt_combo(S, y, C1(2, 1.0), w);
-            bt_rhs(S, w, k(3), sP);
+            rhs(w, k(3));
             bt_combo(S, y, Combo{4, {0, 1, 2, 3}, {1.0 / 6, 2.0 / 6, 2.0 / 6, 1.0 / 6}}, y);
             break;
         default:  // 5
-            bt_rhs(S, y, k(0), sP);
+            rhs(y, k(0));
             bt_combo(S, y, C1(0, 0.25), w);
-            bt_rhs(S, w, k(1), sP);
+            rhs(w, k(1));
             bt_combo(S, y, Combo{2, {0, 1}, {0.125, 0.125}}, w);
-            bt_rhs(S, w, k(2), sP);
+            rhs(w, k(2));
             bt_combo(S, y, Combo{2, {1, 2}, {-0.5, 1.0}}, w);
-            bt_rhs(S, w, k(3), sP);
+            rhs(w, k(3));
             bt_combo(S, y, Combo{2, {0, 3}, {3.0 / 16, 9.0 / 16}}, w);
-            bt_rhs(S, w, k(4), sP);
+            rhs(w, k(4));
             bt_combo(S, y,
                      Combo{5, {0, 1, 2, 3, 4}, {-3.0 / 7, 2.0 / 7, 12.0 / 7, -12.0 / 7, 8.0 / 7}},
                      w);
-            bt_rhs(S, w, k(5), sP);
+            rhs(w, k(5));
             bt_combo(S, y,
                      Combo{5, {0, 2, 3, 4, 5}, {7.0 / 90, 32.0 / 90, 12.0 / 90, 32.0 / 90, 7.0 / 90}},
                      y);
@@ -296,7 +383,17 @@ __global__ void __launch_bounds__(kBatchOrbThreads)
             S.Q[e] = cscale(acc, g);
         }
         __syncthreads();
-        bt_rk_step(S, sP);
+        if (S.split) {
+            // orbital_integration.c:352-434: half step, h and g of the
+            // half-stepped orbitals, B, RK of the nonlinear part, half step
+            bt_half_step(S, S.orb);
+            bt_matrices(S);
+            bt_bmat(S);
+            bt_rk_step(S, sP, true);
+            bt_half_step(S, S.orb);
+        } else {
+            bt_rk_step(S, sP, false);
+        }
         if (S.imag) {
             orthonormalize_block(S.ov, S.orb, scan);
             __syncthreads();
@@ -597,8 +694,17 @@ __global__ void __launch_bounds__(kBatchVecThreads)
     BT_SLOT
     const int M = S.M;
     if (threadIdx.x == 0) {
-        double* wd = (double*)(S.work + 3 * M * M);
-        S.flags[BF_INFO] = sync_rho1(M, S.rho1, S.rinv, S.reg_fac, S.work, wd);
+        // staged in shared memory: the routine's dependent accesses stay on
+        // the SM (same operations and bits as on the arena's copies)
+        __shared__ double2 r1[kBatchMaxOrb * kBatchMaxOrb], ri[kBatchMaxOrb * kBatchMaxOrb];
+        __shared__ double2 w[3 * kBatchMaxOrb * kBatchMaxOrb + kBatchMaxOrb / 2 + 1];
+        const int M2 = M * M;
+        for (int i = 0; i < M2; i++) r1[i] = S.rho1[i];
+        S.flags[BF_INFO] = sync_rho1(M, r1, ri, S.reg_fac, w, (double*)(w + 3 * M2));
+        for (int i = 0; i < M2; i++) {
+            S.rho1[i] = r1[i];
+            S.rinv[i] = ri[i];
+        }
     }
     __syncthreads();
     const double2 E = energy_block(M, S.rho1, S.rho2, S.hob, S.hint);

@@ -36,11 +36,11 @@ struct PairTileMeta {
     int active, real;
 };
 
-template <int M>
-__global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
+template <int M, int V>
+__global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
     bhcp_y_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
                   const int* __restrict__ cnt, int iter) {
-    using PS_ = PairHcShape<M>;
+    using PS_ = PairHcShape<M, V>;
     constexpr int P = PS_::P, PS = PS_::PS, ROWS = PS_::ROWS;
     static_assert(ROWS == batch_pair_rows(M), "tile rows of the host lists");
     extern __shared__ double2 smem[];
@@ -64,11 +64,11 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
                                      active && S.sp.pair_w[P * P].x != 0.0};
         if (!active) return;
         if (wslot[buf] != tl.slot) {
-            pair_stage_w<M>(S.sp.pair_w, Wb + buf * P * WS, pt, PS_::PRODUCERS);
+            pair_stage_w<M, V>(S.sp.pair_w, Wb + buf * P * WS, pt, PS_::PRODUCERS);
             wslot[buf] = tl.slot;
         }
-        pair_gather<M>(S.sp, S.V + (size_t)vin * S.nc, tl.idx, Ab + (size_t)buf * ROWS * PS, pt,
-                       PS_::PRODUCERS);
+        pair_gather<M, V>(S.sp, S.V + (size_t)vin * S.nc, tl.idx, Ab + (size_t)buf * ROWS * PS,
+                          pt, PS_::PRODUCERS);
     };
     BatchTile next{};
     if (producer) {
@@ -87,8 +87,8 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
         } else {
             const PairTileMeta tm = meta[buf];
             if (tm.active)
-                pair_consume<M>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * WS, t, tm.row0,
-                                tm.D2, tm.Y, tm.real != 0);
+                pair_consume<M, V>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * WS, t, tm.row0,
+                                   tm.D2, tm.Y, tm.real != 0);
         }
         __syncthreads();
     }
@@ -184,19 +184,31 @@ __global__ void __launch_bounds__(kBatchVecThreads)
     }
 }
 
-template <int M>
+template <int M, int V>
 constexpr size_t batch_y_smem() {
-    using PS_ = PairHcShape<M>;
+    using PS_ = PairHcShape<M, V>;
     return (2 * (size_t)PS_::P * PS_::WS + 2 * (size_t)PS_::ROWS * PS_::PS) * sizeof(double2);
+}
+
+// the batched tile lists fix the rows per tile: variants 0 and 2
+__host__ __device__ constexpr bool batch_variant_ok(int M, int V) {
+    return (V == 0 || V == 2) && pair_variant_ok(M, V);
+}
+
+template <int M, int V>
+int batch_y_attr() {
+    if constexpr (batch_variant_ok(M, V))
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bhcp_y_kernel<M, V>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)batch_y_smem<M, V>()));
+    return 0;
 }
 
 template <int M>
 int batch_prepare() {
     static std::atomic<uint64_t> done{0};
     return set_attributes_once(done, []() -> int {
-        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bhcp_y_kernel<M>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)batch_y_smem<M>()));
+        if (batch_y_attr<M, 0>() || batch_y_attr<M, 2>()) return -1;
         MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 2>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              gram_smem(M, 2)));
@@ -207,13 +219,27 @@ int batch_prepare() {
     });
 }
 
-template <int M>
-int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
-                     const int* cnt, int iter, int parts, cudaStream_t st) {
-    if (parts & 1) {
-        bhcp_y_kernel<M><<<num_sms(), PairHcShape<M>::THREADS, batch_y_smem<M>(), st>>>(
+template <int M, int V>
+int bhcp_y_launch(const BatchSlot* slots, const BatchTile* hy, const int* cnt, int iter,
+                  cudaStream_t st) {
+    if constexpr (!batch_variant_ok(M, V)) {
+        set_error("batched pair contraction variant %d does not exist for %d orbitals", V, M);
+        return -1;
+    } else {
+        bhcp_y_kernel<M, V><<<num_sms(), PairHcShape<M, V>::THREADS, batch_y_smem<M, V>(), st>>>(
             slots, hy, cnt, iter);
         MCTDHB_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
+}
+
+template <int M>
+int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
+                     const int* cnt, int iter, int parts, int variant, cudaStream_t st) {
+    if (parts & 1) {
+        const int rc = variant == 2 ? bhcp_y_launch<M, 2>(slots, hy, cnt, iter, st)
+                                    : bhcp_y_launch<M, 0>(slots, hy, cnt, iter, st);
+        if (rc) return -1;
     }
     if (parts & 2) {
         bhcp_g_kernel<M><<<num_sms() * 8, kBatchHcRows, 0, st>>>(slots, hg, cnt, iter);

@@ -188,19 +188,48 @@ int hc_prep(const SpaceView& sp, const double2* d_hob, const double2* d_hint, do
 
 static bool hc_templated(int M) { return M >= 2 && M <= kMaxTemplOrb; }
 
-static int hcp_apply(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
-                     cudaStream_t st) {
+static int hcp_apply_v(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
+                       int v, int parts, cudaStream_t st) {
     switch (sp.M) {
-        case 2: return hcp_apply_tmpl<2>(sp, C, HC, ep, st);
-        case 3: return hcp_apply_tmpl<3>(sp, C, HC, ep, st);
-        case 4: return hcp_apply_tmpl<4>(sp, C, HC, ep, st);
-        case 5: return hcp_apply_tmpl<5>(sp, C, HC, ep, st);
-        case 6: return hcp_apply_tmpl<6>(sp, C, HC, ep, st);
-        case 7: return hcp_apply_tmpl<7>(sp, C, HC, ep, st);
-        case 8: return hcp_apply_tmpl<8>(sp, C, HC, ep, st);
+        case 2: return hcp_apply_tmpl<2>(sp, C, HC, ep, v, parts, st);
+        case 3: return hcp_apply_tmpl<3>(sp, C, HC, ep, v, parts, st);
+        case 4: return hcp_apply_tmpl<4>(sp, C, HC, ep, v, parts, st);
+        case 5: return hcp_apply_tmpl<5>(sp, C, HC, ep, v, parts, st);
+        case 6: return hcp_apply_tmpl<6>(sp, C, HC, ep, v, parts, st);
+        case 7: return hcp_apply_tmpl<7>(sp, C, HC, ep, v, parts, st);
+        case 8: return hcp_apply_tmpl<8>(sp, C, HC, ep, v, parts, st);
     }
     set_error("hcp_apply: %d orbitals outside 2..8", sp.M);
     return -1;
+}
+
+// the pair contraction's launch variant for (N, M) (pairhc_tmpl.cuh): the
+// tuned choice, timed on the caller's data (the contraction alone) outside
+// a capture; variants that do not exist for M are skipped
+namespace {
+struct PairTuneCtx {
+    const SpaceView* sp;
+    const double2* C;
+    double2* HC;
+    const HcEpilogue* ep;
+};
+int pair_tune_launch(void* p, int v, cudaStream_t st) {
+    auto* c = (PairTuneCtx*)p;
+    if (!pair_variant_ok(c->sp->M, v)) return 1;  // no such variant: skipped
+    return hcp_apply_v(*c->sp, c->C, c->HC, *c->ep, v, 1, st);
+}
+}  // namespace
+
+static int pair_variant(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
+                        cudaStream_t st) {
+    PairTuneCtx ctx{&sp, C, HC, &ep};
+    const int v = tune_pick("hcp_y", sp.N, sp.M, kPairVariants, st, pair_tune_launch, &ctx);
+    return pair_variant_ok(sp.M, v) ? v : 0;
+}
+
+static int hcp_apply(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
+                     cudaStream_t st) {
+    return hcp_apply_v(sp, C, HC, ep, pair_variant(sp, C, HC, ep, st), 3, st);
 }
 
 static int hc_launch_v(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
@@ -242,7 +271,8 @@ int hc_tune_launch(void* p, int v, cudaStream_t st) {
 
 int hc_variant(const SpaceView& sp, const double2* C, double2* HC, const double2* tab,
                const HcEpilogue& ep, cudaStream_t st) {
-    if (!hc_templated(sp.M) || sp.dim < 4096 || sp.pair_y != nullptr) return 0;
+    if (sp.pair_y != nullptr) return pair_variant(sp, C, HC, ep, st);
+    if (!hc_templated(sp.M) || sp.dim < 4096) return 0;
     HcTuneCtx ctx{&sp, C, HC, tab, &ep};
     return tune_pick("hc", sp.N, sp.M, kHcVariants, st, hc_tune_launch, &ctx);
 }

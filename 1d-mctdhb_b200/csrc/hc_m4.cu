@@ -5,6 +5,6 @@ namespace mctdhb {
 template int hc_launch_tmpl<4>(const SpaceView&, const double2*, double2*, const double2*,
                                 const HcEpilogue&, int, cudaStream_t);
 template int hcp_apply_tmpl<4>(const SpaceView&, const double2*, double2*, const HcEpilogue&,
-                                 cudaStream_t);
+                                 int, int, cudaStream_t);
 template int hcp_prepare_tmpl<4>();
 }

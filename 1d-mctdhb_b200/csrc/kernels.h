@@ -62,13 +62,22 @@ int gram_apply_tmpl(const SpaceView& sp, uint32_t D2, uint32_t D1, const double2
 template <int M>
 int gram_prepare_tmpl();
 
+// Launch variants of the pair contraction (pairhc_tmpl.cuh, PairHcShape):
+// 0 the default tile, 1 half the rows per tile (up to 6 orbitals), 2 the
+// other output-tile grouping per pass (5 orbitals and more)
+__host__ __device__ constexpr bool pair_variant_ok(int M, int V) {
+    return V == 0 || (V == 1 && M * (M + 1) / 2 <= 21) || (V == 2 && M * (M + 1) / 2 > 10);
+}
+constexpr int kPairVariants = 3;
+
 // H.C through the two-boson-annihilated space (pairhc_tmpl.cuh), M <= 8,
-// N >= 2: launch attributes (before any capture) and the two launches
+// N >= 2: launch attributes (before any capture) and the launches
+// (parts & 1 the contraction, parts & 2 the gather-back) of a variant
 template <int M>
 int hcp_prepare_tmpl();
 template <int M>
 int hcp_apply_tmpl(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
-                   cudaStream_t st);
+                   int variant, int parts, cudaStream_t st);
 
 // tune.cu: autotuner.  The launch variant of `kernel` for (current device,
 // N, M): the cached choice, else -- outside a stream capture -- each variant
@@ -78,6 +87,7 @@ int hcp_apply_tmpl(const SpaceView& sp, const double2* C, double2* HC, const HcE
 int tune_pick(const char* kernel, int N, int M, int nvariants, cudaStream_t st,
               int (*launch)(void* ctx, int v, cudaStream_t st), void* ctx);
 int tune_lookup(const char* kernel, int N, int M);  // -1 when not tuned
+void tune_set(const char* kernel, int N, int M, int variant);  // a caller's choice
 
 // hamiltonian.cu
 // the packed coefficient table of h, g (and the pair matrix when sp has one)

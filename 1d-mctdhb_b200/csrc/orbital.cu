@@ -332,11 +332,28 @@ __global__ void orthonormalize_kernel(OrbView o, double2* __restrict__ F) {
     orthonormalize_block(o, F, scan);
 }
 
-// rho1 <- regularised rho1, rinv = rho1^{-1} (one thread; M <= 30)
+// rho1 <- regularised rho1, rinv = rho1^{-1} (one thread; M <= 30).  With
+// dynamic shared memory (smem > 0) the matrices are staged there: the
+// routine's thousands of dependent accesses then stay on the SM instead of
+// going to L2 (about 1 ms at M = 8 in global memory); same operations, same
+// bits.
 __global__ void sync_rho1_kernel(int M, double2* rho1, double2* rinv, double reg_fac,
-                                 double2* work, int* info) {
+                                 double2* work, int* info, int smem) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double* wd = (double*)(work + 3 * M * M);
+    const int M2 = M * M;
+    if (smem > 0) {
+        extern __shared__ double2 sh[];
+        double2 *r1 = sh, *ri = sh + M2, *w = sh + 2 * M2;
+        for (int i = 0; i < M2; i++) r1[i] = rho1[i];
+        const int r = sync_rho1(M, r1, ri, reg_fac, w, (double*)(w + 3 * M2));
+        for (int i = 0; i < M2; i++) {
+            rho1[i] = r1[i];
+            rinv[i] = ri[i];
+        }
+        if (info) *info = r;
+        return;
+    }
+    double* wd = (double*)(work + 3 * M2);
     const int r = sync_rho1(M, rho1, rinv, reg_fac, work, wd);
     if (info) *info = r;
 }
@@ -660,16 +677,10 @@ int orb_set_derivative(OrbCtx& c, int der) {
 //     Op dense, column by column by the Thomas algorithm
 //   DVR / spectral, FFT exponential (:57-82, 375-402): the circulant with
 //     eigenvalues exp(-i dth (i freq a1 - freq^2 a2)) at the FFT frequencies
-int orb_set_split(OrbCtx& c, int split, double dt, int imagtime) {
+int split_half_operator(int G, double dx, double a2, double2 a1v, int periodic, int der,
+                        double dt, int imagtime, std::vector<double2>& op, int* dense) {
     using cd = std::complex<double>;
-    cudaFree(c.d_half);
-    cudaFree(c.d_B);
-    c.d_half = nullptr;
-    c.d_B = nullptr;
-    c.split = 0;
-    if (!split) return 0;
-    const int G = c.G;
-    const bool periodic = c.view.periodic != 0, fd = c.der == kDerFiniteDiff;
+    const bool fd = der == kDerFiniteDiff;
     if (!periodic && !fd) {
         set_error("split step: the FFT exponential needs periodic boundaries");
         return -1;
@@ -678,13 +689,13 @@ int orb_set_split(OrbCtx& c, int split, double dt, int imagtime) {
         set_error("split step: grid of %d points above the operator's limit", G);
         return -1;
     }
-    const double dx = c.view.dx, a2 = c.view.a2, pi = 3.14159265358979323846;
-    const cd a1(c.view.a1.x, c.view.a1.y), I(0.0, 1.0);
+    const double pi = 3.14159265358979323846;
+    const cd a1(a1v.x, a1v.y), I(0.0, 1.0);
     const cd dth = 0.5 * (imagtime ? cd(0.0, -dt) : cd(dt, 0.0));
     const cd mid = I + a2 * dth / dx / dx, up = -a2 * dth / dx / dx / 2.0 - a1 * dth / dx / 4.0,
              lo = -a2 * dth / dx / dx / 2.0 + a1 * dth / dx / 4.0;
     const cd rmid = I - a2 * dth / dx / dx;
-    std::vector<double2> op;
+    op.clear();
     if (periodic) {
         const int n = G - 1;
         std::vector<cd> ex(n), mu(n), cop(n);
@@ -732,15 +743,32 @@ int orb_set_split(OrbCtx& c, int split, double dt, int imagtime) {
                 op[(size_t)j * G + i] = make_double2(x[i].real(), x[i].imag());
         }
     }
+    *dense = periodic ? 0 : 1;
+    return 0;
+}
+
+int orb_set_split(OrbCtx& c, int split, double dt, int imagtime) {
+    cudaFree(c.d_half);
+    cudaFree(c.d_B);
+    c.d_half = nullptr;
+    c.d_B = nullptr;
+    c.split = 0;
+    if (!split) return 0;
+    const int G = c.G;
+    std::vector<double2> op;
+    int dense = 0;
+    if (split_half_operator(G, c.view.dx, c.view.a2, c.view.a1, c.view.periodic, c.der, dt,
+                            imagtime, op, &dense))
+        return -1;
     MCTDHB_CUDA_TRY(cudaMalloc(&c.d_half, op.size() * sizeof(double2)));
     MCTDHB_CUDA_TRY(
         cudaMemcpy(c.d_half, op.data(), op.size() * sizeof(double2), cudaMemcpyHostToDevice));
     MCTDHB_CUDA_TRY(cudaMalloc(&c.d_B, (size_t)c.M * c.M * sizeof(double2)));
-    const int nn = periodic ? G - 1 : G;
+    const int nn = dense ? G : G - 1;
     MCTDHB_CUDA_TRY(cudaFuncSetAttribute(orb_half_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)((size_t)nn * sizeof(double2))));
-    c.half_dense = periodic ? 0 : 1;
+    c.half_dense = dense;
     c.split = 1;
     return 0;
 }
@@ -764,7 +792,10 @@ int orb_orthonormalize(const OrbCtx& c, double2* orb, cudaStream_t st) {
 
 int orb_sync_rho1(const OrbCtx& c, double2* rho1, double2* rinv, double reg_fac, int* d_info,
                   cudaStream_t st) {
-    sync_rho1_kernel<<<1, 32, 0, st>>>(c.M, rho1, rinv, reg_fac, c.d_work, d_info);
+    // rho1, rinv and the 3 M^2 + M work values in shared memory up to 48 KB
+    const size_t sm = (size_t)(5 * c.M * c.M) * sizeof(double2) + (size_t)c.M * sizeof(double);
+    const int smem = sm <= 48 * 1024 ? (int)sm : 0;
+    sync_rho1_kernel<<<1, 32, smem, st>>>(c.M, rho1, rinv, reg_fac, c.d_work, d_info, smem);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

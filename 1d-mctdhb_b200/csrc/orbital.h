@@ -75,6 +75,14 @@ int orb_set_derivative(OrbCtx& c, int der);
 // for time step dt (Crank-Nicolson for finite differences, the FFT
 // exponential for DVR / spectral), again whenever the method changes
 int orb_set_split(OrbCtx& c, int split, double dt, int imagtime);
+// the split step's half-step operator on the host (split_linear_orbitals.c
+// 23-82, 289-402): periodic grids, the circulant kernel of Crank-Nicolson
+// A^{-1} B (finite differences) or of the FFT exponential (DVR, spectral) on
+// the n = G - 1 periodic points (2n - 1 values, *dense = 0); zero bounds
+// (finite differences only), A^{-1} B on all G points column-major
+// (*dense = 1)
+int split_half_operator(int G, double dx, double a2, double2 a1, int periodic, int der,
+                        double dt, int imagtime, std::vector<double2>& op, int* dense);
 // one split step of the orbitals: y -> ynext through the half steps, h and
 // g of the half-stepped orbitals into hob / hint, and RK of the nonlinear part
 int orb_split_step(OrbCtx& c, int order, double dt, const double2* rinv, const double2* rho2,

@@ -32,7 +32,19 @@ namespace mctdhb {
 
 __host__ __device__ constexpr int pair_stride4(int x) { return x + ((12 - x % 8) % 8); }
 
-template <int M>
+// Launch variants of the pair contraction (the autotuner's choices, tune.cu):
+// every variant computes each Y value with the same instructions in the
+// same order, so a choice changes speed, never results.
+//   0  the default tile (below)
+//   1  tiles of half as many rows (up to 6 orbitals): twice the tiles, for
+//      spaces with fewer tiles than SMs
+//   2  the other output-tile grouping per pass (6 and fewer orbitals: one
+//      pass over all output tiles; 7: four at once; 8: two)
+// pair_variant_ok says which exist for M; the batched engine, whose tile
+// lists fix the rows per tile, takes 0 and 2.
+// (pair_variant_ok and kPairVariants: kernels.h)
+
+template <int M, int V = 0>
 struct PairHcShape {
     static constexpr int P = M * (M + 1) / 2;
     static constexpr int CONSUMERS = 256;  // 8 warps: the contraction on the tensor cores
@@ -45,12 +57,12 @@ struct PairHcShape {
     // output pass and W in registers) 16.8 ms; one output pass at 128
     // registers (spills) 14.7 ms.  The gathers want threads.
     static constexpr bool WIDE = P <= 21;
+    static constexpr int ROWS = (WIDE ? 256 : 128) / (V == 1 ? 2 : 1);
+    static constexpr int PRODUCERS = ROWS;
+    static constexpr int THREADS = CONSUMERS + PRODUCERS;
     // W fragments held in registers by the consumers (up to 5 orbitals; at 6
     // they would spill under the 128-register budget of a 512-thread block)
     static constexpr bool WREG = P <= 15;
-    static constexpr int ROWS = WIDE ? 256 : 128;
-    static constexpr int PRODUCERS = ROWS;
-    static constexpr int THREADS = CONSUMERS + PRODUCERS;
     // contraction depth: P rounded up to 4, in KB8 blocks of 8 and KB4 (0 or
     // 1) block of 4 (mma.sync m16n8k8 / m16n8k4); 8-wide output tiles
     static constexpr int KP = (P + 3) / 4 * 4;
@@ -59,7 +71,8 @@ struct PairHcShape {
     static constexpr int NN = (P + 7) / 8;
     // output tiles per pass over a strip: two (three at 8 orbitals) keep
     // the accumulators of the three products within the register budget
-    static constexpr int NG = NN <= 2 ? NN : (NN == 5 ? 3 : 2);
+    static constexpr int NG0 = NN <= 2 ? NN : (NN == 5 ? 3 : 2);
+    static constexpr int NG = V != 2 ? NG0 : (NN <= 4 ? NN : 2);
     // Shared memory, in 16-byte words.  A row of the A tile takes PS = KP
     // rounded up to 8 words, and element q of row r sits at
     // r * PS + (q ^ swz(r)): the 8 rows stored by 8 consecutive producer
@@ -95,10 +108,10 @@ __device__ __forceinline__ void dmma1684(double (&d)[4], double a0, double a1, d
 }
 
 // W (P x P, global) staged into Ws[p * WS + q] by threads t, t + nt, ...
-template <int M>
+template <int M, int V = 0>
 __device__ __forceinline__ void pair_stage_w(const double2* __restrict__ W, double2* Ws, int t,
                                              int nt) {
-    using S = PairHcShape<M>;
+    using S = PairHcShape<M, V>;
     for (int i = t; i < S::P * S::P; i += nt) Ws[(i / S::P) * S::WS + i % S::P] = W[i];
 }
 
@@ -107,10 +120,10 @@ __device__ __forceinline__ void pair_stage_w(const double2* __restrict__ W, doub
 // ---------------------------------------------------------------------------
 // Rows r = r0, r0 + rstep, ... < ROWS of tile `tr` of the (N-2)-boson space
 // into As[at(r, p)]: A_m(Q) = sqrt((m_q+1)(m_l+1+[q=l])) C[m + e_q + e_l].
-template <int M>
+template <int M, int V = 0>
 __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* __restrict__ C,
                                             uint32_t tr, double2* As, int r0, int rstep) {
-    using S = PairHcShape<M>;
+    using S = PairHcShape<M, V>;
     constexpr int P = S::P, ROWS = S::ROWS;
     const int N = sp.N;
     const uint32_t D2 = sp.dim2;
@@ -158,11 +171,11 @@ __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* 
 // last 4 when P rounds to an odd number of 4s).  A fragments hold the real
 // and imaginary part of an element in one 16-byte load.  Columns q >= P
 // read as zero; outputs p >= P and rows m >= D2 are not stored.
-template <int M, bool REAL>
+template <int M, int V, bool REAL>
 __device__ __forceinline__ void pair_contract_mma(const double2* As, const double2* Ws, int cw,
                                                   int lane, uint32_t row0, uint32_t D2,
                                                   double2* __restrict__ Y) {
-    using S = PairHcShape<M>;
+    using S = PairHcShape<M, V>;
     constexpr int P = S::P, WS = S::WS, PS = S::PS, NN = S::NN, NG = S::NG;
     constexpr int KB8 = S::KB8, KB4 = S::KB4, NPASS = (NN + NG - 1) / NG;
     constexpr int STRIPS = S::ROWS / 16, CW = S::CONSUMERS / 32;
@@ -269,14 +282,14 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
 
 // consumer thread t (0 .. CONSUMERS-1) of a tile whose first row is row0;
 // `real`: the flag stored after the P x P entries of W
-template <int M>
+template <int M, int V = 0>
 __device__ __forceinline__ void pair_consume(const double2* As, const double2* Ws, int t,
                                              uint32_t row0, uint32_t D2, double2* __restrict__ Y,
                                              bool real) {
     if (real)
-        pair_contract_mma<M, true>(As, Ws, t >> 5, t & 31, row0, D2, Y);
+        pair_contract_mma<M, V, true>(As, Ws, t >> 5, t & 31, row0, D2, Y);
     else
-        pair_contract_mma<M, false>(As, Ws, t >> 5, t & 31, row0, D2, Y);
+        pair_contract_mma<M, V, false>(As, Ws, t >> 5, t & 31, row0, D2, Y);
 }
 
 // (HC)_row = sum over pairs P = {k <= s} present in the row of
@@ -349,22 +362,23 @@ __device__ __forceinline__ double2 pair_gather_back(const SpaceView& sp,
 // Warp-specialised and double-buffered: while the consumer warps contract
 // tile k from one A buffer, the producer warps unrank and gather tile k + 1
 // into the other; one block barrier per tile hands the buffers over.
-template <int M>
-__global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
+template <int M, int V>
+__global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
     hcp_y_kernel(SpaceView sp, const double2* __restrict__ C, const double2* __restrict__ W,
                  double2* __restrict__ Y, HcEpilogue ep) {
-    using S = PairHcShape<M>;
+    using S = PairHcShape<M, V>;
     constexpr int P = S::P, PS = S::PS, ROWS = S::ROWS;
     extern __shared__ double2 smem[];
     double2* Ws = smem;               // Ws[p * WS + q]
     double2* Ab = smem + P * S::WS;   // two buffers of ROWS x PS
     if (ep.flag != nullptr && *ep.flag != 0) return;  // Lanczos breakdown: no-op
     const int t = threadIdx.x;
-    pair_stage_w<M>(W, Ws, t, S::THREADS);
+    pair_stage_w<M, V>(W, Ws, t, S::THREADS);
     const uint32_t ntiles = (sp.dim2 + ROWS - 1) / ROWS;
     const bool producer = t >= S::CONSUMERS;
     const int pt = t - S::CONSUMERS;
-    if (producer && blockIdx.x < ntiles) pair_gather<M>(sp, C, blockIdx.x, Ab, pt, S::PRODUCERS);
+    if (producer && blockIdx.x < ntiles)
+        pair_gather<M, V>(sp, C, blockIdx.x, Ab, pt, S::PRODUCERS);
     __syncthreads();
     const bool real = W[P * P].x != 0.0;
     int buf = 0;
@@ -372,9 +386,10 @@ __global__ void __launch_bounds__(PairHcShape<M>::THREADS, 1)
         if (producer) {
             const uint32_t nx = tr + gridDim.x;
             if (nx < ntiles)
-                pair_gather<M>(sp, C, nx, Ab + (size_t)(buf ^ 1) * ROWS * PS, pt, S::PRODUCERS);
+                pair_gather<M, V>(sp, C, nx, Ab + (size_t)(buf ^ 1) * ROWS * PS, pt,
+                                  S::PRODUCERS);
         } else {
-            pair_consume<M>(Ab + (size_t)buf * ROWS * PS, Ws, t, tr * ROWS, sp.dim2, Y, real);
+            pair_consume<M, V>(Ab + (size_t)buf * ROWS * PS, Ws, t, tr * ROWS, sp.dim2, Y, real);
         }
         __syncthreads();
     }
@@ -399,32 +414,60 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+template <int M, int V>
+int hcp_set_attr() {
+    if constexpr (pair_variant_ok(M, V))
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(hcp_y_kernel<M, V>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)PairHcShape<M, V>::SMEM));
+    return 0;
+}
+
 template <int M>
 int hcp_prepare_tmpl() {
     static std::atomic<uint64_t> done{0};
     return set_attributes_once(done, []() -> int {
-        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(hcp_y_kernel<M>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)PairHcShape<M>::SMEM));
-        return 0;
+        return hcp_set_attr<M, 0>() || hcp_set_attr<M, 1>() || hcp_set_attr<M, 2>();
     });
+}
+
+// parts & 1: the contraction; parts & 2: the gather-back (with the epilogue)
+template <int M, int V>
+int hcp_launch_v(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
+                 int parts, cudaStream_t st) {
+    if constexpr (!pair_variant_ok(M, V)) {
+        set_error("pair contraction variant %d does not exist for %d orbitals", V, M);
+        return -1;
+    } else {
+        using S = PairHcShape<M, V>;
+        if (parts & 1) {
+            const uint32_t ntiles = (sp.dim2 + S::ROWS - 1) / S::ROWS;
+            const int gy = (int)std::min<uint32_t>(ntiles, (uint32_t)num_sms());
+            if (gy > 0) {
+                hcp_y_kernel<M, V><<<gy, S::THREADS, S::SMEM, st>>>(sp, C, sp.pair_w, sp.pair_y,
+                                                                    ep);
+                MCTDHB_CUDA_TRY(cudaGetLastError());
+            }
+        }
+        if (parts & 2) {
+            const uint32_t need = (sp.dim + 255) / 256;
+            const int gg =
+                (int)std::max<uint32_t>(1u, std::min<uint32_t>(need, (uint32_t)num_sms() * 8));
+            hcp_g_kernel<M><<<gg, 256, 0, st>>>(sp, sp.pair_y, HC, ep);
+            MCTDHB_CUDA_TRY(cudaGetLastError());
+        }
+        return 0;
+    }
 }
 
 template <int M>
 int hcp_apply_tmpl(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,
-                   cudaStream_t st) {
-    using S = PairHcShape<M>;
-    const uint32_t ntiles = (sp.dim2 + S::ROWS - 1) / S::ROWS;
-    const int gy = (int)std::min<uint32_t>(ntiles, (uint32_t)num_sms());
-    if (gy > 0) {
-        hcp_y_kernel<M><<<gy, S::THREADS, S::SMEM, st>>>(sp, C, sp.pair_w, sp.pair_y, ep);
-        MCTDHB_CUDA_TRY(cudaGetLastError());
+                   int variant, int parts, cudaStream_t st) {
+    switch (variant) {
+        case 1: return hcp_launch_v<M, 1>(sp, C, HC, ep, parts, st);
+        case 2: return hcp_launch_v<M, 2>(sp, C, HC, ep, parts, st);
+        default: return hcp_launch_v<M, 0>(sp, C, HC, ep, parts, st);
     }
-    const uint32_t need = (sp.dim + 255) / 256;
-    const int gg = (int)std::max<uint32_t>(1u, std::min<uint32_t>(need, (uint32_t)num_sms() * 8));
-    hcp_g_kernel<M><<<gg, 256, 0, st>>>(sp, sp.pair_y, HC, ep);
-    MCTDHB_CUDA_TRY(cudaGetLastError());
-    return 0;
 }
 
 }  // namespace mctdhb

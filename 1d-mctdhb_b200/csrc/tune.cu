@@ -1,8 +1,11 @@
 // tune.cu -- autotuner for the register-resident kernels.
 //
-// Each tuned kernel (H.C, density matrices) has a few launch variants
-// (block size, barrier interval) that compute every output with the same
-// instructions in the same order, so a choice changes speed, never results.
+// Each tuned kernel (the pair contraction of H.C, single-system and batched;
+// the per-row H.C and density kernels) has a few launch variants (rows per
+// tile, output tiles per pass; block size, barrier interval) that compute
+// every output with the same instructions in the same order, so a choice
+// changes speed, never results.  A launch function returning 1 marks a
+// variant that does not exist for the shape (skipped).
 // The first call for a (kernel, device, N, M) outside a stream capture times
 // every variant on the caller's own data and keeps the fastest; the choice
 // is cached in memory and, when MCTDHB_TUNE_CACHE names a file, appended to
@@ -59,6 +62,14 @@ int tune_lookup(const char* kernel, int N, int M) {
     return it == g_choice.end() ? -1 : it->second;
 }
 
+void tune_set(const char* kernel, int N, int M, int variant) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_cache();
+    g_choice[{kernel, dev, N, M}] = variant;
+}
+
 int tune_pick(const char* kernel, int N, int M, int nvariants, cudaStream_t st,
               int (*launch)(void* ctx, int v, cudaStream_t st), void* ctx) {
     int dev = 0;
@@ -81,7 +92,9 @@ int tune_pick(const char* kernel, int N, int M, int nvariants, cudaStream_t st,
     float best_ms = 1e30f;
     bool ok = true;
     for (int v = 0; v < nvariants && ok; v++) {
-        ok = launch(ctx, v, st) == 0;  // warm-up (and attributes)
+        const int w = launch(ctx, v, st);  // warm-up (and attributes); 1: no such variant
+        if (w == 1) continue;
+        ok = w == 0;
         cudaEventRecord(a, st);
         for (int r = 0; r < 2 && ok; r++) ok = launch(ctx, v, st) == 0;
         cudaEventRecord(b, st);
@@ -102,3 +115,21 @@ int tune_pick(const char* kernel, int N, int M, int nvariants, cudaStream_t st,
 }
 
 }  // namespace mctdhb
+
+extern "C" {
+
+int mctdhb_tune_get(const char* kernel, int npar, int norb) {
+    if (!kernel) return -1;
+    return mctdhb::tune_lookup(kernel, npar, norb);
+}
+
+int mctdhb_tune_set(const char* kernel, int npar, int norb, int variant) {
+    if (!kernel || variant < 0 || variant >= 16) {
+        mctdhb::set_error("mctdhb_tune_set: invalid argument");
+        return -1;
+    }
+    mctdhb::tune_set(kernel, npar, norb, variant);
+    return 0;
+}
+
+}  // extern "C"

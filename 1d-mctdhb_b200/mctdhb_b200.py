@@ -42,6 +42,7 @@ EXPORTED = [
     "mctdhb_batch_poll", "mctdhb_batch_fetch", "mctdhb_batch_release",
     "mctdhb_batch_monitor", "mctdhb_batch_lowest_state",
     "mctdhb_batch_kernel_count", "mctdhb_batch_stream", "mctdhb_batch_launch_hc",
+    "mctdhb_batch_variant", "mctdhb_batch_set_variant", "mctdhb_tune_get", "mctdhb_tune_set",
     "mctdhb_fp64_mma_probe",
     "sync_density_matrices", "set_regulatization_factor", "get_current_regularization_factor",
     "mctdhb_step_create", "mctdhb_step_launch", "mctdhb_step_kernel_count",
@@ -76,7 +77,7 @@ class Job(C.Structure):
                 ("check_every", C.c_int), ("reg_fac", C.c_double),
                 ("pot", C.POINTER(C.c_double)), ("orbitals", C.c_void_p), ("coef", C.c_void_p),
                 ("der_method", C.c_int), ("eig_tol", C.c_double), ("ortho_tol", C.c_double),
-                ("impr_ortho", C.c_int)]
+                ("impr_ortho", C.c_int), ("orb_method", C.c_int)]
 
 
 def load(path=LIB_PATH):
@@ -228,6 +229,14 @@ def load(path=LIB_PATH):
     L.mctdhb_batch_stream.argtypes = [vp]
     L.mctdhb_batch_launch_hc.restype = i
     L.mctdhb_batch_launch_hc.argtypes = [vp, i, i]
+    L.mctdhb_batch_variant.restype = i
+    L.mctdhb_batch_variant.argtypes = [vp, i]
+    L.mctdhb_batch_set_variant.restype = i
+    L.mctdhb_batch_set_variant.argtypes = [vp, i, i]
+    L.mctdhb_tune_get.restype = i
+    L.mctdhb_tune_get.argtypes = [C.c_char_p, i, i]
+    L.mctdhb_tune_set.restype = i
+    L.mctdhb_tune_set.argtypes = [C.c_char_p, i, i, i]
     L.mctdhb_solver_step_phase.restype = i
     L.mctdhb_solver_step_phase.argtypes = [vp, i, vp]
     L.mctdhb_solver_relax.restype = i
@@ -733,10 +742,28 @@ class Batch:
 
         return torch.cuda.ExternalStream(int(load().mctdhb_batch_stream(self.h)))
 
+    def variant(self, norb):
+        """the batched contraction's launch variant for norb (autotuned)"""
+        return int(load().mctdhb_batch_variant(self.h, norb))
+
+    def set_variant(self, norb, variant):
+        """force a variant (-1: tune again); changes speed, never results"""
+        _check(load().mctdhb_batch_set_variant(self.h, norb, variant),
+               "mctdhb_batch_set_variant")
+
     def launch_hc(self, norb, parts=3):
         """one batched H.C launch of the jobs with norb orbitals: parts = 1
         the pair contraction, 2 the gather-back, 3 both"""
         _check(load().mctdhb_batch_launch_hc(self.h, norb, parts), "mctdhb_batch_launch_hc")
+
+
+def tune_get(kernel, npar, norb):
+    """the autotuner's variant for a kernel and Fock space, -1 if untuned"""
+    return int(load().mctdhb_tune_get(kernel.encode(), npar, norb))
+
+
+def tune_set(kernel, npar, norb, variant):
+    _check(load().mctdhb_tune_set(kernel.encode(), npar, norb, variant), "mctdhb_tune_set")
 
 
 def fp64_mma_probe(blocks, iters, out, stream=None):

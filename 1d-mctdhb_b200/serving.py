@@ -94,6 +94,8 @@ class SolverLane:
                 s.set_derivative(der)
             if j.get("impr_ortho"):
                 s.set_orthogonality(True)
+            if j.get("orb_method", 0) == 31:
+                s.set_orb_method(31)
             s.set_potential(j["pot"])
             s.set_interaction(j["g"])
             s.set_state(j["orbitals"], j["coef"])

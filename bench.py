@@ -900,10 +900,11 @@ def run_single(mb, torch, name, steps, warmup):
     d2, d1 = comb(N - 2 + M - 1, M - 1), comb(N - 1 + M - 1, M - 1)
     f_hc = 8.0 * d2 * P * P
     f_dn = 8.0 * (d2 * P * (P + 1) / 2 + d1 * M * (M + 1) / 2)
+    variant = mb.tune_get("hcp_y", N, M)
     sp.close()
     del sp, d_c, hc_out
     torch.cuda.empty_cache()
-    return {"workload": c["workload"],
+    return {"workload": c["workload"], "tuned_variant_hcp_y": variant,
             "step": f"SIL({c['m']} H.C) + rho1 + rho2, one CUDA graph",
             "steps_per_s": 1000.0 / t_step, "ms_per_step": t_step, "norm_after": norm,
             "hc": {"kernels": f"hcp_y_kernel<{M}> (pair contraction, FP64 mma.sync) + "
@@ -1015,6 +1016,11 @@ def run_gpu(args):
     traffic = None
     if tr.get("bhcp_y_m6_bytes_per_launch") and Mtop == 6:  # scaled by the rows processed
         traffic = tr["bhcp_y_m6_bytes_per_launch"] * gt["rows_n_minus_2"] / tr["bhcp_y_m6_rows"]
+    line["tuned_variants"] = {
+        "bhcp_y": {str(m): b.variant(m) for m in groups},
+        "what": "launch variant of the batched pair contraction per orbital count, picked by "
+                "the autotuner on the running jobs (0 the default tile, 2 the other output-tile "
+                "grouping); variants change speed, never results"}
     line["roofline"] = {
         "bound": "tensor", "kernel": f"bhcp_y_kernel<{Mtop}> (pair contraction, FP64 mma.sync)",
         "achieved": gt["contraction_tflops"], "peak": mma_peak, "unit": "TFLOP/s",

@@ -270,8 +270,9 @@ int mctdhb_dev_double_jump_map(mctdhb_space sp, int diff, void* d_strides, void*
 /* The reference integrates one system per process (driver.c:205-330; its
  * globals driver.c:15-19 make it single-instance).  These calls have no
  * counterpart there: each admitted job is one such integration (the step of
- * mctdhb_propagate_step, driver.c:159-201, with FULLSTEP_RUNGEKUTTA orbitals,
- * FINITEDIFF, DVR or SPECTRAL derivatives and LANCZOS coefficients), and all running jobs advance together, one CUDA graph launch
+ * mctdhb_propagate_step, driver.c:159-201, with FULLSTEP_RUNGEKUTTA or
+ * SPLITSTEP orbitals, FINITEDIFF, DVR or SPECTRAL derivatives and LANCZOS
+ * coefficients), and all running jobs advance together, one CUDA graph launch
  * per step of the whole batch.  A job stops on the device after max_steps
  * steps or, in imaginary time, by the reference's energy rule checked every
  * check_every steps (driver.c:47-67 without the eigen-residual test):
@@ -310,6 +311,11 @@ typedef struct {
                                  * with state 3 (the reference exits) */
     int      impr_ortho;        /* 1: the robust projector from the first step
                                  * (orbital_integration.c:22-92) */
+    int      orb_method;        /* 0 or 30 FULLSTEP_RUNGEKUTTA, 31 SPLITSTEP
+                                 * (orbital_integration.c:352-434: exact linear half
+                                 * steps -- Crank-Nicolson for finite differences, the
+                                 * FFT exponential for DVR / spectral on periodic
+                                 * grids -- around RK of the nonlinear part) */
 } mctdhb_job;
 
 typedef struct mctdhb_batch_s* mctdhb_batch;
@@ -354,12 +360,30 @@ int    mctdhb_batch_monitor(mctdhb_batch b, int slot, double* overlap_res, doubl
  * without converging. */
 int    mctdhb_batch_lowest_state(mctdhb_batch b, int slot, int niter, double* energy);
 int    mctdhb_batch_kernel_count(mctdhb_batch b); /* kernels per step graph */
+/* The launch variant of the batched pair contraction for the jobs with
+ * norb orbitals: picked by the autotuner on the running jobs when the step
+ * graph is captured (0 the default tile, 2 the other output-tile grouping);
+ * set_variant forces one (-1: tune again) and re-captures.  A variant
+ * changes speed, never results.  No counterpart in the reference. */
+int    mctdhb_batch_variant(mctdhb_batch b, int norb);
+int    mctdhb_batch_set_variant(mctdhb_batch b, int norb, int variant);
 /* one launch of the batched H.C of the running jobs with norb orbitals
  * (out = H C of each job, on the engine's stream): parts = 1 the pair
  * contraction, 2 the gather-back, 3 both; a measurement hook for timing the
  * dominant kernels of a step */
 int    mctdhb_batch_launch_hc(mctdhb_batch b, int norb, int parts);
 void*  mctdhb_batch_stream(mctdhb_batch b);       /* the engine's cudaStream_t */
+
+/* The autotuner (no counterpart in the reference; the reference's only
+ * tuning is OpenMP scheduling, hamiltonian.c:33-37): the launch variant in
+ * use for a kernel and a Fock space -- "hcp_y" the pair contraction of the
+ * single-system H.C, keyed by (npar, norb); "bhcp_y" the batched one, keyed
+ * by (ceil(log2 rows of the group), norb); "hc" / "dens" the per-row
+ * kernels -- or -1 when not tuned yet; set records a caller's choice (it
+ * changes speed, never results).  MCTDHB_TUNE_CACHE names a file that keeps
+ * the choices across processes. */
+int    mctdhb_tune_get(const char* kernel, int npar, int norb);
+int    mctdhb_tune_set(const char* kernel, int npar, int norb, int variant);
 
 /* Throughput probe of the FP64 tensor cores (no counterpart in the
  * reference): `blocks` blocks of 256 threads, every warp running `iters`

@@ -162,3 +162,46 @@ def test_batch_admission_by_footprint(gpu, oracle):
     n, state, steps, _ = b.poll()
     assert n == 0 and steps[a0] == 5 and steps[a1] == 5
     b.close()
+
+
+SPLIT = [  # N, M, G, imag, rk, dt, g, steps, der, periodic
+    (5, 3, 64, True, 5, 0.01, 0.5, 4, 302, 1),
+    (6, 4, 96, False, 4, 0.005, 0.4, 3, 302, 1),
+    (5, 3, 64, False, 5, 0.005, 0.3, 3, 302, 0),
+    (6, 3, 64, True, 4, 0.01, 0.6, 4, 300, 1),
+    (5, 5, 96, False, 5, 0.005, 0.2, 3, 301, 1),
+]
+
+
+def test_batch_split_step_vs_oracle(gpu, oracle):
+    """split-step orbitals in the batched engine (orbital_integration.c:
+    352-434): Crank-Nicolson half steps (periodic and zero bounds), the FFT
+    exponential for DVR and spectral derivatives, against the oracle's split
+    step, all in one batch; and the same bits alone"""
+    m = 5
+    b = gpu.Batch(8, 256 << 20, m)
+    jobs, slots = [], []
+    for i, (N, M, G, imag, rk, dt, g, steps, der, per) in enumerate(SPLIT):
+        job = make_job(oracle.dim, N, M, G, imag, rk, dt, g, steps, 700 + i, der=der)
+        job["periodic"], job["orb_method"] = per, 31
+        jobs.append(job)
+        slots.append(b.admit(job))
+    assert None not in slots
+    b.step(max(c[7] for c in SPLIT) + 1)
+    for (N, M, G, imag, rk, dt, g, nst, der, per), job, s in zip(SPLIT, jobs, slots):
+        dx = (XF - XI) / (G - 1)
+        st = oracle_init(oracle, N, job["orbitals"], job["coef"], dx, job["pot"], g)
+        for _ in range(nst):
+            oracle.propagate_step(st, N, dx, dt, -0.5, 0.0, g, bool(per), imag, rk, m, job["pot"],
+                                  der=der, orb_method=31)
+        d = b.fetch(s)
+        assert d["steps"] == nst
+        for k in ("orb", "coef", "rho1"):
+            assert rel_err(d[k], st[k]) < 1e-10, (N, M, der, per, k)
+        e_ref = oracle.total_energy(M, st["rho1"], st["rho2"], st["hob"], st["hint"])
+        assert abs(d["energy"] - e_ref.real) < 1e-10 * abs(e_ref)
+    mixed = b.fetch(slots[3])
+    b.close()
+    alone = run_alone(gpu, jobs[3], SPLIT[3][7])
+    for k in ("orb", "coef", "rho1", "rho2"):
+        assert np.array_equal(alone[k], mixed[k]), k
