@@ -51,46 +51,64 @@ __global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
     if (iter == kBatchMonIter && batch_mon(cnt)[M] == 0) return;  // no residual due
     const int nt = batch_cnt(cnt, LIST_HY, M);
     const BatchTile* list = tiles + batch_off(cnt, LIST_HY, M);
-    const int vin = iter < 0 ? 0 : iter;  // input vector V[vin]
     const int t = threadIdx.x;
-    const bool producer = t >= PS_::CONSUMERS;
-    const int pt = t - PS_::CONSUMERS;
-    int wslot[2] = {-1, -1};  // slot whose W each buffer holds (same in every producer)
-    auto fill = [&](const BatchTile tl, int buf) {
-        const BatchSlot& S = slots[tl.slot];
-        const bool active = bt_hc_active(S, iter);
-        if (pt == 0)
-            meta[buf] = PairTileMeta{S.sp.pair_y, tl.idx * (uint32_t)ROWS, S.sp.dim2, active,
-                                     active && S.sp.pair_w[P * P].x != 0.0};
-        if (!active) return;
-        if (wslot[buf] != tl.slot) {
-            pair_stage_w<M, V>(S.sp.pair_w, Wb + buf * P * WS, pt, PS_::PRODUCERS);
-            wslot[buf] = tl.slot;
-        }
-        pair_gather<M, V>(S.sp, S.V + (size_t)vin * S.nc, tl.idx, Ab + (size_t)buf * ROWS * PS,
-                          pt, PS_::PRODUCERS);
-    };
-    BatchTile next{};
-    if (producer) {
+    // Producers and consumers run their own loops and meet at one block
+    // barrier per tile (named barrier 1 over all threads): the producers
+    // fill buffer buf ^ 1 while the consumers contract buffer buf.
+    if (t >= PS_::CONSUMERS) {
+        const int pt = t - PS_::CONSUMERS;
+        const int vin = iter < 0 ? 0 : iter;  // input vector V[vin]
+        int wslot[2] = {-1, -1};  // slot whose W each buffer holds (same in every producer)
+        int tslot = -1;           // slot whose tables the shared table area holds
+        void* tab = Ab + 2 * ROWS * PS;
+        auto fill = [&](const BatchTile tl, int buf) {
+            const BatchSlot& S = slots[tl.slot];
+            const bool active = bt_hc_active(S, iter);
+            if (pt == 0)
+                meta[buf] = PairTileMeta{S.sp.pair_y, tl.idx * (uint32_t)ROWS, S.sp.dim2, active,
+                                         active && S.sp.pair_w[P * P].x != 0.0};
+            if (!active) return;
+            if (wslot[buf] != tl.slot) {
+                pair_stage_w<M, V>(S.sp.pair_w, Wb + buf * P * WS, pt, PS_::PRODUCERS);
+                wslot[buf] = tl.slot;
+            }
+            // the slot's rank tables: the previous fill's reads ended at the
+            // last block barrier; the producers meet before the new reads
+            SpaceView tv = S.sp;
+            if (tslot != tl.slot) {
+                tv = pair_stage_tab(S.sp, tab, pt, PS_::PRODUCERS);
+                pair_producer_barrier<PS_::PRODUCERS>();
+                tslot = tl.slot;
+            } else if (pair_tab_fits(S.sp.N, M)) {
+                tv.sq = (const double*)tab;
+                tv.T = (const uint32_t*)((const double*)tab + S.sp.N + 3);
+            }
+            pair_gather<M, V>(tv, S.V + (size_t)vin * S.nc, tl.idx,
+                              Ab + (size_t)buf * ROWS * PS, pt, PS_::PRODUCERS);
+        };
+        BatchTile next{};
         if ((int)blockIdx.x < nt) fill(list[blockIdx.x], 0);
         if ((int)(blockIdx.x + gridDim.x) < nt) next = list[blockIdx.x + gridDim.x];
-    }
-    __syncthreads();
-    int buf = 0;
-    for (int k = blockIdx.x; k < nt; k += gridDim.x, buf ^= 1) {
-        if (producer) {
+        pair_tile_barrier<PS_::THREADS>();
+        int buf = 0;
+        for (int k = blockIdx.x; k < nt; k += gridDim.x, buf ^= 1) {
             if (k + (int)gridDim.x < nt) {
                 const BatchTile cur = next;
                 if (k + 2 * (int)gridDim.x < nt) next = list[k + 2 * gridDim.x];
                 fill(cur, buf ^ 1);
             }
-        } else {
+            pair_tile_barrier<PS_::THREADS>();
+        }
+    } else {
+        pair_tile_barrier<PS_::THREADS>();
+        int buf = 0;
+        for (int k = blockIdx.x; k < nt; k += gridDim.x, buf ^= 1) {
             const PairTileMeta tm = meta[buf];
             if (tm.active)
                 pair_consume<M, V>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * WS, t, tm.row0,
                                    tm.D2, tm.Y, tm.real != 0);
+            pair_tile_barrier<PS_::THREADS>();
         }
-        __syncthreads();
     }
 }
 
@@ -187,7 +205,8 @@ __global__ void __launch_bounds__(kBatchVecThreads)
 template <int M, int V>
 constexpr size_t batch_y_smem() {
     using PS_ = PairHcShape<M, V>;
-    return (2 * (size_t)PS_::P * PS_::WS + 2 * (size_t)PS_::ROWS * PS_::PS) * sizeof(double2);
+    return (2 * (size_t)PS_::P * PS_::WS + 2 * (size_t)PS_::ROWS * PS_::PS) * sizeof(double2) +
+           kPairTabBytes;
 }
 
 // the batched tile lists fix the rows per tile: variants 0 and 2

@@ -70,10 +70,22 @@ struct RowState {
 // T_x(L) = C(L+x, x+1) <= S.  A closed-form estimate -- exact for x = 0, the
 // root of the quadratic for x = 1, the (x+1)-th root of (x+1)! S less x/2
 // (T_x(L) ~ (L + x/2)^(x+1) / (x+1)!) for x >= 2 -- then corrected against
-// the table; the estimate is within one step for every S < 2^32 and x <= 6
-// (M <= 8, the templated kernels; the runtime-M kernels keep a binary
-// search), so a level costs two table loads instead of a binary search.
-// The corrections make the result exact whatever the estimate.
+// the table; the estimate (the root by the fast hardware power, __powf) is
+// within a step or two for every S < 2^32 and x <= 6 (M <= 8, the templated
+// kernels; the runtime-M kernels keep a binary search), so a level costs a
+// few table loads instead of a binary search.  The corrections make the
+// result exact whatever the estimate.
+// Table reads: read-only global loads (__ldg), or plain (generic) loads
+// when GEN is set -- the table may then sit in shared memory.
+template <bool GEN, typename T>
+__device__ __forceinline__ T tab_ld(const T* p) {
+    if constexpr (GEN)
+        return *p;
+    else
+        return __ldg(p);
+}
+
+template <bool GEN = false>
 __device__ __forceinline__ int cns_level(const uint32_t* __restrict__ Tx, int x, int Lmax,
                                          uint32_t S) {
     if (x == 0) return S < (uint32_t)Lmax ? (int)S : Lmax;
@@ -83,12 +95,12 @@ __device__ __forceinline__ int cns_level(const uint32_t* __restrict__ Tx, int x,
     } else {
         float f = 1.0f;  // (x+1)!
         for (int k = 2; k <= x + 1; k++) f *= (float)k;
-        est = powf(f * (float)S, 1.0f / (float)(x + 1)) - 0.5f * (float)x;
+        est = __powf(f * (float)S, 1.0f / (float)(x + 1)) - 0.5f * (float)x;
     }
     int L = est > 0.0f ? (int)est : 0;
     L = L < Lmax ? L : Lmax;
-    while (L < Lmax && __ldg(Tx + L + 1) <= S) L++;
-    while (L > 0 && __ldg(Tx + L) > S) L--;
+    while (L < Lmax && tab_ld<GEN>(Tx + L + 1) <= S) L++;
+    while (L > 0 && tab_ld<GEN>(Tx + L) > S) L--;
     return L;
 }
 

@@ -56,7 +56,8 @@ inline constexpr PairList<M> kPairs{};
 // Unrank `row` of the space of Np bosons (dimension Dp) with the rank table
 // of a space of N >= Np bosons (row stride N + 1): occupations n[] and the
 // suffix sums U1, U2 of the rank offsets of adding one / two bosons.
-template <int M, int R>
+// GEN: generic table loads (the table may be staged in shared memory).
+template <int M, int R, bool GEN = false>
 __device__ __forceinline__ void gram_unrank(const uint32_t* __restrict__ T, int N, int Np,
                                             uint32_t Dp, uint32_t row, int (&n)[M],
                                             uint32_t (&U1)[M], uint32_t (&U2)[M]) {
@@ -66,8 +67,8 @@ __device__ __forceinline__ void gram_unrank(const uint32_t* __restrict__ T, int 
 #pragma unroll
     for (int x = M - 2; x >= 0; x--) {
         const uint32_t* Tx = T + x * (N + 1);
-        const int lo = cns_level(Tx, x, Lnext, S);
-        S -= __ldg(Tx + lo);
+        const int lo = cns_level<GEN>(Tx, x, Lnext, S);
+        S -= tab_ld<GEN>(Tx + lo);
         n[x + 1] = Lnext - lo;
         L[x] = lo;
         Lnext = lo;
@@ -78,9 +79,9 @@ __device__ __forceinline__ void gram_unrank(const uint32_t* __restrict__ T, int 
 #pragma unroll
     for (int x = M - 2; x >= 0; x--) {
         const uint32_t* Tx = T + x * (N + 1);
-        const uint32_t t0 = __ldg(Tx + L[x]);
-        U1[x] = U1[x + 1] + (__ldg(Tx + L[x] + 1) - t0);
-        if constexpr (R == 2) U2[x] = U2[x + 1] + (__ldg(Tx + L[x] + 2) - t0);
+        const uint32_t t0 = tab_ld<GEN>(Tx + L[x]);
+        U1[x] = U1[x + 1] + (tab_ld<GEN>(Tx + L[x] + 1) - t0);
+        if constexpr (R == 2) U2[x] = U2[x + 1] + (tab_ld<GEN>(Tx + L[x] + 2) - t0);
     }
 }
 
@@ -154,6 +155,8 @@ __device__ __forceinline__ void gram_gather(const SpaceView& sp, uint32_t Dp,
             s2[x] = __ldg(sp.sq + n[x] + 2);
         }
     }
+    // coefficient gathers through L2 only (ld.global.cg), leaving L1 to the
+    // rank and square-root tables
     static_for<P>([&](auto pi) {
         constexpr int p = decltype(pi)::value;
         if (p % PARTS == part) {
@@ -161,7 +164,7 @@ __device__ __forceinline__ void gram_gather(const SpaceView& sp, uint32_t Dp,
             if (live) {
                 if constexpr (R == 1) {
                     const uint32_t j = j0 - U1[p];
-                    v = cscale(__ldg(C + j), __ldg(sp.sq + n[p] + 1));
+                    v = cscale(__ldcg(C + j), __ldg(sp.sq + n[p] + 1));
                 } else {
                     constexpr int q = kPairs<M>.q[p], l = kPairs<M>.l[p];
                     const uint32_t j = j0 - (U1[q] - U1[l]) - U2[l];
@@ -172,7 +175,7 @@ __device__ __forceinline__ void gram_gather(const SpaceView& sp, uint32_t Dp,
                         f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[q] + 2);
                     else
                         f = __ldg(sp.sq + n[q] + 1) * __ldg(sp.sq + n[l] + 1);
-                    v = cscale(__ldg(C + j), f);
+                    v = cscale(__ldcg(C + j), f);
                 }
             }
             As[r * PS + S::col(p)] = v;

@@ -224,7 +224,7 @@ static int pair_variant(const SpaceView& sp, const double2* C, double2* HC, cons
                         cudaStream_t st) {
     PairTuneCtx ctx{&sp, C, HC, &ep};
     const int v = tune_pick("hcp_y", sp.N, sp.M, kPairVariants, st, pair_tune_launch, &ctx);
-    return pair_variant_ok(sp.M, v) ? v : 0;
+    return v >= 0 && v < kPairVariants && pair_variant_ok(sp.M, v) ? v : 0;
 }
 
 static int hcp_apply(const SpaceView& sp, const double2* C, double2* HC, const HcEpilogue& ep,

@@ -64,9 +64,10 @@ int gram_prepare_tmpl();
 
 // Launch variants of the pair contraction (pairhc_tmpl.cuh, PairHcShape):
 // 0 the default tile, 1 half the rows per tile (up to 6 orbitals), 2 the
-// other output-tile grouping per pass (5 orbitals and more)
+// other output-tile grouping per pass (6 orbitals and more; below, it is
+// the default grouping)
 __host__ __device__ constexpr bool pair_variant_ok(int M, int V) {
-    return V == 0 || (V == 1 && M * (M + 1) / 2 <= 21) || (V == 2 && M * (M + 1) / 2 > 10);
+    return V == 0 || (V == 1 && M * (M + 1) / 2 <= 21) || (V == 2 && M * (M + 1) / 2 > 16);
 }
 constexpr int kPairVariants = 3;
 
@@ -105,6 +106,7 @@ int hc_apply(const SpaceView& sp, const double2* C, double2* HC, const double2* 
 // density.cu
 int dens_grid(const SpaceView& sp);
 size_t dens_partial_elems(const SpaceView& sp);  // doubles2 in the partial buffer
+size_t gram_partial_elems(const SpaceView& sp);  // those of the Gram kernels (M <= 8)
 int dens_apply(const SpaceView& sp, const double2* C, double2* partial, double2* rho1,
                double2* rho2, const int* d_desc, cudaStream_t st);
 int dens_descriptors(int M, int* host_desc);  // returns count; desc = 5 ints/elem

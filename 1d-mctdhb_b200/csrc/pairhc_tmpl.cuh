@@ -32,14 +32,18 @@ namespace mctdhb {
 
 __host__ __device__ constexpr int pair_stride4(int x) { return x + ((12 - x % 8) % 8); }
 
+// shared memory for the producers' rank and square-root tables
+constexpr int kPairTabBytes = 8192;
+
 // Launch variants of the pair contraction (the autotuner's choices, tune.cu):
 // every variant computes each Y value with the same instructions in the
 // same order, so a choice changes speed, never results.
 //   0  the default tile (below)
 //   1  tiles of half as many rows (up to 6 orbitals): twice the tiles, for
 //      spaces with fewer tiles than SMs
-//   2  the other output-tile grouping per pass (6 and fewer orbitals: one
-//      pass over all output tiles; 7: four at once; 8: two)
+//   2  the other output-tile grouping per pass (6 orbitals: one pass over
+//      all three output tiles; 7: four at once; 8: two; below 6 orbitals
+//      the default already takes all tiles in one pass)
 // pair_variant_ok says which exist for M; the batched engine, whose tile
 // lists fix the rows per tile, takes 0 and 2.
 // (pair_variant_ok and kPairVariants: kernels.h)
@@ -63,9 +67,14 @@ struct PairHcShape {
     // W fragments held in registers by the consumers (up to 5 orbitals; at 6
     // they would spill under the 128-register budget of a 512-thread block)
     static constexpr bool WREG = P <= 15;
-    // contraction depth: P rounded up to 4, in KB8 blocks of 8 and KB4 (0 or
-    // 1) block of 4 (mma.sync m16n8k8 / m16n8k4); 8-wide output tiles
-    static constexpr int KP = (P + 3) / 4 * 4;
+    // contraction depth on the tensor cores: P rounded up to 4, in KB8
+    // blocks of 8 and KB4 (0 or 1) block of 4 (mma.sync m16n8k8 / m16n8k4);
+    // 8-wide output tiles.  When P is one above a multiple of 4 (21 pairs,
+    // six orbitals) the last input pair is added by FP64 FMAs on the
+    // accumulator fragments after the MMAs (KTAIL) instead of a padded
+    // block: 20 columns on the tensor cores instead of 24.
+    static constexpr bool KTAIL = P % 4 == 1 && P > 4;
+    static constexpr int KP = KTAIL ? P - 1 : (P + 3) / 4 * 4;
     static constexpr int KB8 = KP / 8;
     static constexpr int KB4 = (KP % 8) / 4;
     static constexpr int NN = (P + 7) / 8;
@@ -79,12 +88,27 @@ struct PairHcShape {
     // lanes fall in 8 different bank groups, and so do the 8 lanes (rows g,
     // g + 1, columns t = 0..3) of each phase of a fragment load.  W rows take
     // WS = 4 (mod 8) words.
-    static constexpr int PS = (KP + 7) / 8 * 8;
+    static constexpr int PS = ((KTAIL ? P : KP) + 7) / 8 * 8;
     static constexpr int WS = pair_stride4(P);
-    static constexpr size_t SMEM = (2 * (size_t)ROWS * PS + (size_t)P * WS) * sizeof(double2);
+    static constexpr size_t SMEM =
+        (2 * (size_t)ROWS * PS + (size_t)P * WS) * sizeof(double2) + kPairTabBytes;
     __host__ __device__ static constexpr int swz(int r) { return ((r & 1) << 2) | ((r >> 1) & 3); }
     __host__ __device__ static constexpr int at(int r, int q) { return r * PS + (q ^ swz(r)); }
 };
+
+// barrier 1 over the block's NT threads (producer and consumer loops meet
+// here from their own code paths)
+template <int NT>
+__device__ __forceinline__ void pair_tile_barrier() {
+    asm volatile("bar.sync 1, %0;\n" ::"n"(NT) : "memory");
+}
+
+// barrier 2 over the NP producer threads (table staging in the batched
+// kernel)
+template <int NP>
+__device__ __forceinline__ void pair_producer_barrier() {
+    asm volatile("bar.sync 2, %0;\n" ::"n"(NP) : "memory");
+}
 
 // FP64 mma.sync m16n8k8: D(16x8) += A(16x8) B(8x8).  With g = lane / 4 and
 // t = lane % 4, lane l holds A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4];
@@ -105,6 +129,30 @@ __device__ __forceinline__ void dmma1684(double (&d)[4], double a0, double a1, d
         "{%0, %1, %2, %3};"
         : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
         : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// The rank table (M - 1 rows of N + 1) and the square-root table (N + 3)
+// of a space staged in shared memory for the producers' unranking, when
+// they fit kPairTabBytes (else the view keeps the global tables): the
+// unrank is a chain of dependent table reads, and the L1 left beside the
+// contraction's shared memory does not hold them against the gathers.
+__host__ __device__ constexpr bool pair_tab_fits(int N, int M) {
+    return (N + 3) * 8 + (M - 1) * (N + 1) * 4 <= kPairTabBytes;
+}
+// tab: kPairTabBytes of shared memory (8-byte aligned); threads t, t + nt, ...
+// copy; the caller synchronises its threads before the view is used
+__device__ __forceinline__ SpaceView pair_stage_tab(const SpaceView& sp, void* tab, int t,
+                                                    int nt) {
+    SpaceView v = sp;
+    if (!pair_tab_fits(sp.N, sp.M)) return v;
+    double* sq = (double*)tab;
+    uint32_t* T = (uint32_t*)(sq + sp.N + 3);
+    const int nsq = sp.N + 3, nT = (sp.M - 1) * (sp.N + 1);
+    for (int i = t; i < nsq; i += nt) sq[i] = sp.sq[i];
+    for (int i = t; i < nT; i += nt) T[i] = sp.T[i];
+    v.sq = sq;
+    v.T = T;
+    return v;
 }
 
 // W (P x P, global) staged into Ws[p * WS + q] by threads t, t + nt, ...
@@ -134,7 +182,7 @@ __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* 
         int n[M];
         uint32_t U1[M], U2[M];
         if (live) {
-            gram_unrank<M, 2>(sp.T, N, N - 2, D2, row, n, U1, U2);
+            gram_unrank<M, 2, true>(sp.T, N, N - 2, D2, row, n, U1, U2);
         } else {
 #pragma unroll
             for (int x = 0; x < M; x++) n[x] = 0, U1[x] = 0u, U2[x] = 0u;
@@ -144,8 +192,8 @@ __device__ __forceinline__ void pair_gather(const SpaceView& sp, const double2* 
         double s1[M], s2[M];
 #pragma unroll
         for (int x = 0; x < M; x++) {
-            s1[x] = __ldg(sp.sq + n[x] + 1);
-            s2[x] = __ldg(sp.sq + n[x] + 2);
+            s1[x] = sp.sq[n[x] + 1];
+            s2[x] = sp.sq[n[x] + 2];
         }
         static_for<P>([&](auto pi) {
             constexpr int p = decltype(pi)::value;
@@ -251,6 +299,31 @@ __device__ __forceinline__ void pair_contract_mma(const double2* As, const doubl
                         } else {
                             dmma1684(t2[n], a0.y, a1.y, b0.y);
                             dmma1684(t3[n], a0.x + a0.y, a1.x + a1.y, b0.x + b0.y);
+                        }
+                    }
+                }
+            }
+            if constexpr (S::KTAIL) {
+                // input pair P - 1: D[g][2t + j] += A[g][P-1] W[2t + j][P-1]
+                // (rows g + 8 alike), after the tensor-core columns
+                const double2 e0 = aat(a_g, P - 1), e1 = aat(a_h, P - 1);
+#pragma unroll
+                for (int n = 0; n < NG; n++) {
+                    const int nt = n0 + n;
+                    if (nt >= NN) continue;
+#pragma unroll
+                    for (int j = 0; j < 2; j++) {
+                        const double2 w = wat(nt * 8 + 2 * t + j, P - 1);
+                        t1[n][j] = fma(e0.x, w.x, t1[n][j]);
+                        t1[n][j + 2] = fma(e1.x, w.x, t1[n][j + 2]);
+                        if constexpr (REAL) {
+                            t2[n][j] = fma(e0.y, w.x, t2[n][j]);
+                            t2[n][j + 2] = fma(e1.y, w.x, t2[n][j + 2]);
+                        } else {
+                            t2[n][j] = fma(e0.y, w.y, t2[n][j]);
+                            t2[n][j + 2] = fma(e1.y, w.y, t2[n][j + 2]);
+                            t3[n][j] = fma(e0.x + e0.y, w.x + w.y, t3[n][j]);
+                            t3[n][j + 2] = fma(e1.x + e1.y, w.x + w.y, t3[n][j + 2]);
                         }
                     }
                 }
@@ -374,11 +447,13 @@ __global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
     if (ep.flag != nullptr && *ep.flag != 0) return;  // Lanczos breakdown: no-op
     const int t = threadIdx.x;
     pair_stage_w<M, V>(W, Ws, t, S::THREADS);
+    const SpaceView tv = pair_stage_tab(sp, Ab + 2 * ROWS * PS, t, S::THREADS);
+    __syncthreads();
     const uint32_t ntiles = (sp.dim2 + ROWS - 1) / ROWS;
     const bool producer = t >= S::CONSUMERS;
     const int pt = t - S::CONSUMERS;
     if (producer && blockIdx.x < ntiles)
-        pair_gather<M, V>(sp, C, blockIdx.x, Ab, pt, S::PRODUCERS);
+        pair_gather<M, V>(tv, C, blockIdx.x, Ab, pt, S::PRODUCERS);
     __syncthreads();
     const bool real = W[P * P].x != 0.0;
     int buf = 0;
@@ -386,7 +461,7 @@ __global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
         if (producer) {
             const uint32_t nx = tr + gridDim.x;
             if (nx < ntiles)
-                pair_gather<M, V>(sp, C, nx, Ab + (size_t)(buf ^ 1) * ROWS * PS, pt,
+                pair_gather<M, V>(tv, C, nx, Ab + (size_t)(buf ^ 1) * ROWS * PS, pt,
                                   S::PRODUCERS);
         } else {
             pair_consume<M, V>(Ab + (size_t)buf * ROWS * PS, Ws, t, tr * ROWS, sp.dim2, Y, real);

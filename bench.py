@@ -764,6 +764,60 @@ def serve_plain(mb, torch, arrivals):
     return lat, time.perf_counter() - t0 - arrivals[0][0], energy
 
 
+def run_mix_convergence(mb, torch, chunk=20):
+    """the batched workload as configured, to the end: every job of the mix
+    relaxed until its energy changes by less than 1e-10 between steps or
+    5000 steps, batched (all admitted at once, `chunk` batch steps between
+    polls) against the plain path (each job alone to its own stop through
+    mctdhb_solver_relax, one after the other).  Wall clock; the jobs' step
+    counts and energies of the two paths are compared."""
+    jobs = mix_jobs()
+    b = mb.Batch(len(jobs), arena_bytes(mb, jobs), LZ)
+    slots = [b.admit(j) for j in jobs]
+    assert None not in slots, "the arena is sized for every job"
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    done_at = {}
+    while True:
+        b.step(chunk)
+        n, st, _, _ = b.poll()
+        now = time.perf_counter() - t0
+        for i, s in enumerate(slots):
+            if st[s] != 1 and i not in done_at:
+                done_at[i] = now
+        if n == 0:
+            break
+    t_b = time.perf_counter() - t0
+    res_b = []
+    for s in slots:
+        r = b.fetch(s)
+        res_b.append({k: r[k] for k in ("energy", "steps", "converged")})
+    b.close()
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    plain_e, plain_steps, plain_done = [], [], []
+    for j in jobs:
+        e, n = plain_job(mb, torch, j)
+        plain_e.append(e)
+        plain_steps.append(n)
+        plain_done.append(time.perf_counter() - t0)
+    t_p = time.perf_counter() - t0
+    steps_b = [int(r["steps"]) for r in res_b]
+    e_b = [float(r["energy"]) for r in res_b]
+    return {
+        "jobs": len(jobs), "energy_tol": 1e-10, "max_steps": 5000,
+        "batched": {"makespan_s": t_b, "p50_done_s": float(np.median(list(done_at.values()))),
+                    "converged": sum(1 for r in res_b if r["converged"]),
+                    "steps_mean": float(np.mean(steps_b)), "steps_max": max(steps_b),
+                    "poll_every_steps": chunk},
+        "plain": {"makespan_s": t_p, "p50_done_s": float(np.median(plain_done))},
+        "makespan_speedup": t_p / t_b,
+        "steps_equal": steps_b == plain_steps,
+        "energy_max_rel_diff": max(abs(a - c) / abs(c) for a, c in zip(e_b, plain_e)),
+        "what": "the whole mix relaxed to its stop rule, batched against one job at a time "
+                "(wall clock, both on the device with the same stop rule)"}
+
+
 def percentiles(lat):
     a = np.asarray(lat)
     return {"p50_s": float(np.percentile(a, 50)), "p99_s": float(np.percentile(a, 99)),
@@ -1163,6 +1217,9 @@ def main():
     ap.add_argument("--serve-real-steps", type=int, default=500)
     ap.add_argument("--serve-big-frac", type=float, default=0.05)
     ap.add_argument("--serve-nmax", type=int, default=60)
+    ap.add_argument("--mix-convergence", action="store_true",
+                    help="the whole mix relaxed to its stop rule, batched and one at a time "
+                         "(its own JSON line; tens of minutes)")
     ap.add_argument("--profile", action="store_true",
                     help="one profiled batch step of a small mix (for ncu captures)")
     ap.add_argument("--profile-kernels", metavar="N,M", nargs="?", const="30,8",
@@ -1178,6 +1235,13 @@ def main():
             mb, torch, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs,
             args.serve_imag_steps, args.serve_real_steps, args.serve_big_frac,
             args.serve_nmax)}), flush=True)
+    elif args.mix_convergence:
+        import torch
+
+        import mctdhb_b200 as mb
+
+        torch.cuda.set_device(0)
+        print(json.dumps({"mix_convergence": run_mix_convergence(mb, torch)}), flush=True)
     elif args.profile:
         run_profile()
     elif args.profile_kernels:
