@@ -178,14 +178,14 @@ static uint32_t annihilated_dim(const SpaceView& sp, int R) {
     return sp.N >= R ? (uint32_t)fock_dimension(sp.N - R, sp.M) : 0u;
 }
 
-static size_t gram_partial(const SpaceView& sp) {
+size_t gram_partial_elems(const SpaceView& sp) {
     return (size_t)gram_blocks(sp.M, 2, annihilated_dim(sp, 2)) * gram_entries(sp.M, 2) +
            (size_t)gram_blocks(sp.M, 1, annihilated_dim(sp, 1)) * gram_entries(sp.M, 1);
 }
 
 size_t dens_partial_elems(const SpaceView& sp) {
     const size_t per_row = (size_t)dens_slices(sp) * dens_ep(sp.M);
-    return dens_templated(sp.M) ? std::max(per_row, gram_partial(sp)) : per_row;
+    return dens_templated(sp.M) ? std::max(per_row, gram_partial_elems(sp)) : per_row;
 }
 
 // M <= 8: the Gram-matrix kernels (gram_tmpl.cuh)

@@ -11,18 +11,21 @@
 // one file-scope device array of kScratchBytes, which every GPU that loads
 // the library holds until the process exits.
 //
-// The kernels are the ones mctdhb_dev_density_matrices runs (dens_kernel
-// for norb <= 8, dens_generic_kernel above, then dens_finalize_kernel); only
-// their scratch comes from here, and the grid is capped so the partial sums
-// fit.  Layout of the array for one call (each part 256-byte aligned):
+// The kernels are the ones mctdhb_dev_density_matrices runs: for norb <= 8
+// the Gram-matrix kernels (gram_tmpl.cuh; their block count is a function
+// of (npar, norb) alone, at most 296 partial sums of each density, so the
+// result is the same as that entry point's, bit for bit), above that
+// dens_generic_kernel and dens_finalize_kernel with the grid capped so the
+// partial sums fit.  Only their scratch comes from here.  Layout of the
+// array for one call (each part 256-byte aligned):
 //   T     (norb-1) x (npar+1) uint32   rank table T_m(L) = C(L+m, m+1)
 //   sq    npar+3 doubles               sqrt(0..npar+2)
-//   desc  5 ints per density element  (kind, k, s, q, l)
-//   part  slices x EP complex          per-block partial sums
+//   desc  5 ints per density element  (kind, k, s, q, l; generic kernel)
+//   part  partial sums                (Gram blocks, or slices x EP complex)
 // Every call rewrites the parts it reads before the kernels read them; the
-// templated kernel stores (does not accumulate) its slice and the generic
-// kernel zeroes its own slices first, so nothing has to start at zero and
-// nothing carries over from the previous call.
+// kernels store (do not accumulate) their partial sums, or zero their own
+// slices first, so nothing has to start at zero and nothing carries over
+// from the previous call.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,8 +43,6 @@ namespace {
 
 constexpr size_t kScratchBytes = MCTDHB_NOALLOC_SCRATCH_BYTES;
 constexpr int kMaxDevices = 64;
-// templated kernel: 2 resident 128-thread blocks per SM x 148 SMs
-constexpr int kTemplBlocks = 296;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -152,16 +153,16 @@ extern "C" int mctdhb_dev_density_matrices_noalloc(uint16_t npar, uint16_t norb,
     const size_t off_part = off_desc + align256((size_t)5 * E * sizeof(int));
     const size_t slice = (size_t)EP * sizeof(double2);
     const size_t fit = off_part < kScratchBytes ? (kScratchBytes - off_part) / slice : 0;
-    // slices: one per block (templated kernel), one per warp (generic, 4 per block)
-    const int grid = templ ? (int)std::min<size_t>({(size_t)dens_grid(sp), kTemplBlocks, fit})
-                           : (int)std::min<size_t>((size_t)dens_grid(sp), fit / 4);
-    if (grid < 1) {
+    // generic kernel: one slice per warp, 4 per block
+    const int grid = templ ? 1 : (int)std::min<size_t>((size_t)dens_grid(sp), fit / 4);
+    const size_t need = templ ? off_part + gram_partial_elems(sp) * sizeof(double2)
+                              : off_part + 4 * slice;
+    if (grid < 1 || need > kScratchBytes) {
         set_error("%s: %d particles in %d orbitals need %zu bytes of scratch; the fixed scratch "
-                  "array holds %zu (MCTDHB_NOALLOC_SCRATCH_BYTES)", fn, N, M,
-                  off_part + (templ ? 1 : 4) * slice, kScratchBytes);
+                  "array holds %zu (MCTDHB_NOALLOC_SCRATCH_BYTES)", fn, N, M, need,
+                  kScratchBytes);
         return -1;
     }
-    const int slices = templ ? grid : grid * 4;
     unsigned char* base = nullptr;
     if (scratch_address(&base)) return -1;
     uint32_t* T = (uint32_t*)base;
@@ -178,28 +179,14 @@ extern "C" int mctdhb_dev_density_matrices_noalloc(uint16_t npar, uint16_t norb,
     MCTDHB_CUDA_TRY(cudaGetLastError());
     const double2* C = (const double2*)d_coef;
     if (templ) {
-        // variant 0 of dens_launch_tmpl; grid 0 sets its launch attributes only
-        switch (M) {
-#define NOALLOC_DENS(m)                                                    \
-    case m:                                                                \
-        if (dens_launch_tmpl<m>(sp, nullptr, nullptr, 0, 0, st) ||         \
-            dens_launch_tmpl<m>(sp, C, part, grid, 0, st))                 \
-            return -1;                                                     \
-        break;
-            NOALLOC_DENS(2)
-            NOALLOC_DENS(3)
-            NOALLOC_DENS(4)
-            NOALLOC_DENS(5)
-            NOALLOC_DENS(6)
-            NOALLOC_DENS(7)
-            NOALLOC_DENS(8)
-#undef NOALLOC_DENS
-        }
-    } else {
-        dens_generic_kernel<<<grid, 128, 0, st>>>(sp, C, part, EP);
-        MCTDHB_CUDA_TRY(cudaGetLastError());
+        // the Gram kernels (launch attributes set once per device, then the
+        // two Gram passes and their fixed-order finalisation)
+        if (dens_prepare(sp, C, part, st)) return -1;
+        return dens_apply(sp, C, part, (double2*)d_rho1, (double2*)d_rho2, desc, st);
     }
-    dens_finalize_kernel<<<(E + 127) / 128, 128, 0, st>>>(M, E, EP, slices, part, desc,
+    dens_generic_kernel<<<grid, 128, 0, st>>>(sp, C, part, EP);
+    MCTDHB_CUDA_TRY(cudaGetLastError());
+    dens_finalize_kernel<<<(E + 127) / 128, 128, 0, st>>>(M, E, EP, grid * 4, part, desc,
                                                           (double2*)d_rho1, (double2*)d_rho2);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     return 0;

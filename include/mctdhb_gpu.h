@@ -392,8 +392,9 @@ int    mctdhb_tune_set(const char* kernel, int npar, int norb, int variant);
  * The roofline denominator of the pair contraction. */
 int    mctdhb_fp64_mma_probe(int blocks, int iters, void* d_out, void* stream);
 
-/* rho1 and rho2 of C, as mctdhb_dev_density_matrices computes them, with no
- * device allocation at all.  This entry point has no counterpart in the
+/* rho1 and rho2 of C, as mctdhb_dev_density_matrices computes them (the
+ * same kernels; for norb <= 8 the same bits), with no device allocation at
+ * all.  This entry point has no counterpart in the
  * reference.  It is for callers that cannot let a library call cudaMalloc
  * or cudaFree: a process whose device memory is owned by its own pool
  * allocator (PyTorch's caching allocator, an arena reserved at start-up),

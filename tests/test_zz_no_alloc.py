@@ -71,6 +71,8 @@ def test_noalloc_matches_density_matrices(gpu, N, M):
             assert np.all(np.isfinite(got1)) and np.all(np.isfinite(got2)), f"call {call}"
             assert rel_err(got1, want1) < TOL, f"rho1, call {call}"
             assert rel_err(got2, want2) < TOL, f"rho2, call {call}"
+            if 2 <= M <= 8:  # the same Gram kernels and block count: the same bits
+                assert np.array_equal(got1, want1) and np.array_equal(got2, want2), call
     finally:
         L.mctdhb_space_destroy(h)
 
