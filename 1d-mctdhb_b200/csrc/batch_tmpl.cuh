@@ -216,6 +216,7 @@ __host__ __device__ constexpr bool batch_variant_ok(int M, int V) {
 
 template <int M, int V>
 int batch_y_attr() {
+    static_assert(batch_y_smem<M, V>() <= 227 * 1024, "shared memory of one block (227 KB)");
     if constexpr (batch_variant_ok(M, V))
         MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bhcp_y_kernel<M, V>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -491,6 +491,7 @@ __global__ void __launch_bounds__(256)
 
 template <int M, int V>
 int hcp_set_attr() {
+    static_assert(PairHcShape<M, V>::SMEM <= 227 * 1024, "shared memory of one block (227 KB)");
     if constexpr (pair_variant_ok(M, V))
         MCTDHB_CUDA_TRY(cudaFuncSetAttribute(hcp_y_kernel<M, V>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
