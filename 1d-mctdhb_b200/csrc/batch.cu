@@ -315,7 +315,10 @@ int hc_group(int M, const BatchSlot* slots, const BatchTile* hy, const BatchTile
 }
 
 // the batched contraction variants (0 and 2, pairhc_tmpl.cuh)
-bool batch_v_ok(int M, int v) { return (v == 0 || v == 2) && pair_variant_ok(M, v); }
+bool batch_v_ok(int M, int v) {
+    return M >= kBatchMinOrb && M <= kBatchMaxOrb &&
+           (v == 3 || ((v == 0 || v == 2) && pair_variant_ok(M, v)));
+}
 
 // rho1 / rho2 of the slots of orbital count M (the slot list gives the
 // finalize blocks)
@@ -467,7 +470,8 @@ int tune_group(mctdhb_batch_s* b, int M) {
     int bucket = 0;
     while ((1ull << bucket) < rows) bucket++;
     BatchTuneCtx ctx{b, M};
-    const int v = tune_pick("bhcp_y", bucket, M, kPairVariants, b->st, batch_tune_launch, &ctx);
+    const int v = tune_pick("bhcp_y", bucket, M, kBatchPairVariants, b->st, batch_tune_launch,
+                            &ctx);
     b->pair_v[M] = batch_v_ok(M, v) ? v : 0;
     return 0;
 }

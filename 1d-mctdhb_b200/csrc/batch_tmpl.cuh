@@ -52,6 +52,16 @@ __global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
     const int nt = batch_cnt(cnt, LIST_HY, M);
     const BatchTile* list = tiles + batch_off(cnt, LIST_HY, M);
     const int t = threadIdx.x;
+    __shared__ uint64_t bar_full[2], bar_empty[2];  // variant 3's handover
+    if constexpr (PS_::MBAR) {
+        if (t == 0) {
+            mbar_init(&bar_full[0], PS_::PRODUCERS);
+            mbar_init(&bar_full[1], PS_::PRODUCERS);
+            mbar_init(&bar_empty[0], PS_::CONSUMERS);
+            mbar_init(&bar_empty[1], PS_::CONSUMERS);
+        }
+        __syncthreads();
+    }
     // Producers and consumers run their own loops and meet at one block
     // barrier per tile (named barrier 1 over all threads): the producers
     // fill buffer buf ^ 1 while the consumers contract buffer buf.
@@ -86,6 +96,21 @@ __global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
             pair_gather<M, V>(tv, S.V + (size_t)vin * S.nc, tl.idx,
                               Ab + (size_t)buf * ROWS * PS, pt, PS_::PRODUCERS);
         };
+        if constexpr (PS_::MBAR) {
+            // item i goes to buffer i & 1 once the consumers released it
+            // (their item i - 2), then the buffer is marked full
+            int i = 0;
+            for (int k = blockIdx.x; k < nt; k += gridDim.x, i++) {
+                const int buf = i & 1;
+                if (i >= 2 && !mbar_wait(&bar_empty[buf], ((i >> 1) - 1) & 1)) {
+                    slots[list[k].slot].flags[BF_STATE] = SLOT_ABORTED;  // handover lost
+                    return;
+                }
+                fill(list[k], buf);
+                mbar_arrive(&bar_full[buf]);
+            }
+            return;
+        }
         BatchTile next{};
         if ((int)blockIdx.x < nt) fill(list[blockIdx.x], 0);
         if ((int)(blockIdx.x + gridDim.x) < nt) next = list[blockIdx.x + gridDim.x];
@@ -100,6 +125,22 @@ __global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
             pair_tile_barrier<PS_::THREADS>();
         }
     } else {
+        if constexpr (PS_::MBAR) {
+            int i = 0;
+            for (int k = blockIdx.x; k < nt; k += gridDim.x, i++) {
+                const int buf = i & 1;
+                if (!mbar_wait(&bar_full[buf], (i >> 1) & 1)) {
+                    slots[list[k].slot].flags[BF_STATE] = SLOT_ABORTED;  // handover lost
+                    return;
+                }
+                const PairTileMeta tm = meta[buf];
+                if (tm.active)
+                    pair_consume<M, V>(Ab + (size_t)buf * ROWS * PS, Wb + buf * P * WS, t,
+                                       tm.row0, tm.D2, tm.Y, tm.real != 0);
+                mbar_arrive(&bar_empty[buf]);
+            }
+            return;
+        }
         pair_tile_barrier<PS_::THREADS>();
         int buf = 0;
         for (int k = blockIdx.x; k < nt; k += gridDim.x, buf ^= 1) {
@@ -209,9 +250,9 @@ constexpr size_t batch_y_smem() {
            kPairTabBytes;
 }
 
-// the batched tile lists fix the rows per tile: variants 0 and 2
+// the batched tile lists fix the rows per tile: variants 0, 2 and 3
 __host__ __device__ constexpr bool batch_variant_ok(int M, int V) {
-    return (V == 0 || V == 2) && pair_variant_ok(M, V);
+    return V == 3 || ((V == 0 || V == 2) && pair_variant_ok(M, V));
 }
 
 template <int M, int V>
@@ -228,7 +269,7 @@ template <int M>
 int batch_prepare() {
     static std::atomic<uint64_t> done{0};
     return set_attributes_once(done, []() -> int {
-        if (batch_y_attr<M, 0>() || batch_y_attr<M, 2>()) return -1;
+        if (batch_y_attr<M, 0>() || batch_y_attr<M, 2>() || batch_y_attr<M, 3>()) return -1;
         MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 2>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              gram_smem(M, 2)));
@@ -257,8 +298,9 @@ template <int M>
 int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
                      const int* cnt, int iter, int parts, int variant, cudaStream_t st) {
     if (parts & 1) {
-        const int rc = variant == 2 ? bhcp_y_launch<M, 2>(slots, hy, cnt, iter, st)
-                                    : bhcp_y_launch<M, 0>(slots, hy, cnt, iter, st);
+        const int rc = variant == 3   ? bhcp_y_launch<M, 3>(slots, hy, cnt, iter, st)
+                       : variant == 2 ? bhcp_y_launch<M, 2>(slots, hy, cnt, iter, st)
+                                      : bhcp_y_launch<M, 0>(slots, hy, cnt, iter, st);
         if (rc) return -1;
     }
     if (parts & 2) {

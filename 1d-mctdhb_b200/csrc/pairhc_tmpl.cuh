@@ -82,6 +82,10 @@ struct PairHcShape {
     // the accumulators of the three products within the register budget
     static constexpr int NG0 = NN <= 2 ? NN : (NN == 5 ? 3 : 2);
     static constexpr int NG = V != 2 ? NG0 : (NN <= 4 ? NN : 2);
+    // variant 3 (batched kernel): the tiles handed over through a full and
+    // an empty mbarrier per buffer instead of a block barrier per tile, so
+    // each warp moves on as soon as its buffer is ready
+    static constexpr bool MBAR = V == 3;
     // Shared memory, in 16-byte words.  A row of the A tile takes PS = KP
     // rounded up to 8 words, and element q of row r sits at
     // r * PS + (q ^ swz(r)): the 8 rows stored by 8 consecutive producer
@@ -95,6 +99,38 @@ struct PairHcShape {
     __host__ __device__ static constexpr int swz(int r) { return ((r & 1) << 2) | ((r >> 1) & 3); }
     __host__ __device__ static constexpr int at(int r, int q) { return r * PS + (q ^ swz(r)); }
 };
+
+// mbarriers in shared memory (CTA scope): init by one thread before a block
+// barrier; arrive (release) by every thread of a role; a wait (acquire)
+// that gives up after about two seconds of clock cycles and returns false,
+// so a handover that never comes cannot hold the GPU
+__device__ __forceinline__ unsigned mbar_addr(const uint64_t* bar) {
+    return (unsigned)__cvta_generic_to_shared(bar);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar_addr(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(
+                     mbar_addr(bar))
+                 : "memory");
+}
+constexpr long long kMbarWaitCycles = 4000000000LL;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    const long long t0 = clock64();
+    for (;;) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(mbar_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > kMbarWaitCycles) return false;
+    }
+}
 
 // barrier 1 over the block's NT threads (producer and consumer loops meet
 // here from their own code paths)

@@ -1074,7 +1074,8 @@ def run_gpu(args):
         "bhcp_y": {str(m): b.variant(m) for m in groups},
         "what": "launch variant of the batched pair contraction per orbital count, picked by "
                 "the autotuner on the running jobs (0 the default tile, 2 the other output-tile "
-                "grouping); variants change speed, never results"}
+                "grouping, 3 the default tile handed over through mbarriers); variants change "
+                "speed, never results"}
     line["roofline"] = {
         "bound": "tensor", "kernel": f"bhcp_y_kernel<{Mtop}> (pair contraction, FP64 mma.sync)",
         "achieved": gt["contraction_tflops"], "peak": mma_peak, "unit": "TFLOP/s",

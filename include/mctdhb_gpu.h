@@ -362,7 +362,9 @@ int    mctdhb_batch_lowest_state(mctdhb_batch b, int slot, int niter, double* en
 int    mctdhb_batch_kernel_count(mctdhb_batch b); /* kernels per step graph */
 /* The launch variant of the batched pair contraction for the jobs with
  * norb orbitals: picked by the autotuner on the running jobs when the step
- * graph is captured (0 the default tile, 2 the other output-tile grouping);
+ * graph is captured (0 the default tile, 2 the other output-tile grouping,
+ * 3 the default tile handed over through mbarriers instead of a block
+ * barrier per tile);
  * set_variant forces one (-1: tune again) and re-captures.  A variant
  * changes speed, never results.  No counterpart in the reference. */
 int    mctdhb_batch_variant(mctdhb_batch b, int norb);

@@ -73,27 +73,29 @@ def job(dim, N, M, G, seed):
 
 
 def test_batched_variants_same_bits(gpu, oracle):
-    """the same jobs stepped with the batched contraction's variants 0 and 2
-    give the same bits; the tuner's own choice is an existing variant"""
+    """the same jobs stepped with the batched contraction's variants 0, 2
+    (other output-tile grouping, from six orbitals) and 3 (mbarrier
+    handover of the tiles) give the same bits; the tuner's own choice is an
+    existing variant"""
     jobs = [job(oracle.dim, 12, 5, 96, 1), job(oracle.dim, 10, 6, 64, 2),
             job(oracle.dim, 8, 8, 64, 3)]
     res = {}
-    for v in (None, 0, 2):
+    for v in (None, 0, 2, 3):
         b = gpu.Batch(4, sum(gpu.Batch.job_bytes(j, 5) for j in jobs) + (32 << 20), 5)
         try:
             slots = [b.admit(j) for j in jobs]
+            orbs = (6, 8) if v == 2 else (5, 6, 8)
             if v is not None:
-                for M in (6, 8):
+                for M in orbs:
                     b.set_variant(M, v)
             b.step(3)
             res[v] = [b.fetch(s) for s in slots]
-            assert b.variant(5) == 0  # the only batched variant at five orbitals
-            for M in (6, 8):
+            for M in orbs:
                 got = b.variant(M)
-                assert got == (v if v is not None else got) and got in (0, 2)
+                assert got == (v if v is not None else got) and got in (0, 2, 3)
         finally:
             b.close()
-    for v in (0, None):
+    for v in (0, 3, None):
         for a, c in zip(res[2], res[v]):
             for k in ("orb", "coef", "rho1", "rho2"):
                 assert np.array_equal(a[k], c[k]), (v, k)
