@@ -65,13 +65,13 @@ int gram_prepare_tmpl();
 // Launch variants of the pair contraction (pairhc_tmpl.cuh, PairHcShape):
 // 0 the default tile, 1 half the rows per tile (up to 6 orbitals), 2 the
 // other output-tile grouping per pass (6 orbitals and more; below, it is
-// the default grouping); the batched kernel adds 3, variant 0's tiles
-// handed over through mbarriers (batch_tmpl.cuh)
+// the default grouping), 3 variant 0's tiles handed over through mbarriers
 __host__ __device__ constexpr bool pair_variant_ok(int M, int V) {
-    return V == 0 || (V == 1 && M * (M + 1) / 2 <= 21) || (V == 2 && M * (M + 1) / 2 > 16);
+    return V == 0 || V == 3 || (V == 1 && M * (M + 1) / 2 <= 21) ||
+           (V == 2 && M * (M + 1) / 2 > 16);
 }
-constexpr int kPairVariants = 3;       // single-system kernel: 0, 1, 2
-constexpr int kBatchPairVariants = 4;  // batched kernel: 0, 2 and 3 (mbarrier handover)
+constexpr int kPairVariants = 4;       // single-system kernel: 0, 1, 2, 3
+constexpr int kBatchPairVariants = 4;  // batched kernel: 0, 2, 3
 
 // H.C through the two-boson-annihilated space (pairhc_tmpl.cuh), M <= 8,
 // N >= 2: launch attributes (before any capture) and the launches

@@ -82,9 +82,9 @@ struct PairHcShape {
     // the accumulators of the three products within the register budget
     static constexpr int NG0 = NN <= 2 ? NN : (NN == 5 ? 3 : 2);
     static constexpr int NG = V != 2 ? NG0 : (NN <= 4 ? NN : 2);
-    // variant 3 (batched kernel): the tiles handed over through a full and
-    // an empty mbarrier per buffer instead of a block barrier per tile, so
-    // each warp moves on as soon as its buffer is ready
+    // variant 3: the tiles handed over through a full and an empty
+    // mbarrier per buffer instead of a block barrier per tile, so each warp
+    // moves on as soon as its buffer is ready
     static constexpr bool MBAR = V == 3;
     // Shared memory, in 16-byte words.  A row of the A tile takes PS = KP
     // rounded up to 8 words, and element q of row r sits at
@@ -484,6 +484,15 @@ __global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
     const int t = threadIdx.x;
     pair_stage_w<M, V>(W, Ws, t, S::THREADS);
     const SpaceView tv = pair_stage_tab(sp, Ab + 2 * ROWS * PS, t, S::THREADS);
+    __shared__ uint64_t bar_full[2], bar_empty[2];  // variant 3's handover
+    if constexpr (S::MBAR) {
+        if (t == 0) {
+            mbar_init(&bar_full[0], S::PRODUCERS);
+            mbar_init(&bar_full[1], S::PRODUCERS);
+            mbar_init(&bar_empty[0], S::CONSUMERS);
+            mbar_init(&bar_empty[1], S::CONSUMERS);
+        }
+    }
     __syncthreads();
     const uint32_t ntiles = (sp.dim2 + ROWS - 1) / ROWS;
     const bool producer = t >= S::CONSUMERS;
@@ -492,6 +501,35 @@ __global__ void __launch_bounds__(PairHcShape<M, V>::THREADS, 1)
         pair_gather<M, V>(tv, C, blockIdx.x, Ab, pt, S::PRODUCERS);
     __syncthreads();
     const bool real = W[P * P].x != 0.0;
+    if constexpr (S::MBAR) {
+        // variant 3: the same tiles handed over through mbarriers.  A lost
+        // handover (a wait that ran out) leaves NaN in Y, so the H.C and
+        // everything after it come out NaN instead of silently wrong.
+        int i = 0;
+        for (uint32_t tr = blockIdx.x; tr < ntiles; tr += gridDim.x, i++) {
+            const int buf = i & 1;
+            if (producer) {
+                if (i >= 1 && !mbar_wait(&bar_empty[buf ^ 1], ((i - 1) >> 1) & 1)) {
+                    Y[0] = make_double2(__longlong_as_double(0x7ff8000000000000LL), 0.0);
+                    return;
+                }
+                const uint32_t nx = tr + gridDim.x;
+                if (nx < ntiles)
+                    pair_gather<M, V>(tv, C, nx, Ab + (size_t)(buf ^ 1) * ROWS * PS, pt,
+                                      S::PRODUCERS);
+                mbar_arrive(&bar_full[buf ^ 1]);
+            } else {
+                if (i >= 1 && !mbar_wait(&bar_full[buf], ((i - 1) >> 1) & 1)) {
+                    Y[0] = make_double2(__longlong_as_double(0x7ff8000000000000LL), 0.0);
+                    return;
+                }
+                pair_consume<M, V>(Ab + (size_t)buf * ROWS * PS, Ws, t, tr * ROWS, sp.dim2, Y,
+                                   real);
+                mbar_arrive(&bar_empty[buf]);
+            }
+        }
+        return;
+    }
     int buf = 0;
     for (uint32_t tr = blockIdx.x; tr < ntiles; tr += gridDim.x, buf ^= 1) {
         if (producer) {
@@ -539,7 +577,8 @@ template <int M>
 int hcp_prepare_tmpl() {
     static std::atomic<uint64_t> done{0};
     return set_attributes_once(done, []() -> int {
-        return hcp_set_attr<M, 0>() || hcp_set_attr<M, 1>() || hcp_set_attr<M, 2>();
+        return hcp_set_attr<M, 0>() || hcp_set_attr<M, 1>() || hcp_set_attr<M, 2>() ||
+               hcp_set_attr<M, 3>();
     });
 }
 
@@ -578,6 +617,7 @@ int hcp_apply_tmpl(const SpaceView& sp, const double2* C, double2* HC, const HcE
     switch (variant) {
         case 1: return hcp_launch_v<M, 1>(sp, C, HC, ep, parts, st);
         case 2: return hcp_launch_v<M, 2>(sp, C, HC, ep, parts, st);
+        case 3: return hcp_launch_v<M, 3>(sp, C, HC, ep, parts, st);
         default: return hcp_launch_v<M, 0>(sp, C, HC, ep, parts, st);
     }
 }

@@ -12,8 +12,9 @@ from oracle import hermite_orbitals
 pytestmark = pytest.mark.gpu
 
 # variants of the pair contraction per orbital count (kernels.h,
-# pair_variant_ok): 0 always, 1 up to 6 orbitals, 2 from 6 orbitals
-VARIANTS = {4: [0, 1], 5: [0, 1], 6: [0, 1, 2], 8: [0, 2]}
+# pair_variant_ok): 0 and 3 (mbarrier handover) always, 1 up to 6 orbitals,
+# 2 from 6 orbitals
+VARIANTS = {4: [0, 1, 3], 5: [0, 1, 3], 6: [0, 1, 2, 3], 8: [0, 2, 3]}
 
 
 @pytest.mark.parametrize("N,M", [(14, 4), (12, 5), (20, 6), (12, 8)])
