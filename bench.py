@@ -964,7 +964,10 @@ def run_single(mb, torch, name, steps, warmup):
             "hc": {"kernels": f"hcp_y_kernel<{M}> (pair contraction, FP64 mma.sync) + "
                               f"hcp_g_kernel<{M}> (gather-back)",
                    "ms_per_launch": t_hc * 1e3, "contraction_flops": f_hc,
-                   "contraction_tflops": f_hc / t_hc / 1e12,
+                   "contraction_tflops_over_hc_time": f_hc / t_hc / 1e12,
+                   "contraction_tflops_note": "the contraction's FLOPs over the whole H.C time "
+                                              "(contraction + gather-back); the contraction "
+                                              "alone is timed by ncu under profiles/",
                    "pair_scratch_bytes": 16.0 * d2 * P,
                    "gather_model_gbs": b_hc / t_hc / 1e9,
                    "gather_model_note": "32 nc + 16 G bytes (one 16-byte gather per distinct "
