@@ -89,12 +89,12 @@ int job_layout(int N, int M, int G, int lz, int der, int periodic, int split, Jo
     L.D2 = (uint32_t)fock_dimension(N - 2, M);
     L.vtiles = (int)((dim + kBatchVecRows - 1) / kBatchVecRows);
     L.ytiles = (int)((L.D2 + batch_pair_rows(M) - 1) / batch_pair_rows(M));
-    // Gram slices: consecutive row tiles, at most kBatchMaxSlices per order
-    for (int R = 1; R <= 2; R++) {
-        const uint64_t Dp = R == 2 ? L.D2 : L.D1;
-        const uint64_t ntr = (Dp + gram_rows(M, R) - 1) / gram_rows(M, R);
-        L.gk[R] = (int)std::max<uint64_t>(1, (ntr + kBatchMaxSlices - 1) / kBatchMaxSlices);
-        L.gs[R] = (int)((ntr + L.gk[R] - 1) / L.gk[R]);
+    // rho2 Gram slices: consecutive row tiles, at most kBatchMaxSlices (rho1
+    // follows from rho2: no rho1 Gram pass)
+    {
+        const uint64_t ntr = (L.D2 + gram_rows(M, 2) - 1) / gram_rows(M, 2);
+        L.gk[2] = (int)std::max<uint64_t>(1, (ntr + kBatchMaxSlices - 1) / kBatchMaxSlices);
+        L.gs[2] = (int)((ntr + L.gk[2] - 1) / L.gk[2]);
     }
     const size_t n = (size_t)M * G, M2 = (size_t)M * M, M4 = M2 * M2, z = sizeof(double2);
     const size_t P = (size_t)M * (M + 1) / 2;
@@ -125,8 +125,7 @@ int job_layout(int N, int M, int G, int lz, int der, int periodic, int split, Jo
     L.o_out = take((size_t)dim * z);
     L.o_part = take((size_t)kBatchMaxLz * L.vtiles * z);
     L.o_py = take((size_t)L.D2 * P * z);
-    L.o_gpart = take(((size_t)L.gs[2] * gram_entries(M, 2) + (size_t)L.gs[1] * gram_entries(M, 1)) *
-                     z);
+    L.o_gpart = take((size_t)L.gs[2] * gram_entries(M, 2) * z);
     if (split && !periodic && der != 0 && der != kDerFiniteDiff) {
         set_error("batch: the split step's FFT exponential needs periodic boundaries");
         return -1;
@@ -163,7 +162,7 @@ struct mctdhb_batch_s {
     double2* d_scal = nullptr;  // max_slots x BS_TOTAL
     int* d_flags = nullptr;     // max_slots x BF_TOTAL
     // work lists (device) and their pinned host images: vector tiles, and the
-    // per-M lists LIST_HG, LIST_HY, LIST_G2, LIST_G1 (batch.h)
+    // per-M lists LIST_HG, LIST_HY, LIST_G2 (batch.h)
     size_t cap_vec = 0, cap[kBatchLists] = {};
     int* d_list = nullptr;  // [0] count, [1..] slots
     BatchTile* d_vec = nullptr;
@@ -174,7 +173,7 @@ struct mctdhb_batch_s {
     BatchTile* h_tl[kBatchLists] = {};
     int* h_cnt = nullptr;
     // single-slot lists of the admission set-up: [0] 1, [1] slot, then a
-    // count block; Gram slices of R = 2 at d_pro_g, of R = 1 after them
+    // count block; its rho2 Gram slices at d_pro_g
     int* d_pro = nullptr;
     BatchTile* d_pro_g = nullptr;
     int* h_pro = nullptr;
@@ -271,7 +270,6 @@ int rebuild_lists(mctdhb_batch_s* b) {
             for (uint32_t r = 0; r < h.L.nc; r += kBatchHcRows) push(LIST_HG, r);
             for (int t = 0; t < h.L.ytiles; t++) push(LIST_HY, (uint32_t)t);
             for (int g = 0; g < h.L.gs[2]; g++) push(LIST_G2, (uint32_t)g);
-            for (int g = 0; g < h.L.gs[1]; g++) push(LIST_G1, (uint32_t)g);
         }
         for (int li = 0; li < kBatchLists; li++)
             batch_cnts(b->h_cnt, li)[M] = (int)n[li] - batch_offs(b->h_cnt, li)[M];
@@ -322,16 +320,16 @@ bool batch_v_ok(int M, int v) {
 
 // rho1 / rho2 of the slots of orbital count M (the slot list gives the
 // finalize blocks)
-int dens_group(int M, const BatchSlot* slots, const BatchTile* g2, const BatchTile* g1,
-               const int* cnt, const int* list, const int* nlist, int nblocks, cudaStream_t st) {
+int dens_group(int M, const BatchSlot* slots, const BatchTile* g2, const int* cnt,
+               const int* list, const int* nlist, int nblocks, cudaStream_t st) {
     switch (M) {
-        case 2: return gram_batch_launch<2>(slots, g2, g1, cnt, list, nlist, nblocks, st);
-        case 3: return gram_batch_launch<3>(slots, g2, g1, cnt, list, nlist, nblocks, st);
-        case 4: return gram_batch_launch<4>(slots, g2, g1, cnt, list, nlist, nblocks, st);
-        case 5: return gram_batch_launch<5>(slots, g2, g1, cnt, list, nlist, nblocks, st);
-        case 6: return gram_batch_launch<6>(slots, g2, g1, cnt, list, nlist, nblocks, st);
-        case 7: return gram_batch_launch<7>(slots, g2, g1, cnt, list, nlist, nblocks, st);
-        case 8: return gram_batch_launch<8>(slots, g2, g1, cnt, list, nlist, nblocks, st);
+        case 2: return gram_batch_launch<2>(slots, g2, cnt, list, nlist, nblocks, st);
+        case 3: return gram_batch_launch<3>(slots, g2, cnt, list, nlist, nblocks, st);
+        case 4: return gram_batch_launch<4>(slots, g2, cnt, list, nlist, nblocks, st);
+        case 5: return gram_batch_launch<5>(slots, g2, cnt, list, nlist, nblocks, st);
+        case 6: return gram_batch_launch<6>(slots, g2, cnt, list, nlist, nblocks, st);
+        case 7: return gram_batch_launch<7>(slots, g2, cnt, list, nlist, nblocks, st);
+        case 8: return gram_batch_launch<8>(slots, g2, cnt, list, nlist, nblocks, st);
     }
     return 0;
 }
@@ -418,8 +416,7 @@ int enqueue_step(mctdhb_batch_s* b, unsigned mask) {
     MCTDHB_CUDA_TRY(cudaGetLastError());
     // densities, rho1 synchronisation, energy, stop rules
     if (per_group(b, mask, [&](int M, cudaStream_t s) {
-            return dens_group(M, S, b->d_tl[LIST_G2], b->d_tl[LIST_G1], b->d_cnt, sl, nL, sgrid,
-                              s);
+            return dens_group(M, S, b->d_tl[LIST_G2], b->d_cnt, sl, nL, sgrid, s);
         }))
         return -1;
     bt_tail_kernel<<<sgrid, kBatchVecThreads, 0, st>>>(S, sl, nL, 0, mon);
@@ -556,7 +553,6 @@ int mctdhb_batch_create(int max_slots, size_t arena_bytes, int lanczos_iter, mct
     b->cap[LIST_HG] = max_rows / kBatchHcRows + max_slots;
     b->cap[LIST_HY] = max_rows / 64 + max_slots;
     b->cap[LIST_G2] = max_rows / 64 + max_slots;
-    b->cap[LIST_G1] = max_rows / 64 + max_slots;
     bool bad = cudaMalloc(&b->arena, std::max<size_t>(b->arena_bytes, 256)) ||
                cudaMalloc(&b->d_slots, max_slots * sizeof(BatchSlot)) ||
                cudaMalloc(&b->d_scal, (size_t)max_slots * BS_TOTAL * sizeof(double2)) ||
@@ -565,12 +561,12 @@ int mctdhb_batch_create(int max_slots, size_t arena_bytes, int lanczos_iter, mct
                cudaMalloc(&b->d_vec, b->cap_vec * sizeof(BatchTile)) ||
                cudaMalloc(&b->d_cnt, kCntInts * sizeof(int)) ||
                cudaMalloc(&b->d_pro, (2 + kCntInts) * sizeof(int)) ||
-               cudaMalloc(&b->d_pro_g, 2 * kBatchMaxSlices * sizeof(BatchTile)) ||
+               cudaMalloc(&b->d_pro_g, kBatchMaxSlices * sizeof(BatchTile)) ||
                cudaMallocHost(&b->h_list, (max_slots + 1) * sizeof(int)) ||
                cudaMallocHost(&b->h_vec, b->cap_vec * sizeof(BatchTile)) ||
                cudaMallocHost(&b->h_cnt, kCntInts * sizeof(int)) ||
                cudaMallocHost(&b->h_pro, (2 + kCntInts) * sizeof(int)) ||
-               cudaMallocHost(&b->h_pro_g, 2 * kBatchMaxSlices * sizeof(BatchTile));
+               cudaMallocHost(&b->h_pro_g, kBatchMaxSlices * sizeof(BatchTile));
     for (int li = 0; li < kBatchLists && !bad; li++)
         bad = cudaMalloc(&b->d_tl[li], b->cap[li] * sizeof(BatchTile)) ||
               cudaMallocHost(&b->h_tl[li], b->cap[li] * sizeof(BatchTile));
@@ -813,14 +809,11 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     int* pc = hp + 2;
     batch_offs(pc, LIST_G2)[M] = 0;
     batch_cnts(pc, LIST_G2)[M] = L.gs[2];
-    batch_offs(pc, LIST_G1)[M] = 0;
-    batch_cnts(pc, LIST_G1)[M] = L.gs[1];
     for (int q = 0; q < L.gs[2]; q++) b->h_pro_g[q] = BatchTile{s, (uint32_t)q};
-    for (int q = 0; q < L.gs[1]; q++) b->h_pro_g[kBatchMaxSlices + q] = BatchTile{s, (uint32_t)q};
     const int* pl = b->d_pro;
     const int* dpc = b->d_pro + 2;
     if (cudaMemcpyAsync(b->d_pro, hp, (2 + kCntInts) * sizeof(int), cudaMemcpyHostToDevice, st) ||
-        cudaMemcpyAsync(b->d_pro_g, b->h_pro_g, 2 * kBatchMaxSlices * sizeof(BatchTile),
+        cudaMemcpyAsync(b->d_pro_g, b->h_pro_g, kBatchMaxSlices * sizeof(BatchTile),
                         cudaMemcpyHostToDevice, st)) {
         set_error("mctdhb_batch_admit: upload failed");
         return undo();
@@ -828,8 +821,7 @@ int mctdhb_batch_admit(mctdhb_batch b, const mctdhb_job* job, int* slot) {
     bt_orbital_kernel<<<1, kBatchOrbThreads, kBatchMaxGrid * sizeof(double), st>>>(
         b->d_slots, pl + 1, pl, 1, nullptr);
     if (prepare_group(M) ||
-        dens_group(M, b->d_slots, b->d_pro_g, b->d_pro_g + kBatchMaxSlices, dpc, pl + 1, pl, 1,
-                   st))
+        dens_group(M, b->d_slots, b->d_pro_g, dpc, pl + 1, pl, 1, st))
         return undo();
     bt_tail_kernel<<<1, kBatchVecThreads, 0, st>>>(b->d_slots, pl + 1, pl, 1, nullptr);
     const cudaError_t e = cudaGetLastError();

@@ -65,8 +65,8 @@ struct BatchSlot {
     uint32_t nc, max_steps;
     int vtiles;   // ceil(nc / kBatchVecRows)
     int ytiles;   // tiles of the (N-2)-boson space of the pair-space H.C
-    int gs[3];    // Gram slices of the (N-R)-boson space, index R = 1, 2
-    int gk[3];    // row tiles per Gram slice, index R
+    int gs[3];    // rho2 Gram slices of the (N-2)-boson space at index 2 (1 unused)
+    int gk[3];    // row tiles per Gram slice, index 2
     uint32_t D1;  // D(N-1, M); D(N-2, M) is sp.dim2
     int pad1;
     double dt, etol, reg_fac;
@@ -85,7 +85,7 @@ struct BatchSlot {
     const double2* half;
     double2* B;
     double2 *out, *part;
-    double2* gpart;      // Gram partials: gs[2] slices of rho2's, then gs[1] of rho1's
+    double2* gpart;      // rho2 Gram partials: gs[2] slices
     double2* scal;       // BS_TOTAL
     int* flags;          // BF_TOTAL
 };
@@ -104,9 +104,8 @@ struct BatchTile {
 constexpr int kBatchNumM = kBatchMaxOrb + 1;
 constexpr int LIST_HG = 0;  // H.C gather-back: idx = first row (kBatchHcRows rows)
 constexpr int LIST_HY = 1;  // H.C pair contraction: idx = tile of the (N-2)-space
-constexpr int LIST_G2 = 2;  // rho2 Gram: idx = slice
-constexpr int LIST_G1 = 3;  // rho1 Gram: idx = slice
-constexpr int kBatchLists = 4;
+constexpr int LIST_G2 = 2;  // rho2 Gram: idx = slice (rho1 follows from rho2)
+constexpr int kBatchLists = 3;
 constexpr int kBatchCntInts = 1 + 2 * kBatchLists * kBatchNumM;
 // after the count block: one flag per orbital count, set in a step when a
 // slot of that count needs the monitor H.C (eigen residual), cleared at the
@@ -144,9 +143,8 @@ template <int M>
 int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTile* hg,
                      const int* cnt, int iter, int parts, int variant, cudaStream_t st);
 template <int M>
-int gram_batch_launch(const BatchSlot* slots, const BatchTile* g2, const BatchTile* g1,
-                      const int* cnt, const int* list, const int* nlist, int nblocks,
-                      cudaStream_t st);
+int gram_batch_launch(const BatchSlot* slots, const BatchTile* g2, const int* cnt,
+                      const int* list, const int* nlist, int nblocks, cudaStream_t st);
 template <int M>
 int batch_prepare();
 

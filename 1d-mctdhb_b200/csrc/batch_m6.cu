@@ -3,7 +3,7 @@
 namespace mctdhb {
 template int hcp_batch_launch<6>(const BatchSlot*, const BatchTile*, const BatchTile*, const int*,
                                  int, int, int, cudaStream_t);
-template int gram_batch_launch<6>(const BatchSlot*, const BatchTile*, const BatchTile*,
-                                  const int*, const int*, const int*, int, cudaStream_t);
+template int gram_batch_launch<6>(const BatchSlot*, const BatchTile*, const int*, const int*,
+                                  const int*, int, cudaStream_t);
 template int batch_prepare<6>();
 }  // namespace mctdhb

@@ -184,23 +184,24 @@ __global__ void __launch_bounds__(kBatchHcRows)
     }
 }
 
-// Gram partial of slice `idx` of a slot: its gk[R] consecutive row tiles of
-// the (N-R)-boson space, summed into gpart (gram_tmpl.cuh building blocks)
-template <int M, int R>
+// rho2 Gram partial of slice `idx` of a slot: its gk[2] consecutive row
+// tiles of the (N-2)-boson space, summed into gpart (gram_tmpl.cuh building
+// blocks); rho1 follows from rho2 in bgram_finalize_kernel
+template <int M>
 __global__ void __launch_bounds__(kGramThreads, 2)
     bgram_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
                  const int* __restrict__ cnt) {
+    constexpr int R = 2;
     using GS = GramShape<M, R>;
-    constexpr int LIST = R == 2 ? LIST_G2 : LIST_G1;
     extern __shared__ double2 As[];
-    const int nt = batch_cnt(cnt, LIST, M);
-    const BatchTile* list = tiles + batch_off(cnt, LIST, M);
+    const int nt = batch_cnt(cnt, LIST_G2, M);
+    const BatchTile* list = tiles + batch_off(cnt, LIST_G2, M);
     const GramRole<M, R> role(threadIdx.x);
     for (int k = blockIdx.x; k < nt; k += gridDim.x) {
         const BatchTile tl = list[k];
         const BatchSlot& S = slots[tl.slot];
         if (S.flags[BF_STATE] != SLOT_RUNNING) continue;  // block-uniform
-        const uint32_t Dp = R == 2 ? S.sp.dim2 : S.D1;
+        const uint32_t Dp = S.sp.dim2;
         const uint32_t ntr = (Dp + GS::ROWS - 1) / GS::ROWS;
         const uint32_t t0 = tl.idx * (uint32_t)S.gk[R];
         const uint32_t t1 = min(t0 + (uint32_t)S.gk[R], ntr);
@@ -215,32 +216,29 @@ __global__ void __launch_bounds__(kGramThreads, 2)
             gram_accumulate<M, R>(As, role, acc);
             __syncthreads();
         }
-        double2* out = S.gpart + (R == 2 ? (size_t)tl.idx * gram_entries(M, 2)
-                                         : (size_t)S.gs[2] * gram_entries(M, 2) +
-                                               (size_t)tl.idx * gram_entries(M, 1));
-        gram_store<M, R>(role, acc, As, out);
+        gram_store<M, R>(role, acc, As, S.gpart + (size_t)tl.idx * gram_entries(M, 2));
     }
 }
 
-// rho1 / rho2 of every running slot of orbital count M: fixed-order sum of
-// the slot's slices and the reference's symmetric fill (gram_fill)
+// rho2 of every running slot of orbital count M: fixed-order sum of the
+// slot's slices and the reference's symmetric fill (gram_fill); then rho1
+// from rho2 (rho1_from_rho2: every batched job has two or more bosons)
 template <int M>
 __global__ void __launch_bounds__(kBatchVecThreads)
     bgram_finalize_kernel(const BatchSlot* __restrict__ slots, const int* __restrict__ list,
                           const int* __restrict__ nlist) {
     if ((int)blockIdx.x >= *nlist) return;
     const BatchSlot& S = slots[list[blockIdx.x]];
-    if (S.M != M || S.flags[BF_STATE] != SLOT_RUNNING) return;
-    constexpr int ENT2 = gram_entries(M, 2), ENT1 = gram_entries(M, 1);
-    for (int e = threadIdx.x; e < ENT2 + ENT1; e += blockDim.x) {
-        const bool two = e < ENT2;
-        const int ee = two ? e : e - ENT2;
-        const int ns = two ? S.gs[2] : S.gs[1], ent = two ? ENT2 : ENT1;
-        const double2* part = two ? S.gpart : S.gpart + (size_t)S.gs[2] * ENT2;
+    if (S.M != M || S.flags[BF_STATE] != SLOT_RUNNING) return;  // block-uniform
+    constexpr int ENT2 = gram_entries(M, 2);
+    const int ns = S.gs[2];
+    for (int e = threadIdx.x; e < ENT2; e += blockDim.x) {
         double2 v = make_double2(0.0, 0.0);
-        for (int q = 0; q < ns; q++) v = cadd(v, part[(size_t)q * ent + ee]);
-        gram_fill<M>(two ? 2 : 1, ee, v, S.rho1, S.rho2);
+        for (int q = 0; q < ns; q++) v = cadd(v, S.gpart[(size_t)q * ENT2 + e]);
+        gram_fill<M>(2, e, v, S.rho1, S.rho2);
     }
+    __syncthreads();  // the block's rho2 stores are visible to the whole block
+    rho1_from_rho2<M>(S.sp.N, S.rho2, S.rho1, threadIdx.x, blockDim.x);
 }
 
 template <int M, int V>
@@ -270,12 +268,9 @@ int batch_prepare() {
     static std::atomic<uint64_t> done{0};
     return set_attributes_once(done, []() -> int {
         if (batch_y_attr<M, 0>() || batch_y_attr<M, 2>() || batch_y_attr<M, 3>()) return -1;
-        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 2>,
+        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              gram_smem(M, 2)));
-        MCTDHB_CUDA_TRY(cudaFuncSetAttribute(bgram_kernel<M, 1>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             gram_smem(M, 1)));
         return 0;
     });
 }
@@ -311,12 +306,9 @@ int hcp_batch_launch(const BatchSlot* slots, const BatchTile* hy, const BatchTil
 }
 
 template <int M>
-int gram_batch_launch(const BatchSlot* slots, const BatchTile* g2, const BatchTile* g1,
-                      const int* cnt, const int* list, const int* nlist, int nblocks,
-                      cudaStream_t st) {
-    bgram_kernel<M, 2><<<num_sms() * 2, kGramThreads, gram_smem(M, 2), st>>>(slots, g2, cnt);
-    MCTDHB_CUDA_TRY(cudaGetLastError());
-    bgram_kernel<M, 1><<<num_sms() * 2, kGramThreads, gram_smem(M, 1), st>>>(slots, g1, cnt);
+int gram_batch_launch(const BatchSlot* slots, const BatchTile* g2, const int* cnt,
+                      const int* list, const int* nlist, int nblocks, cudaStream_t st) {
+    bgram_kernel<M><<<num_sms() * 2, kGramThreads, gram_smem(M, 2), st>>>(slots, g2, cnt);
     MCTDHB_CUDA_TRY(cudaGetLastError());
     bgram_finalize_kernel<M><<<std::max(nblocks, 1), kBatchVecThreads, 0, st>>>(slots, list, nlist);
     MCTDHB_CUDA_TRY(cudaGetLastError());

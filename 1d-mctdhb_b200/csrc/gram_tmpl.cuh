@@ -6,7 +6,10 @@
 // bosons removed.  Inserting the identity of the (N-R)-boson space,
 //     rho2[k,s,q,l] = sum_m conj(A_m(k,s)) A_m(q,l),  A_m(q,l) = <m|a_q a_l|C>,
 //     rho1[k][l]    = sum_m conj(B_m(k))   B_m(l),    B_m(l)   = <m|a_l|C>,
-// with m over the D(N-2, M) (resp. D(N-1, M)) configurations.  Each A value
+// with m over the D(N-2, M) (resp. D(N-1, M)) configurations.  With two or
+// more bosons only the rho2 Gram matrix is formed: rho1[k][l] =
+// sum_s rho2[k,s,s,l] / (N-1) (rho1_from_rho2); the rho1 Gram pass runs for
+// one boson, where rho2 vanishes.  Each A value
 // is one scaled coefficient, A_m(q,l) = sqrt((m_q+1)(m_l+1+[q=l])) C[m+e_q+e_l]:
 // at N=30, M=8 that is 6.7 M rows x 36 pairs = 242 M gathers (against the
 // ~3 G coupling gathers of a per-row pass) and a 36 x 36 Hermitian Gram
@@ -268,6 +271,25 @@ __device__ inline void gram_fill(int R, int ee, double2 v, double2* __restrict__
         }
 }
 
+// rho1 from the filled rho2 (N >= 2 bosons): sum_s a+_s a_s counts the N - 1
+// bosons left after a_l, so rho1[k][l] = sum_s rho2[k,s,s,l] / (N - 1).  The
+// sum runs over s in order; rho2[l,s,s,k] is the exact conjugate of
+// rho2[k,s,s,l] (gram_fill), so rho1 comes out exactly Hermitian with a
+// real diagonal.  Threads t, t + nt, ... take one entry each.
+template <int M>
+__device__ __forceinline__ void rho1_from_rho2(int N, const double2* __restrict__ rho2,
+                                               double2* __restrict__ rho1, int t, int nt) {
+    constexpr int M2 = M * M, M3 = M2 * M;
+    const double d = (double)(N - 1);
+    for (int e = t; e < M2; e += nt) {
+        const int k = e / M, l = e % M;
+        double2 v = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int s = 0; s < M; s++) v = cadd(v, rho2[k + s * M + s * M2 + l * M3]);
+        rho1[e] = make_double2(v.x / d, v.y / d);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // single-system kernels
 // ---------------------------------------------------------------------------
@@ -296,14 +318,16 @@ __global__ void __launch_bounds__(kGramThreads, 2)
 }
 
 // Sum of the block partials (block order) and the fill of rho1 / rho2; one
-// thread per packed entry, rho2's first.
+// thread per packed entry, rho2's first.  nent = ENT2 fills rho2 alone
+// (rho1 then follows from rho2: gram_rho1_kernel).
 template <int M>
-__global__ void gram_finalize_kernel(int blocks2, int blocks1, const double2* __restrict__ part2,
+__global__ void gram_finalize_kernel(int nent, int blocks2, int blocks1,
+                                     const double2* __restrict__ part2,
                                      const double2* __restrict__ part1, double2* __restrict__ rho1,
                                      double2* __restrict__ rho2) {
     constexpr int ENT2 = gram_entries(M, 2), ENT1 = gram_entries(M, 1);
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= ENT2 + ENT1) return;
+    if (e >= nent) return;
     const bool two = e < ENT2;
     const int ee = two ? e : e - ENT2;
     const int nb = two ? blocks2 : blocks1, ent = two ? ENT2 : ENT1;
@@ -311,6 +335,12 @@ __global__ void gram_finalize_kernel(int blocks2, int blocks1, const double2* __
     double2 v = make_double2(0.0, 0.0);
     for (int b = 0; b < nb; b++) v = cadd(v, part[(size_t)b * ent + ee]);
     gram_fill<M>(two ? 2 : 1, ee, v, rho1, rho2);
+}
+
+template <int M>
+__global__ void __launch_bounds__(64) gram_rho1_kernel(int N, const double2* __restrict__ rho2,
+                                                      double2* __restrict__ rho1) {
+    rho1_from_rho2<M>(N, rho2, rho1, threadIdx.x, blockDim.x);
 }
 
 template <int M, int R>
@@ -340,14 +370,21 @@ int gram_prepare_tmpl() {
 template <int M>
 int gram_apply_tmpl(const SpaceView& sp, uint32_t D2, uint32_t D1, const double2* C,
                     double2* partial, double2* rho1, double2* rho2, cudaStream_t st) {
-    const int b2 = gram_blocks(M, 2, D2), b1 = gram_blocks(M, 1, D1);
+    // two or more bosons: rho1 from rho2 (rho1_from_rho2), no rho1 Gram pass
+    const bool derive = sp.N >= 2;
+    const int b2 = gram_blocks(M, 2, D2), b1 = derive ? 0 : gram_blocks(M, 1, D1);
     double2* part2 = partial;
     double2* part1 = partial + (size_t)b2 * gram_entries(M, 2);
     if (gram_launch<M, 2>(sp, D2, C, part2, b2, st)) return -1;
     if (gram_launch<M, 1>(sp, D1, C, part1, b1, st)) return -1;
-    constexpr int ENT = gram_entries(M, 2) + gram_entries(M, 1);
-    gram_finalize_kernel<M><<<(ENT + 127) / 128, 128, 0, st>>>(b2, b1, part2, part1, rho1, rho2);
+    const int ent = gram_entries(M, 2) + (derive ? 0 : gram_entries(M, 1));
+    gram_finalize_kernel<M><<<(ent + 127) / 128, 128, 0, st>>>(ent, b2, b1, part2, part1, rho1,
+                                                               rho2);
     MCTDHB_CUDA_TRY(cudaGetLastError());
+    if (derive) {
+        gram_rho1_kernel<M><<<1, 64, 0, st>>>(sp.N, rho2, rho1);
+        MCTDHB_CUDA_TRY(cudaGetLastError());
+    }
     return 0;
 }
 

@@ -165,7 +165,7 @@ def test_hc_dropin_vs_golden(gpu, gold):
 # density matrices
 # ---------------------------------------------------------------------------
 DENS_SIZES = [(10, 4), (2, 2), (6, 1), (25, 3), (16, 5), (14, 6), (9, 7), (8, 8), (30, 6),
-              (4, 9)]
+              (4, 9), (2, 7), (3, 8)]
 
 
 @pytest.mark.parametrize("N,M", DENS_SIZES)
@@ -180,6 +180,22 @@ def test_density_vs_oracle(gpu, oracle, N, M):
     sp.density_matrices(dev(c), r1, r2)
     assert rel_err(host(r1).reshape(M, M), oracle.onebody_dm(N, M, c)) < TOL
     assert rel_err(host(r2), oracle.twobody_dm(N, M, c)) < TOL
+
+
+@pytest.mark.parametrize("M", [3, 5, 8])
+def test_density_one_boson(gpu, oracle, M):
+    """one boson: rho1 from its own Gram pass (with two or more bosons it is
+    the partial trace of rho2), rho2 identically zero"""
+    import torch
+
+    rng = np.random.default_rng(2100 + M)
+    sp = gpu.Space(1, M)
+    c = rand_coef(rng, sp.dim)
+    r1 = torch.empty(M * M, dtype=torch.complex128, device="cuda")
+    r2 = torch.full((M ** 4,), 1.0 + 1.0j, dtype=torch.complex128, device="cuda")
+    sp.density_matrices(dev(c), r1, r2)
+    assert rel_err(host(r1).reshape(M, M), oracle.onebody_dm(1, M, c)) < TOL
+    assert not np.any(host(r2))
 
 
 def test_density_dropin_vs_golden(gpu, gold):

@@ -143,3 +143,16 @@ def test_energy_identity(oracle):
         e1 = np.vdot(c, oracle.apply_hamiltonian(N, M, c, h, g))
         e2 = oracle.total_energy(M, oracle.onebody_dm(N, M, c), oracle.twobody_dm(N, M, c), h, g)
         assert abs(e1 - e2) < 1e-12 * abs(e1)
+
+
+def test_rho1_is_partial_trace_of_rho2(oracle):
+    """sum_s rho2[k,s,s,l] = (N-1) rho1[k][l]: the identity the device uses to
+    form rho1 from rho2 (two or more bosons), checked on the oracle's own
+    restatement of set_onebody_dm and set_twobody_dm (density_matrices.c:9,55)"""
+    rng = np.random.default_rng(12)
+    for N, M in [(2, 3), (10, 4), (8, 6), (5, 8), (12, 2)]:
+        c = rand_coef(rng, oracle.dim(N, M))
+        r1 = oracle.onebody_dm(N, M, c)
+        r2 = oracle.twobody_dm(N, M, c).reshape(M, M, M, M)  # [l, q, s, k]
+        trace = np.einsum("lssk->kl", r2) / (N - 1)
+        assert rel_err(trace, r1) < 1e-13, (N, M)
