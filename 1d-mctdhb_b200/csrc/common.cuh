@@ -199,13 +199,20 @@ int set_attributes_once(std::atomic<uint64_t>& done, F&& set) {
     return 0;
 }
 
+// SM count of the current device, read once per device (an atomic slot per
+// device ordinal, so host threads on different devices neither race nor
+// share a count)
 inline int num_sms() {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const bool slot = dev >= 0 && dev < 64;
+    int n = slot ? cache[dev].load(std::memory_order_relaxed) : 0;
+    if (n <= 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            n <= 0)
+            n = 148;
+        if (slot) cache[dev].store(n, std::memory_order_relaxed);
     }
     return n;
 }
