@@ -497,18 +497,19 @@ void propagate_coef_sil(MCTDHBDataStruct mctdhb, Carray cnext) {
     lanczos_fetch(h->lw, m, &iters, (double2*)lw->decomp_diag, (double2*)lw->decomp_offd, c->st);
 }
 
-// synchronize.c:10-33: the regularisation factor of sync_density_matrices
-static double g_reg_fac = 1e-9;
+// synchronize.c:10-33: the regularisation factor of sync_density_matrices,
+// process-wide as in the reference (atomic: callers on other threads read it)
+static std::atomic<double> g_reg_fac{1e-9};
 
 void set_regulatization_factor(double reg_fac) {
     if (reg_fac > 1e-6 || reg_fac < 1e-13) {
         set_error("set_regulatization_factor: %.1E outside [1E-13, 1E-6]", reg_fac);
         return;
     }
-    g_reg_fac = reg_fac;
+    g_reg_fac.store(reg_fac);
 }
 
-double get_current_regularization_factor(void) { return g_reg_fac; }
+double get_current_regularization_factor(void) { return g_reg_fac.load(); }
 
 void sync_density_matrices(MultiConfiguration mc, ManyBodyState psi) {
     if (!check_mc(mc, "sync_density_matrices") || !psi) return;
@@ -529,7 +530,7 @@ void sync_density_matrices(MultiConfiguration mc, ManyBodyState psi) {
         if (!*mctdhb_gpu_last_error()) set_error("sync_density_matrices: CUDA failure");
         return;
     }
-    if (sync_rho1(M, r1.data(), rinv.data(), g_reg_fac, work.data(), wd.data()) != 0)
+    if (sync_rho1(M, r1.data(), rinv.data(), g_reg_fac.load(), work.data(), wd.data()) != 0)
         set_error("sync_density_matrices: one-body density matrix is singular");
     for (int i = 0; i < M; i++)
         for (int j = 0; j < M; j++) {
