@@ -13,8 +13,9 @@
 //
 // The kernels are the ones mctdhb_dev_density_matrices runs: for norb <= 8
 // the Gram-matrix kernels (gram_tmpl.cuh; their block count is a function
-// of (npar, norb) alone, at most 296 partial sums of each density, so the
-// result is the same as that entry point's, bit for bit), above that
+// of (npar, norb) alone, at most 296 partial sums of rho2 -- and of rho1 for
+// one boson; with more, rho1 is rho2's partial trace -- so the result is the
+// same as that entry point's, bit for bit), above that
 // dens_generic_kernel and dens_finalize_kernel with the grid capped so the
 // partial sums fit.  Only their scratch comes from here.  Layout of the
 // array for one call (each part 256-byte aligned):
