@@ -130,6 +130,9 @@ def test_vs_reference_kernels(oracle, reference, N, M):
         r2 = reference.twobody_dm(mc, c)
         assert not np.isnan(r2).any(), "reference leaves a rho2 element unset"
         assert rel_err(oracle.twobody_dm(N, M, c), r2) < 1e-13
+        if N >= 2:  # rho1 as the partial trace of rho2, on the reference's own outputs
+            trace = np.einsum("lssk->kl", r2.reshape(M, M, M, M)) / (N - 1)
+            assert rel_err(trace, reference.onebody_dm(mc, c)) < 1e-13
     finally:
         reference.lib.destroy_multiconf_struct(mc)
 
