@@ -275,10 +275,12 @@ __device__ inline void gram_fill(int R, int ee, double2 v, double2* __restrict__
 // bosons left after a_l, so rho1[k][l] = sum_s rho2[k,s,s,l] / (N - 1).  The
 // sum runs over s in order; rho2[l,s,s,k] is the exact conjugate of
 // rho2[k,s,s,l] (gram_fill), so rho1 comes out exactly Hermitian with a
-// real diagonal.  Threads t, t + nt, ... take one entry each.
+// real diagonal.  Threads t, t + nt, ... take one entry each.  rho2 may have
+// been written earlier in the same kernel (the batched finalize), so it is
+// read through a plain pointer: no read-only (non-coherent) cache path.
 template <int M>
-__device__ __forceinline__ void rho1_from_rho2(int N, const double2* __restrict__ rho2,
-                                               double2* __restrict__ rho1, int t, int nt) {
+__device__ __forceinline__ void rho1_from_rho2(int N, const double2* rho2, double2* rho1, int t,
+                                               int nt) {
     constexpr int M2 = M * M, M3 = M2 * M;
     const double d = (double)(N - 1);
     for (int e = t; e < M2; e += nt) {
